@@ -1,0 +1,191 @@
+/*
+ * lakde_b200 — C ABI of the B200 (sm_100a) kernels for the variational-inference
+ * hot path of the locally adaptive KDEs of falkaer/lakde.
+ *
+ * Conventions shared by every entry point:
+ *  - plain device pointers and sizes; no framework types cross this boundary;
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream);
+ *    every call is asynchronous on that stream and never synchronises;
+ *  - dtype codes are the lakde_dtype values below; value arrays are row-major
+ *    and contiguous unless strides are passed explicitly;
+ *  - the caller owns and allocates every buffer, outputs included, exactly as the
+ *    reference's torch ops receive a preallocated `out`;
+ *  - the return value is a lakde_status; on failure lakde_last_error() gives a
+ *    message (per host thread).  Invalid indices found on the device do not fault:
+ *    the affected output rows are written as NaN.
+ *
+ * References are file:line inside the reference project (falkaer/lakde).
+ */
+#ifndef LAKDE_B200_H_
+#define LAKDE_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define LAKDE_API __attribute__((visibility("default")))
+#else
+#define LAKDE_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  LAKDE_F32 = 0,
+  LAKDE_F64 = 1,
+  LAKDE_I32 = 2,
+  LAKDE_I64 = 3
+} lakde_dtype;
+
+typedef enum {
+  LAKDE_OK = 0,
+  LAKDE_EINVAL = 1,      /* bad sizes, pointers or strides */
+  LAKDE_EDTYPE = 2,      /* unsupported dtype combination */
+  LAKDE_ECUDA = 3,       /* a CUDA runtime call failed */
+  LAKDE_EUNSUPPORTED = 4 /* shape outside what the kernels implement */
+} lakde_status;
+
+/* Message describing the last failed call on this host thread ("" if none). */
+LAKDE_API const char *lakde_last_error(void);
+
+/* Version of this ABI (incremented on any signature change). */
+LAKDE_API int lakde_abi_version(void);
+
+/* Largest data dimensionality D the factorisation and sparse kernels accept. */
+LAKDE_API int lakde_max_dim(void);
+
+/* ------------------------------------------------------------------------- */
+/* The three ops of the reference extension (same argument meaning).         */
+/* ------------------------------------------------------------------------- */
+
+/*
+ * CSR row pointer from a sorted row-index vector: out[i] = #{p : ind[p] < i},
+ * i = 0..M.  Replaces lakde::ind2ptr_cuda(Tensor ind, int M, Tensor out)
+ * (csrc/cuda/convert_cuda.cu:46-65, registered :67-68; Python wrapper
+ * lakde/kernels.py:93-100).  ind: I32/I64 [nnz]; out: I32/I64 [M+1].
+ * nnz == 0 writes zeros, as the reference does.
+ */
+LAKDE_API int lakde_ind2ptr(const void *ind, int ind_dtype, int64_t nnz, int64_t M,
+                  void *out, int out_dtype, void *stream);
+
+/*
+ * Dense Cholesky quad forms out[n,m] = || W_triu[n]^T (Xm[m] - Xn[n]) ||^2.
+ * Replaces lakde::chol_quad_form_cuda(W_triu, Xn, Xm, out)
+ * (csrc/cuda/chol_quad_form.cu:78-114; wrapper lakde/kernels.py:115-120).
+ * W_triu [N,D,D] must be upper triangular; entries below the diagonal are not
+ * read.  Strides are in elements (W: 3, Xn/Xm/out: 2), like the reference.
+ * dtype: F32 or F64.
+ */
+LAKDE_API int lakde_chol_quad_form(int dtype, const void *W_triu, const int64_t *W_strides,
+                         const void *Xn, const int64_t *Xn_strides,
+                         const void *Xm, const int64_t *Xm_strides, void *out,
+                         const int64_t *out_strides, int64_t N, int64_t M,
+                         int64_t D, void *stream);
+
+/*
+ * Responsibility-weighted scatter covariance (the M-step),
+ * out[n] = sum_{p in row n} value[p] (Xm[col[p]] - Xn[n]) (Xm[col[p]] - Xn[n])^T,
+ * written as a full symmetric D x D matrix.  Replaces
+ * lakde::W_inv_cuda(rowptr, col, value, Xn, Xm, out)
+ * (csrc/cuda/W_inv_cuda.cu:70-137; wrapper lakde/kernels.py:102-113).
+ * rowptr: I32/I64 [N+1]; col: I32/I64 [nnz]; value: dtype [nnz];
+ * Xn [N,D], Xm [M,D], out [N,D,D] contiguous.  dtype: F32 or F64.  A row with
+ * a column index outside [0, M) or a decreasing rowptr is written as NaN.
+ */
+LAKDE_API int lakde_W_inv(int dtype, const void *rowptr, int rowptr_dtype, const void *col,
+                int col_dtype, const void *value, const void *Xn,
+                const void *Xm, void *out, int64_t N, int64_t M, int64_t D,
+                void *stream);
+
+/* ------------------------------------------------------------------------- */
+/* New ops of the hot path.                                                   */
+/* ------------------------------------------------------------------------- */
+
+/*
+ * Batched posterior factorisation in FP64 with the per-matrix jitter ladder.
+ * For every n:
+ *   A_n = scale_n * P_n + S_n,   scale_n = nu_0 * a_n / b_n (if a, b given, else 1)
+ *   L_n = chol(A_n + jitter_n I); on failure jitter_n is re-laddered from zero
+ *         through eps * (2^(k+1) - 1), k = 0..31, and info_n = -1 if none works
+ *   W_triu_n = L_n^-T (upper),  logdet_W_n = 2 sum_i log W_triu_n[i,i]
+ *   trace_n  = || T_n^T W_triu_n ||_F^2   (if T given)
+ * Restates lakde/local_adaptive_kde.py:83-96 (calc_posterior),
+ * lakde/linalg_util.py:109-170 (stabilize_/stabilized_cholesky), :49-52
+ * (tril_inverse), :30-37 (chol_logdet, chol_mm_trace).
+ * P (optional) and T (optional) are [D,D] blocks with a batch stride in
+ * elements (0 = one matrix shared by all n).  S [N,D,D] contiguous.
+ * jitter [N] is read and updated in place.  Outputs: W_triu [N,D,D],
+ * L [N,D,D] (optional), logdet_W [N], info [N] (int32: 0 ok, -1 ladder failed),
+ * trace [N] (optional).  All value arrays have `dtype` (F32/F64); a, b, nu_0
+ * too.  D <= lakde_max_dim().
+ */
+LAKDE_API int lakde_posterior_factor(int dtype, int64_t N, int64_t D, const void *S,
+                           const void *P, int64_t P_batch_stride,
+                           const void *nu_0, const void *a, const void *b,
+                           void *jitter, double eps, void *W_triu, void *L,
+                           void *logdet_W, int32_t *info, const void *T,
+                           int64_t T_batch_stride, void *trace, void *stream);
+
+/*
+ * Sparse-pair E-step numerators.  For kernel n in [0, N) and every pair p of
+ * its CSR row (rowptr over the N kernels, col = point index into X[npts,D]):
+ *   logrho[p] = 0.5 (mvdigamma(nu_n / 2, D) + D log 2 + logdet_W_n)
+ *               - 0.5 nu_n || W_triu_n^T (X[col[p]] - X[n + kernel_offset]) ||^2
+ * and logrho[p] = -inf for the self pair col[p] == n + kernel_offset.
+ * Restates lakde/local_adaptive_kde.py:36-44 and :126-128 on a pair pattern.
+ */
+LAKDE_API int lakde_estep_logrho(int dtype, int64_t N, int64_t D, int64_t npts,
+                       const void *rowptr, int rowptr_dtype, const void *col,
+                       int col_dtype, const void *X, int64_t kernel_offset,
+                       const void *W_triu, const void *nu, const void *logdet_W,
+                       void *logrho, void *stream);
+
+/*
+ * Per-point normaliser, responsibilities and rebalance over a pair pattern
+ * given point-major: pairs of point m are pos[cptr[m] .. cptr[m+1]) (indices
+ * into logrho / r).  mode 0 (initial pass): c_m = logsumexp_n logrho.
+ * mode 1 (update): c_m = logaddexp(logsubexp(c_m, log(rsum_m) + c_m), logsumexp).
+ * Then r = exp(logrho - c_m), zeroed where r <= threshold; s_m = max(sum r, eps);
+ * c_m += log s_m; r *= clamp(1 / s_m, tiny, max); rsum_m = sum of the new r.
+ * Restates lakde/local_adaptive_kde.py:120-145 (partial_expectation_step at
+ * block_size = N) and :156-181 (rebalance_responsibilities_).
+ * cptr: I64 [npts+1]; pos: I32/I64 [nnz]; logrho, r: dtype [nnz];
+ * c, rsum: dtype [npts] (in/out).
+ */
+LAKDE_API int lakde_estep_normalise(int dtype, int64_t npts, const void *cptr,
+                          const void *pos, int pos_dtype, const void *logrho,
+                          void *r, void *c, void *rsum, int mode,
+                          double threshold, void *stream);
+
+/*
+ * Student-t log coefficients of the predictive density:
+ *   log_coeff_n = lgamma((nu_n+1)/2) - lgamma((nu_n+1-D)/2) + logdet_W_n / 2
+ *                 - D/2 log(pi), evaluated in FP64 (lakde/local_adaptive_kde.py:209-214).
+ */
+LAKDE_API int lakde_pred_coeff(int dtype, int64_t N, int64_t D, const void *nu,
+                     const void *logdet_W, void *log_coeff, void *stream);
+
+/* Workspace bytes lakde_log_pred_density needs for N kernels and Nq queries. */
+LAKDE_API size_t lakde_log_pred_density_workspace(int dtype, int64_t N, int64_t Nq,
+                                        int64_t D);
+
+/*
+ * Predictive log density of Nq queries under the N-kernel Student-t mixture:
+ *   out[q] = -log N + logsumexp_n [ log_coeff_n
+ *            - (nu_n + 1)/2 log1p(|| W_triu_n^T (Y[q] - X[n]) ||^2) ]
+ * (lakde/local_adaptive_kde.py:200-223).  workspace: device buffer of at least
+ * lakde_log_pred_density_workspace() bytes.
+ */
+LAKDE_API int lakde_log_pred_density(int dtype, int64_t N, int64_t Nq, int64_t D,
+                           const void *X, const void *W_triu, const void *nu,
+                           const void *log_coeff, const void *Y, void *out,
+                           void *workspace, size_t workspace_bytes,
+                           void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LAKDE_B200_H_ */

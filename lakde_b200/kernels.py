@@ -1,0 +1,267 @@
+"""Drop-in replacement for lakde/kernels.py backed by the sm_100a library.
+
+The three custom ops keep the reference schemas in the ``lakde`` namespace
+(csrc/cuda/convert_cuda.cu:67-68, W_inv_cuda.cu:139-140,
+chol_quad_form.cu:116-117):
+
+    lakde::ind2ptr_cuda(Tensor ind, int M, Tensor out) -> Tensor
+    lakde::W_inv_cuda(Tensor rowptr, Tensor col, Tensor value, Tensor Xn, Tensor Xm, Tensor out) -> Tensor
+    lakde::chol_quad_form_cuda(Tensor W_triu, Tensor Xn, Tensor Xm, Tensor out) -> Tensor
+
+and the Python wrappers ``ind2ptr``, ``calc_W_inv`` and ``chol_quad_form``
+keep the signatures of lakde/kernels.py:93-120.  The caller-visible
+difference: tensors on the CPU are rejected with an error instead of being
+routed to the slow torch fallbacks; the ops run only on the GPU.  float16
+values are not supported (float32 and float64 are).
+
+The new ops of the fused path (posterior factorisation, sparse E-step,
+normaliser, predictive density) are exposed as functions below; each maps
+one-to-one onto an entry point of include/lakde_b200.h.
+"""
+
+import torch
+
+from . import _native as nat
+
+_LIB = torch.library.Library("lakde", "DEF")
+_LIB.define("ind2ptr_cuda(Tensor ind, int M, Tensor out) -> Tensor")
+_LIB.define("W_inv_cuda(Tensor rowptr, Tensor col, Tensor value, Tensor Xn, Tensor Xm, Tensor out) -> Tensor")
+_LIB.define("chol_quad_form_cuda(Tensor W_triu, Tensor Xn, Tensor Xm, Tensor out) -> Tensor")
+
+
+def _assert(cond, msg="Input mismatch"):
+    if not cond:
+        raise RuntimeError(msg)
+
+
+def _ind2ptr_cuda(ind, M, out):
+    nat.require_cuda(ind, out, op="ind2ptr_cuda")
+    _assert(ind.dim() == 1 and ind.is_contiguous(), "ind must be a contiguous 1-d tensor")
+    _assert(out.dim() == 1 and out.numel() == M + 1 and out.is_contiguous(), "out must be contiguous with M + 1 entries")
+    lib = nat.lib()
+    nat.check(
+        lib.lakde_ind2ptr(
+            nat.ptr(ind), nat.dtype_code(ind), ind.numel(), M, nat.ptr(out), nat.dtype_code(out), nat.stream_of(out)
+        ),
+        "ind2ptr_cuda",
+    )
+    return out
+
+
+def _W_inv_cuda(rowptr, col, value, Xn, Xm, out):
+    nat.require_cuda(rowptr, col, value, Xn, Xm, out, op="W_inv_cuda")
+    _assert(rowptr.dim() == 1)
+    _assert(col.dim() == 1)
+    _assert(value.size(0) == col.size(0))
+    _assert(value.dim() == 1)
+    _assert(Xn.dim() == 2)
+    _assert(Xm.dim() == 2)
+    N, D = Xn.shape
+    _assert(rowptr.numel() - 1 == N)
+    _assert(Xm.size(1) == D)
+    _assert(Xn.is_contiguous() and Xm.is_contiguous() and out.is_contiguous())
+    _assert(rowptr.is_contiguous() and col.is_contiguous() and value.is_contiguous())
+    _assert(out.shape == (N, D, D), "out must have shape [N, D, D]")
+    _assert(value.dtype == Xn.dtype == Xm.dtype == out.dtype, "value, Xn, Xm and out must share a dtype")
+    nat.check(
+        nat.lib().lakde_W_inv(
+            nat.dtype_code(value),
+            nat.ptr(rowptr),
+            nat.dtype_code(rowptr),
+            nat.ptr(col),
+            nat.dtype_code(col),
+            nat.ptr(value),
+            nat.ptr(Xn),
+            nat.ptr(Xm),
+            nat.ptr(out),
+            N,
+            Xm.size(0),
+            D,
+            nat.stream_of(out),
+        ),
+        "W_inv_cuda",
+    )
+    return out
+
+
+def _chol_quad_form_cuda(W_triu, Xn, Xm, out):
+    nat.require_cuda(W_triu, Xn, Xm, out, op="chol_quad_form_cuda")
+    _assert(W_triu.dim() == 3)
+    _assert(Xn.dim() == 2)
+    _assert(Xm.dim() == 2)
+    N, M, D = Xn.size(0), Xm.size(0), Xn.size(1)
+    _assert(Xm.size(1) == D)
+    _assert(W_triu.size(0) == N)
+    _assert(W_triu.size(1) == D)
+    _assert(W_triu.size(2) == D)
+    _assert(out.dim() == 2 and out.size(0) == N and out.size(1) == M, "out must have shape [N, M]")
+    _assert(W_triu.dtype == Xn.dtype == Xm.dtype == out.dtype, "all tensors must share a dtype")
+    nat.check(
+        nat.lib().lakde_chol_quad_form(
+            nat.dtype_code(W_triu),
+            nat.ptr(W_triu),
+            nat.strides(W_triu),
+            nat.ptr(Xn),
+            nat.strides(Xn),
+            nat.ptr(Xm),
+            nat.strides(Xm),
+            nat.ptr(out),
+            nat.strides(out),
+            N,
+            M,
+            D,
+            nat.stream_of(out),
+        ),
+        "chol_quad_form_cuda",
+    )
+    return out
+
+
+_LIB.impl("ind2ptr_cuda", _ind2ptr_cuda, "CUDA")
+_LIB.impl("W_inv_cuda", _W_inv_cuda, "CUDA")
+_LIB.impl("chol_quad_form_cuda", _chol_quad_form_cuda, "CUDA")
+
+
+# --------------------------------------------------------------------------
+# Python wrappers with the reference signatures (lakde/kernels.py:93-120)
+# --------------------------------------------------------------------------
+
+
+def ind2ptr(ind, M, out=None):
+    assert ind.is_contiguous()
+    if out is None:
+        out = ind.new_empty(M + 1)
+    nat.require_cuda(ind, op="ind2ptr")
+    return torch.ops.lakde.ind2ptr_cuda(ind, M, out)
+
+
+def calc_W_inv(rowptr, col, value, Xn, Xm):
+    assert rowptr.is_contiguous()
+    assert col.is_contiguous()
+    assert value.is_contiguous()
+    assert Xn.is_contiguous()
+    assert Xm.is_contiguous()
+    nat.require_cuda(rowptr, op="calc_W_inv")
+    N, D = Xn.shape
+    out = value.new_empty(N, D, D)
+    return torch.ops.lakde.W_inv_cuda(rowptr, col, value, Xn, Xm, out)
+
+
+def chol_quad_form(W_triu, Xn, Xm):
+    nat.require_cuda(W_triu, op="chol_quad_form")
+    out = W_triu.new_empty(Xn.size(0), Xm.size(0))
+    return torch.ops.lakde.chol_quad_form_cuda(W_triu, Xn, Xm, out)
+
+
+# --------------------------------------------------------------------------
+# New ops of the hot path
+# --------------------------------------------------------------------------
+
+
+def posterior_factor(S, jitter, eps, P=None, nu_0=None, a=None, b=None, T=None, want_L=False, info=None, out=None):
+    """FP64 jittered Cholesky of A_n = nu_0 a_n / b_n P_n + S_n (see include/lakde_b200.h).
+
+    Returns (W_triu, logdet_W, info, L or None, trace or None); ``jitter`` is
+    updated in place.  ``P`` and ``T`` may be [D, D] (shared) or [N, D, D].
+    """
+    nat.require_cuda(S, jitter, P, nu_0, a, b, T, op="posterior_factor")
+    N, D, _ = S.shape
+    S = S.contiguous()
+    dt = S.dtype
+    W = torch.empty_like(S) if out is None else out
+    logdet = S.new_empty(N)
+    info = S.new_empty(N, dtype=torch.int32) if info is None else info
+    L = torch.empty_like(S) if want_L else None
+    trace = S.new_empty(N) if T is not None else None
+
+    def batch(M):
+        if M is None:
+            return None, 0
+        M = M.to(dt).contiguous()
+        return M, (0 if M.dim() == 2 else D * D)
+
+    P, pbs = batch(P)
+    T, tbs = batch(T)
+    if nu_0 is not None:
+        nu_0 = nu_0.to(dt).reshape(1).contiguous()
+    if a is not None:
+        a = a.to(dt).contiguous()
+        b = b.to(dt).contiguous()
+    assert jitter.dtype == dt and jitter.is_contiguous() and jitter.numel() == N
+    nat.check(
+        nat.lib().lakde_posterior_factor(
+            nat.dtype_code(S), N, D, nat.ptr(S), nat.ptr(P), pbs, nat.ptr(nu_0), nat.ptr(a), nat.ptr(b),
+            nat.ptr(jitter), float(eps), nat.ptr(W), nat.ptr(L), nat.ptr(logdet), nat.ptr(info), nat.ptr(T), tbs,
+            nat.ptr(trace), nat.stream_of(S),
+        ),
+        "posterior_factor",
+    )
+    return W, logdet, info, L, trace
+
+
+def estep_logrho(rowptr, col, X, W_triu, nu, logdet_W, kernel_offset=0, out=None):
+    """log rho for every pair of a kernel-major CSR pattern (see include/lakde_b200.h)."""
+    nat.require_cuda(rowptr, col, X, W_triu, nu, logdet_W, op="estep_logrho")
+    N = rowptr.numel() - 1
+    D = X.size(1)
+    out = X.new_empty(col.numel()) if out is None else out
+    nat.check(
+        nat.lib().lakde_estep_logrho(
+            nat.dtype_code(X), N, D, X.size(0), nat.ptr(rowptr), nat.dtype_code(rowptr), nat.ptr(col),
+            nat.dtype_code(col), nat.ptr(X), kernel_offset, nat.ptr(W_triu), nat.ptr(nu), nat.ptr(logdet_W),
+            nat.ptr(out), nat.stream_of(X),
+        ),
+        "estep_logrho",
+    )
+    return out
+
+
+def estep_normalise(cptr, pos, logrho, r, c, rsum, mode, threshold):
+    """Per-point normaliser, responsibilities and rebalance (see include/lakde_b200.h)."""
+    nat.require_cuda(cptr, pos, logrho, r, c, rsum, op="estep_normalise")
+    assert cptr.dtype == torch.int64
+    nat.check(
+        nat.lib().lakde_estep_normalise(
+            nat.dtype_code(logrho), c.numel(), nat.ptr(cptr), nat.ptr(pos), nat.dtype_code(pos), nat.ptr(logrho),
+            nat.ptr(r), nat.ptr(c), nat.ptr(rsum), int(mode), float(threshold or 0.0), nat.stream_of(c),
+        ),
+        "estep_normalise",
+    )
+
+
+def pred_coeff(nu, logdet_W, D, out=None):
+    nat.require_cuda(nu, logdet_W, op="pred_coeff")
+    out = torch.empty_like(nu) if out is None else out
+    nat.check(
+        nat.lib().lakde_pred_coeff(
+            nat.dtype_code(nu), nu.numel(), D, nat.ptr(nu), nat.ptr(logdet_W), nat.ptr(out), nat.stream_of(nu)
+        ),
+        "pred_coeff",
+    )
+    return out
+
+
+def log_pred_density_workspace_bytes(dtype, N, Nq, D):
+    return int(nat.lib().lakde_log_pred_density_workspace(nat._DTYPE_CODES[dtype], N, Nq, D))
+
+
+def log_pred_density(X, W_triu, nu, log_coeff, Y, out=None, workspace=None):
+    """Student-t mixture log density of the rows of Y (see include/lakde_b200.h)."""
+    nat.require_cuda(X, W_triu, nu, log_coeff, Y, op="log_pred_density")
+    N, D = X.shape
+    Y = Y.contiguous()
+    Nq = Y.size(0)
+    out = Y.new_empty(Nq) if out is None else out
+    if Nq == 0:
+        return out
+    need = log_pred_density_workspace_bytes(X.dtype, N, Nq, D)
+    if workspace is None or workspace.numel() < need:
+        workspace = torch.empty(need, dtype=torch.uint8, device=X.device)
+    nat.check(
+        nat.lib().lakde_log_pred_density(
+            nat.dtype_code(X), N, Nq, D, nat.ptr(X), nat.ptr(W_triu), nat.ptr(nu), nat.ptr(log_coeff),
+            nat.ptr(Y), nat.ptr(out), nat.ptr(workspace), workspace.numel(), nat.stream_of(X),
+        ),
+        "log_pred_density",
+    )
+    return out

@@ -190,10 +190,7 @@ def knn_graph(X, k, include_self=False, block=1024):
             cand = part[r]
             dc = d2[r, cand]
             order = np.lexsort((cand, dc))
-            sel = cand[order][:k]
-            # enforce the tie rule on the boundary: any index with a distance
-            # equal to the k-th that was left out must not precede a chosen one
-            out[s + r] = sel
+            out[s + r] = cand[order][:k]
     return out
 
 
@@ -783,3 +780,63 @@ def log_pred_density_from_factors(X, Y, W_triu, nu, logdet_W):
     Q = chol_quad_form(W_triu, X, Y)
     lp = log_coeff[:, None] - (nu[:, None] + 1) / 2 * np.log1p(Q)
     return (-math.log(N) + logsumexp0(lp.astype(X.dtype))).astype(X.dtype)
+
+
+# ---------------------------------------------------------------------------
+# the E-step on a fixed pair pattern at block_size = N
+# (lakde/local_adaptive_kde.py:98-181 with pairs outside the pattern at -inf)
+# ---------------------------------------------------------------------------
+
+
+def sparse_log_rho(rowptr, col, X, W_triu, nu, logdet_W, kernel_offset=0):
+    """log rho for the pairs of a kernel-major CSR pattern (lakde/local_adaptive_kde.py:36-44, 126-128)."""
+    rows = _rows_of(rowptr)
+    col = np.asarray(col, dtype=np.int64)
+    D = X.shape[1]
+    self_idx = rows + kernel_offset
+    delta = X[col] - X[self_idx]
+    y = np.einsum("pji,pj->pi", np.triu(W_triu)[rows], delta, optimize=True)
+    Q = (y * y).sum(-1)
+    lr = (Q * (-0.5 * nu[rows]) + log_rho_const(nu, logdet_W, D)[rows]).astype(X.dtype)
+    lr[col == self_idx] = -np.inf
+    return lr
+
+
+def sparse_normalise(col, logrho, c, rsum, npts, mode, threshold=0.0):
+    """Per-point normaliser, thresholded responsibilities and rebalance.
+
+    mode 0 restates the initial pass (lakde/local_knn_kde.py:157-193:
+    c = logaddexp(c, logsumexp), then r and the rebalance); mode 1 the update
+    (lakde/local_adaptive_kde.py:120-145 at block_size = N, then :156-181).
+    Returns (r, c_new, rsum_new).
+    """
+    dt = logrho.dtype
+    col = np.asarray(col, dtype=np.int64)
+    fi = np.finfo(dt)
+    mx = np.full(npts, -np.inf, dtype=dt)
+    np.maximum.at(mx, col, logrho)
+    ms = np.where(np.isfinite(mx), mx, 0).astype(dt)
+    se = np.zeros(npts, dtype=dt)
+    with np.errstate(invalid="ignore"):
+        np.add.at(se, col, np.exp(logrho - ms[col]).astype(dt))
+    with np.errstate(divide="ignore"):
+        lse = np.where(np.isfinite(mx), np.log(se) + ms, -np.inf).astype(dt)
+    if mode == 0:
+        c_new = np.logaddexp(c, lse).astype(dt)
+    else:
+        with np.errstate(divide="ignore"):
+            old = (np.log(rsum) + c).astype(dt)
+        c_new = np.logaddexp(logsubexp(c, old), lse).astype(dt)
+    with np.errstate(invalid="ignore"):
+        r = np.exp(logrho - c_new[col]).astype(dt)
+    if threshold:
+        r = np.where(r > threshold, r, 0).astype(dt)
+    sums = np.zeros(npts, dtype=dt)
+    np.add.at(sums, col, r)
+    sums = np.maximum(sums, fi.eps).astype(dt)
+    c_fin = (c_new + np.log(sums)).astype(dt)
+    coeff = np.clip((1 / sums).astype(dt), fi.tiny, fi.max).astype(dt)
+    r = (r * coeff[col]).astype(dt)
+    rs = np.zeros(npts, dtype=dt)
+    np.add.at(rs, col, r)
+    return r, c_fin, rs

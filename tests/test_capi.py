@@ -1,0 +1,71 @@
+"""The C-ABI library: it loads without a GPU, exports every entry point the
+header declares, and rejects bad arguments before touching the device."""
+
+import ctypes
+import os
+import re
+
+import pytest
+import torch
+
+from .conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "lakde_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"LAKDE_API\s+[\w\s\*]+?\b(lakde_\w+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def nat():
+    from lakde_b200 import _native
+
+    return _native
+
+
+def test_header_and_library_agree(nat):
+    names = declared_symbols()
+    assert len(names) >= 12
+    lib = ctypes.CDLL(nat.library_path())
+    for n in names:
+        assert hasattr(lib, n), n
+    assert sorted(nat.exported_symbols()) == names
+
+
+def test_metadata(nat):
+    lib = nat.lib()
+    assert lib.lakde_abi_version() == 1
+    assert lib.lakde_max_dim() == 64
+
+
+def test_invalid_arguments_are_rejected_on_the_host(nat):
+    lib = nat.lib()
+    st = lib.lakde_W_inv(0, None, 2, None, 2, None, None, None, None, -1, 0, 3, None)
+    assert st == 1
+    assert b"invalid" in lib.lakde_last_error()
+    assert lib.lakde_chol_quad_form(0, None, None, None, None, None, None, None, None, 1, 1, 0, None) == 1
+    assert lib.lakde_ind2ptr(None, 2, 5, -1, None, 2, None) == 1
+    assert lib.lakde_estep_normalise(0, 3, None, None, 2, None, None, None, None, 7, 0.0, None) == 1
+    assert lib.lakde_log_pred_density_workspace(0, 100, 10, 65) == 0
+    assert lib.lakde_log_pred_density_workspace(5, 100, 10, 8) == 0
+    assert lib.lakde_log_pred_density_workspace(0, 100, 10, 8) > 0
+    # an unsupported dtype code is reported as such
+    assert lib.lakde_posterior_factor(7, 1, 2, ctypes.c_void_p(8), None, 0, None, None, None,
+                                      ctypes.c_void_p(8), 0.0, ctypes.c_void_p(8), None, ctypes.c_void_p(8),
+                                      ctypes.c_void_p(8), None, 0, None, None) in (1, 2)
+
+
+def test_cpu_tensors_are_rejected():
+    from lakde_b200 import kernels
+
+    W = torch.eye(3).expand(4, 3, 3).contiguous()
+    X = torch.zeros(4, 3)
+    with pytest.raises((RuntimeError, NotImplementedError)):
+        kernels.chol_quad_form(W, X, X)
+    with pytest.raises((RuntimeError, NotImplementedError)):
+        kernels.ind2ptr(torch.zeros(3, dtype=torch.int64), 4)
+    with pytest.raises((RuntimeError, NotImplementedError)):
+        kernels.calc_W_inv(torch.zeros(5, dtype=torch.int64), torch.zeros(0, dtype=torch.int64), torch.zeros(0),
+                           X, X)

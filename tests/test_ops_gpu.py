@@ -1,0 +1,287 @@
+"""Parity of the CUDA ops (through the C ABI) with the golden vectors of the
+reference and with the oracle."""
+
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import lakde_oracle as O
+
+from .conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda"
+
+
+@pytest.fixture(scope="module")
+def K():
+    from lakde_b200 import kernels
+
+    return kernels
+
+
+@pytest.fixture(scope="module")
+def ops():
+    return np.load(os.path.join(GOLDEN, "ops.npz"))
+
+
+def t(a, dtype=None):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(DEV, dtype=dtype)
+
+
+def rand_upper(rng, N, D, dtype):
+    W = np.triu(rng.standard_normal((N, D, D)))
+    W[:, np.arange(D), np.arange(D)] = np.abs(W[:, np.arange(D), np.arange(D)]) + 0.5
+    return W.astype(dtype)
+
+
+# ----------------------------------------------------------------- quad form
+@pytest.mark.parametrize("dt", ["f32", "f64"])
+@pytest.mark.parametrize("D", [1, 2, 5, 8, 17, 33])
+def test_quad_form_golden(K, ops, dt, D):
+    k = f"quad_{dt}_d{D}"
+    Q = K.chol_quad_form(t(ops[k + "_W"]), t(ops[k + "_Xn"]), t(ops[k + "_Xm"]))
+    rtol = 1e-5 if dt == "f32" else 1e-12
+    np.testing.assert_allclose(Q.cpu().numpy(), ops[k + "_Q"], rtol=rtol, atol=rtol)
+
+
+@pytest.mark.parametrize("D", [2, 8, 21, 43, 63, 64])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_quad_form_random_strided(K, D, dtype):
+    rng = np.random.default_rng(D)
+    N, M = 37, 301
+    W = (rand_upper(rng, N, D, dtype) / np.sqrt(D)).astype(dtype)
+    Xn = rng.standard_normal((N, D)).astype(dtype)
+    Xm = rng.standard_normal((M, D)).astype(dtype)
+    ref = O.chol_quad_form(W.astype(np.float64), Xn.astype(np.float64), Xm.astype(np.float64))
+    # strided inputs and a transposed output, as the reference op accepts
+    Wt = t(np.ascontiguousarray(W.transpose(0, 2, 1))).transpose(1, 2)
+    Xnt = t(np.ascontiguousarray(Xn.T)).T
+    out = torch.empty(M, N, dtype=Wt.dtype, device=DEV).T
+    torch.ops.lakde.chol_quad_form_cuda(Wt, Xnt, t(Xm), out)
+    rtol = 2e-5 if dtype == np.float32 else 1e-11
+    np.testing.assert_allclose(out.cpu().numpy(), ref, rtol=rtol, atol=rtol * ref.max())
+
+
+def test_quad_form_rejects_large_d_and_cpu(K):
+    W = torch.zeros(2, 65, 65, device=DEV)
+    X = torch.zeros(2, 65, device=DEV)
+    with pytest.raises(RuntimeError, match="exceeds"):
+        K.chol_quad_form(W, X, X)
+    with pytest.raises(RuntimeError):
+        K.chol_quad_form(W.cpu(), X.cpu(), X.cpu())
+
+
+# ------------------------------------------------------------- scatter (M-step)
+@pytest.mark.parametrize("dt", ["f32", "f64"])
+@pytest.mark.parametrize("D", [1, 3, 7, 16])
+@pytest.mark.parametrize("idx", [(torch.int64, torch.int64), (torch.int32, torch.int32), (torch.int32, torch.int64),
+                                 (torch.int64, torch.int32)])
+def test_W_inv_golden(K, ops, dt, D, idx):
+    k = f"winv_{dt}_d{D}"
+    rowptr, col, value, Xn, Xm = (ops[f"{k}_{n}"] for n in ("rowptr", "col", "value", "Xn", "Xm"))
+    S = K.calc_W_inv(t(rowptr, idx[0]), t(col, idx[1]), t(value), t(Xn), t(Xm))
+    rtol = 1e-5 if dt == "f32" else 1e-12
+    np.testing.assert_allclose(S.cpu().numpy(), ops[k + "_S"], rtol=rtol, atol=rtol)
+
+
+@pytest.mark.parametrize("D", [2, 8, 21, 43, 63])
+def test_W_inv_random(K, D):
+    rng = np.random.default_rng(100 + D)
+    N, M = 50, 400
+    counts = rng.integers(0, 150, size=N)
+    counts[[3, 17]] = 0
+    counts[5] = 700  # a long row (several chunks)
+    rowptr = np.concatenate([[0], np.cumsum(counts)])
+    col = rng.integers(0, M, size=rowptr[-1])
+    val = rng.uniform(0, 1, size=rowptr[-1]).astype(np.float32)
+    Xn = rng.standard_normal((N, D)).astype(np.float32)
+    Xm = rng.standard_normal((M, D)).astype(np.float32)
+    ref = O.calc_W_inv(rowptr, col, val.astype(np.float64), Xn.astype(np.float64), Xm.astype(np.float64))
+    S = K.calc_W_inv(t(rowptr), t(col, torch.int32), t(val), t(Xn), t(Xm)).cpu().numpy()
+    np.testing.assert_allclose(S, ref, rtol=1e-4, atol=1e-4 * np.abs(ref).max())
+    np.testing.assert_array_equal(S, np.swapaxes(S, 1, 2))
+
+
+@pytest.mark.parametrize("D", [3, 40])
+def test_W_inv_invalid_column_gives_nan_row(K, D):
+    rowptr = torch.tensor([0, 2, 4], device=DEV)
+    col = torch.tensor([0, 1, 1, 99], device=DEV)
+    val = torch.ones(4, device=DEV)
+    X = torch.randn(3, D, device=DEV)
+    S = K.calc_W_inv(rowptr, col, val, X[:2].contiguous(), X)
+    assert torch.isfinite(S[0]).all()
+    assert torch.isnan(S[1]).all()
+
+
+# ------------------------------------------------------------------- ind2ptr
+@pytest.mark.parametrize("din,dout", [(torch.int32, torch.int32), (torch.int64, torch.int64),
+                                      (torch.int32, torch.int64)])
+def test_ind2ptr(K, ops, din, dout):
+    row = t(ops["ind2ptr_row"], din)
+    M = int(ops["ind2ptr_M"])
+    out = torch.empty(M + 1, dtype=dout, device=DEV)
+    torch.ops.lakde.ind2ptr_cuda(row, M, out)
+    np.testing.assert_array_equal(out.cpu().numpy(), ops["ind2ptr_out"])
+    empty = K.ind2ptr(torch.zeros(0, dtype=din, device=DEV), 7)
+    assert empty.cpu().tolist() == [0] * 8
+
+
+def test_ind2ptr_large(K):
+    rng = np.random.default_rng(0)
+    row = np.sort(rng.integers(0, 100_000, size=3_000_000))
+    out = K.ind2ptr(t(row), 100_000)
+    np.testing.assert_array_equal(out.cpu().numpy(), O.ind2ptr(row, 100_000))
+
+
+# ---------------------------------------------------------- posterior factor
+@pytest.mark.parametrize("dt", ["f32", "f64"])
+def test_factor_jitter_ladder_golden(K, ops, dt):
+    X = ops[f"chol_{dt}_X"]
+    jit = t(np.zeros(len(X), X.dtype))
+    W, logdet, info, L, _ = K.posterior_factor(t(X), jit, np.finfo(X.dtype).eps, want_L=True)
+    assert (info.cpu().numpy() == 0).all()
+    jit = jit.cpu().numpy()
+    ref = ops[f"chol_{dt}_jitter"]
+    np.testing.assert_array_equal(jit[:4], 0)
+    np.testing.assert_array_equal(jit == 0, ref == 0)
+    eps = np.finfo(X.dtype).eps
+    nz = jit != 0
+    k = np.log2(jit[nz] / eps + 1)
+    np.testing.assert_allclose(k, np.round(k), atol=1e-9)
+    if dt == "f64":
+        assert jit[6] == ref[6]
+    # the factor of the jittered matrix: L L^T reproduces X + jitter I (the
+    # rank-deficient ones only up to rounding), and the full-rank ones match LAPACK
+    Xj = X.astype(np.float64) + np.eye(X.shape[1]) * jit[:, None, None]
+    Lg = L.cpu().numpy().astype(np.float64)
+    recon = Lg @ np.swapaxes(Lg, 1, 2)
+    scale = np.abs(Xj).max(axis=(1, 2))[:, None, None]
+    tol = 64 * np.finfo(X.dtype).eps * X.shape[1]
+    assert (np.abs(recon - Xj) <= tol * scale).all()
+    Lref = np.linalg.cholesky(Xj[:4])
+    np.testing.assert_allclose(Lg[:4], Lref, rtol=1e-4, atol=1e-5 * np.abs(Lref).max())
+
+
+def spd(rng, N, D, cond=1e3):
+    A = rng.standard_normal((N, D, D))
+    Q, _ = np.linalg.qr(A)
+    ev = np.exp(rng.uniform(0, np.log(cond), size=(N, D)))
+    return np.einsum("nij,nj,nkj->nik", Q, ev, Q)
+
+
+@pytest.mark.parametrize("D", [1, 2, 5, 8, 13, 21, 43, 63])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_factor_random(K, D, dtype):
+    rng = np.random.default_rng(D)
+    N = 67
+    S = spd(rng, N, D).astype(dtype)
+    P = spd(rng, N, D).astype(dtype)
+    a = rng.uniform(1, 3, N).astype(dtype)
+    b = rng.uniform(1, 3, N).astype(dtype)
+    nu0 = np.array(D + 1.5, dtype=dtype)
+    Tm = np.tril(rng.standard_normal((N, D, D))).astype(dtype)
+    jit = t(np.zeros(N, dtype))
+    W, logdet, info, L, trace = K.posterior_factor(t(S), jit, np.finfo(dtype).eps, P=t(P), nu_0=t(nu0), a=t(a),
+                                                   b=t(b), T=t(Tm), want_L=True)
+    assert (info.cpu().numpy() == 0).all() and (jit.cpu().numpy() == 0).all()
+    A = (P.astype(np.float64) * (nu0 * (a / b)).astype(np.float64)[:, None, None]) + S
+    Lr = np.linalg.cholesky(A)
+    Ur = np.swapaxes(np.linalg.inv(Lr), 1, 2)
+    rtol = 1e-4 if dtype == np.float32 else 1e-9
+    np.testing.assert_allclose(W.cpu().numpy(), Ur, rtol=rtol, atol=rtol * np.abs(Ur).max())
+    np.testing.assert_allclose(L.cpu().numpy(), Lr, rtol=rtol, atol=rtol * np.abs(Lr).max())
+    np.testing.assert_allclose(logdet.cpu().numpy(), O.chol_logdet(Ur), rtol=rtol, atol=rtol * 10)
+    np.testing.assert_allclose(trace.cpu().numpy(), O.chol_mm_trace(Tm.astype(np.float64), Ur), rtol=10 * rtol)
+
+
+def test_factor_shared_prior_and_failure(K):
+    rng = np.random.default_rng(3)
+    D, N = 6, 10
+    S = spd(rng, N, D)
+    P = spd(rng, 1, D)[0]
+    jit = t(np.zeros(N))
+    W, logdet, info, _, trace = K.posterior_factor(t(S), jit, 2.2e-16, P=t(P), T=t(P))
+    A = S + P
+    Ur = np.swapaxes(np.linalg.inv(np.linalg.cholesky(A)), 1, 2)
+    np.testing.assert_allclose(W.cpu().numpy(), Ur, rtol=1e-9, atol=1e-12)
+    # a matrix no ladder rung repairs: info = -1 and NaN outputs
+    bad = -np.eye(D)[None].repeat(2, 0) * 1e3
+    jit = t(np.zeros(2))
+    W, logdet, info, _, _ = K.posterior_factor(t(bad), jit, 2.2e-16)
+    assert (info.cpu().numpy() == -1).all()
+    assert torch.isnan(W).all() and torch.isnan(logdet).all()
+
+
+# ----------------------------------------------------------- sparse E-step
+def small_problem(rng, N=300, D=5, K=12, dtype=np.float32):
+    X = rng.standard_normal((N, D)).astype(dtype)
+    graph = O.knn_graph(X, K)
+    (pat,) = O.knn_pattern(graph)
+    rows, cols = pat
+    rowptr = O.ind2ptr(rows, N)
+    W = rand_upper(rng, N, D, dtype) * 2
+    nu = rng.uniform(D + 1, D + 10, N).astype(dtype)
+    logdet = O.chol_logdet(W).astype(dtype)
+    return X, rowptr, cols, W, nu, logdet
+
+
+@pytest.mark.parametrize("D", [2, 5, 21])
+def test_estep_logrho_and_normalise(K, D):
+    rng = np.random.default_rng(D)
+    X, rowptr, cols, W, nu, logdet = small_problem(rng, D=D)
+    N = len(X)
+    lr = K.estep_logrho(t(rowptr), t(cols, torch.int32), t(X), t(W), t(nu), t(logdet)).cpu().numpy()
+    ref = O.sparse_log_rho(rowptr, cols, X, W, nu, logdet)
+    np.testing.assert_allclose(lr, ref, rtol=1e-4, atol=1e-4 * np.abs(ref).max())
+    # point-major view
+    order = np.argsort(cols, kind="stable")
+    cptr = O.ind2ptr(cols[order], N)
+    c0 = np.full(N, -np.inf, np.float32)
+    rs0 = np.zeros(N, np.float32)
+    for mode, thr in ((0, 0.0), (1, 1e-3)):
+        lr_t = t(ref)
+        r = torch.zeros_like(lr_t)
+        c = t(c0.copy())
+        rs = t(rs0.copy())
+        K.estep_normalise(t(cptr), t(order), lr_t, r, c, rs, mode, thr)
+        r_ref, c_ref, rs_ref = O.sparse_normalise(cols, ref, c0, rs0, N, mode, thr)
+        np.testing.assert_allclose(r.cpu().numpy(), r_ref, rtol=1e-5, atol=1e-7)
+        np.testing.assert_allclose(c.cpu().numpy(), c_ref, rtol=1e-6, atol=1e-5)
+        np.testing.assert_allclose(rs.cpu().numpy(), rs_ref, rtol=1e-5)
+        c0, rs0 = c_ref, rs_ref
+
+
+def test_estep_self_pairs_are_excluded(K):
+    rng = np.random.default_rng(9)
+    X = rng.standard_normal((50, 3)).astype(np.float32)
+    graph = O.knn_graph(X, 5, include_self=True)
+    ((rows, cols),) = O.knn_pattern(graph)
+    W = rand_upper(rng, 50, 3, np.float32)
+    nu = np.full(50, 6, np.float32)
+    logdet = O.chol_logdet(W).astype(np.float32)
+    lr = K.estep_logrho(t(O.ind2ptr(rows, 50)), t(cols), t(X), t(W), t(nu), t(logdet)).cpu().numpy()
+    assert np.all(np.isneginf(lr[rows == cols]))
+    assert np.all(np.isfinite(lr[rows != cols]))
+
+
+# ---------------------------------------------------------- predictive density
+@pytest.mark.parametrize("D", [2, 8, 21, 43, 63])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_log_pred_density(K, D, dtype):
+    rng = np.random.default_rng(D)
+    N, Nq = 1500, 700
+    X = rng.standard_normal((N, D)).astype(dtype)
+    Y = rng.standard_normal((Nq, D)).astype(dtype)
+    W = (rand_upper(rng, N, D, dtype) / np.sqrt(D)).astype(dtype)
+    nu = rng.uniform(D + 1, D + 30, N).astype(dtype)
+    logdet = O.chol_logdet(W).astype(dtype)
+    lc = K.pred_coeff(t(nu), t(logdet), D)
+    out = K.log_pred_density(t(X), t(W), t(nu), lc, t(Y)).cpu().numpy()
+    ref = O.log_pred_density_from_factors(X.astype(np.float64), Y.astype(np.float64), W.astype(np.float64),
+                                          nu.astype(np.float64), logdet.astype(np.float64))
+    atol = 2e-4 if dtype == np.float32 else 1e-9
+    np.testing.assert_allclose(out, ref, rtol=0, atol=atol * max(1, D / 8))
