@@ -1,0 +1,446 @@
+"""Benchmark of the lakde VI hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload gas8|bsds63|...]
+                    [--impl reference]
+
+A step is one VI iteration of LocalKNearestKDE over all N kernels (fused
+batch schedule on the kNN candidate pattern), on seeded synthetic data with
+the shape of the named workload.  Inputs are resident in HBM; L2 is flushed
+between timed steps.  Rank 0 prints one JSON line with the whole-job
+throughput, the roofline of the dominant kernel, the end-to-end number
+through the public API with host buffers, the CPU baseline (the oracle port
+timed on a bounded sample) and the SM clocks sampled during the timed region.
+Under torchrun (N > 1) each rank runs an independent replica.
+"""
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "VI iters/s and log_pred_density pts/s, mixed vs plain FP32 GPU at ≤1e-3 nats"
+
+WORKLOADS = {
+    # name: (generator kwargs, K, threshold, description)
+    "gas8": (dict(n_train=200_000, n_test=20_000), 50, 5e-4,
+             "LocalKNearestKDE d=8 N_train=200000 N_test=20000 K=50 (10-component heavy-tail mixture)"),
+    "bsds63": (dict(n_train=1_000_000, n_test=16_384), 100, 5e-4,
+               "LocalKNearestKDE d=63 N_train=1000000 N_test=16384 K=100 (20-component decaying-spectrum mixture)"),
+    "spec21": (dict(n_train=300_000, n_test=4_096), 64, 5e-4,
+               "LocalKNearestKDE d=21 N_train=300000 N_test=4096 K=64 (12-component mixture)"),
+    "circle2d": (dict(n_train=2_000, n_test=1_000), 20, 0.0,
+                 "LocalKNearestKDE d=2 N_train=2000 N_test=1000 K=20 (8-Gaussian circle)"),
+}
+
+
+def make_data(name):
+    from lakde_b200 import synthetic as syn
+
+    kw, k, thr, desc = WORKLOADS[name]
+    gen = {"gas8": syn.heavy_tail_mixture, "bsds63": syn.decaying_spectrum_mixture,
+           "spec21": syn.wide_spectrum_mixture, "circle2d": syn.circle_gmm}[name]
+    Xtr, Xte = gen(seed=0, **kw)
+    return Xtr, Xte, k, thr, desc
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic(kernel, workload):
+    """Per-launch DRAM bytes of `kernel` from a committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    v = d.get(workload, {}).get(kernel)
+    return None if v is None else float(v)
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def wait_for_samples(self, n, timeout_s, keep_busy):
+        """Keeps the GPU busy until the sampler has produced n samples."""
+        t0 = time.perf_counter()
+        while len(self.samples) < n and time.perf_counter() - t0 < timeout_s:
+            keep_busy()
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 8:
+                self.samples.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for s in self.samples for n, v in zip(names, s[4:8]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def alg_bytes(N, D, nnz, es=4):
+    """Compulsory bytes per launch of the four kernels of one iteration."""
+    T = D * D
+    return {
+        "mstep": 8 * (N + 1) + 4 * nnz + es * nnz + es * N * D + es * N * T + es * N,
+        "posterior_factor": 3 * es * N * T + es * N * T + 3 * es * N + 4 * es * N + 4 * N,
+        "estep_logrho": 8 * (N + 1) + 4 * nnz + es * N * D + es * N * T + 2 * es * N + es * nnz,
+        "estep_normalise": 8 * (N + 1) + 4 * nnz + es * nnz + es * nnz + 4 * es * N,
+    }
+
+
+def timed_steps(eng, steps, flush, torch):
+    """Times each fused iteration with CUDA events (L2 flushed before each),
+    and within it the M-step, the factorisation and the E-step."""
+    stream = torch.cuda.current_stream()
+    parts = {"mstep": 0.0, "posterior_factor": 0.0, "estep": 0.0, "updates": 0.0}
+    total = 0.0
+    for _ in range(steps):
+        flush.zero_()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+        ev[0].record(stream)
+        eng.mstep()
+        ev[1].record(stream)
+        eng.factor()
+        ev[2].record(stream)
+        eng.estep(mode=1)
+        ev[3].record(stream)
+        torch.mul(eng.nu, eng.trace, out=eng.sigma_0_lambda_mm_trace)
+        torch.add(eng.sigma_0_lambda_mm_trace * (eng.nu_0 / 2), eng.b_0, out=eng.b)
+        ev[4].record(stream)
+        torch.cuda.synchronize()
+        for i, name in enumerate(parts):
+            parts[name] += ev[i].elapsed_time(ev[i + 1])
+        total += ev[0].elapsed_time(ev[4])
+    return total, parts
+
+
+def split_estep(eng, reps, flush, torch):
+    """Average durations of the two E-step kernels, timed separately."""
+    from lakde_b200 import kernels as K
+
+    stream = torch.cuda.current_stream()
+    t_lr = t_nm = 0.0
+    for _ in range(reps):
+        flush.zero_()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        rowptr, col = eng._tri()
+        e[0].record(stream)
+        K.estep_logrho(rowptr, col, eng.X, eng.U, eng.nu, eng.logdet_W, out=eng.logrho)
+        e[1].record(stream)
+        K.estep_normalise(eng.pattern.cptr, eng.pattern.pos, eng.logrho, eng.r, eng.c, eng.rsum, 1, eng.threshold)
+        e[2].record(stream)
+        torch.cuda.synchronize()
+        t_lr += e[0].elapsed_time(e[1])
+        t_nm += e[1].elapsed_time(e[2])
+    return t_lr / reps, t_nm / reps
+
+
+def cpu_baseline(Xtr, graph, k, thr, budget_s=20.0):
+    """The reference algorithm (oracle port, numpy) timed on a bounded sample:
+    one partial step (kernel block of 512, dense E-step against every point)
+    of the block schedule, extrapolated to one VI iteration over all blocks."""
+    from oracle import lakde_oracle as O
+
+    N, D = Xtr.shape
+    B = 512
+    m = O.KNNKDEOracle(k=graph.astype(np.int64), block_size=B)
+    m.init_parameters_(Xtr, thr)
+    # state after initialisation without the two dense initial epochs (they do
+    # not change the cost of a step): unit normalisers and the prior posterior
+    m.rnm_log_consts[:] = 0.0
+    m.nu[:] = float(m.nu_0)
+    m.logdet_W[:] = 0.0
+    m.logdet_sigma_0[:] = 0.0
+    m.sigma_0_lambda_mm_trace[:] = 1.0
+    t0 = time.perf_counter()
+    steps = 0
+    while True:
+        m.partial_step_(Xtr, steps % ((N - 1) // B + 1), thr)
+        steps += 1
+        if time.perf_counter() - t0 > budget_s or steps >= 2:
+            break
+    per_step = (time.perf_counter() - t0) / steps
+    n_blocks = (N - 1) // B + 1
+    iters_per_s = 1.0 / (per_step * n_blocks)
+    return {
+        "value": iters_per_s,
+        "unit": "VI iters/s",
+        "cores": os.cpu_count(),
+        "kind": "port",
+        "sample": f"{steps} partial step(s) of the block schedule (block 512 of {N} kernels, dense E-step over all "
+                  f"{N} points, numpy oracle) at {per_step:.2f} s each, extrapolated x{n_blocks} blocks",
+    }
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    Xtr, Xte, k, thr, desc = make_data(args.workload)
+    from oracle import lakde_oracle as O
+
+    # kNN graph for the sample: exact ranks of the first block's neighbourhoods only
+    N = len(Xtr)
+    graph = np.empty((N, k), dtype=np.int64)
+    rng = np.random.default_rng(0)
+    # the sampled steps read the graph rows of their own blocks only; other rows
+    # get random neighbours (they do not enter the timed work)
+    graph[:] = rng.integers(0, N, size=(N, k))
+    graph[:1024] = O.knn_graph(Xtr, k)[:1024] if N <= 1024 else _block_knn(Xtr, k, 1024)
+    # each timed step is one bounded sample (about 10-30 s); stop after ~90 s
+    vals = []
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.steps)):
+        vals.append(cpu_baseline(Xtr, graph, k, thr, budget_s=5.0))
+        if time.perf_counter() - t0 > 90.0:
+            break
+    v = statistics.median([x["value"] for x in vals])
+    cb = dict(vals[-1])
+    cb["value"] = v
+    args.steps = len(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "VI iters/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{args.workload}: {desc}", "schedule": "block_size=512, dense E-step"},
+        "cpu_baseline": cb,
+        "e2e": {"value": v, "unit": "VI iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _block_knn(X, k, rows):
+    X64 = X.astype(np.float64)
+    out = np.empty((rows, k), dtype=np.int64)
+    for s in range(0, rows, 256):
+        d = ((X64[s:s + 256, None, :] - X64[None]) ** 2).sum(-1)
+        d[np.arange(min(256, rows - s)), s + np.arange(min(256, rows - s))] = np.inf
+        part = np.argpartition(d, k, axis=1)[:, :k]
+        dd = np.take_along_axis(d, part, 1)
+        out[s:s + 256] = np.take_along_axis(part, np.argsort(dd, axis=1, kind="stable"), 1)
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="gas8", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=dev)
+
+    from lakde_b200 import LocalKNearestKDE
+
+    Xtr, Xte, k, thr, desc = make_data(args.workload)
+    X = torch.tensor(Xtr, device=dev)
+    Y = torch.tensor(Xte, device=dev)
+    model = LocalKNearestKDE(k_or_knn_graph=k, fused=True, cuda_graph=False)
+    t_init = time.perf_counter()
+    model.fit(X, iterations=0, sparsity_threshold=thr)
+    torch.cuda.synchronize()
+    t_init = time.perf_counter() - t_init
+    eng = model.engine
+    N, D = X.shape
+    nnz = eng.pattern.nnz
+    for _ in range(args.warmup):
+        eng.step()
+    torch.cuda.synchronize()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local).__enter__()
+
+    def busy():
+        for _ in range(20):
+            eng.step()
+        torch.cuda.synchronize()
+
+    clocks.wait_for_samples(3, 20.0, busy)
+    n_before = len(clocks.samples)
+    total_ms, per_kernel = timed_steps(eng, args.steps, flush, torch)
+    torch.cuda.synchronize()
+    clocks.wait_for_samples(n_before + 2, 20.0, busy)
+    clocks.__exit__(None, None, None)
+    t_lr, t_nm = split_estep(eng, max(3, args.steps // 2), flush, torch)
+    ms_per_step = total_ms / args.steps
+    if world > 1:
+        t = torch.tensor([ms_per_step], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_per_step = float(t)
+    value = world * 1000.0 / ms_per_step
+
+    # per-kernel average durations and the roofline of the dominant one
+    durations = {
+        "mstep": per_kernel["mstep"] / args.steps,
+        "posterior_factor": per_kernel["posterior_factor"] / args.steps,
+        "estep_logrho": t_lr,
+        "estep_normalise": t_nm,
+    }
+    dom = max(durations, key=durations.get)
+    ab = alg_bytes(N, D, nnz)
+    peak, peak_kind = load_peaks()
+    achieved = ab[dom] / (durations[dom] * 1e-3) / 1e9
+    traffic = load_traffic(dom, args.workload)
+
+    # log_pred_density throughput (queries resident in HBM)
+    for _ in range(2):
+        model.log_pred_density(X, Y)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lpd_reps = 3
+    e0.record()
+    for _ in range(lpd_reps):
+        lpd = model.log_pred_density(X, Y)
+    e1.record()
+    torch.cuda.synchronize()
+    lpd_ms = e0.elapsed_time(e1) / lpd_reps
+    lpd_pts = len(Xte) / (lpd_ms * 1e-3)
+
+    # end to end through the public API with host buffers: pinned X -> device,
+    # one partial_step_, ELBO read back to the host
+    Xh = torch.tensor(Xtr).pin_memory()
+    Xd = torch.empty_like(X)
+    torch.cuda.synchronize()
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        Xd.copy_(Xh, non_blocking=True)
+        eng.X = Xd
+        model.partial_step_(Xd, 0, sparsity_threshold=thr)
+        elbo = float(model.compute_elbo(Xd))
+        b.record()
+        torch.cuda.synchronize()
+        e2e_ms += a.elapsed_time(b)
+    eng.X = X
+    e2e_ms /= args.steps
+    model.check_errors_()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(Xtr, model.knn_graph.cpu().numpy(), k, thr)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "VI iters/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_per_step,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "precision": "fp32 (plain FP32 GPU kernels; FP64 factorisations)",
+            "config": {
+                "workload": f"{args.workload}: {desc}",
+                "schedule": "fused batch VI (block_size=N) on the kNN candidate pattern",
+                "nnz_pairs": nnz,
+                "sparsity_threshold": thr,
+                "l2": "flushed (256 MB write) before every timed step",
+                "parallelism": f"{world} independent replica(s)" if world > 1 else "single GPU",
+                "init_s": round(t_init, 3),
+            },
+            "roofline": {
+                "kernel": dom,
+                "bound": "hbm",
+                "achieved": achieved,
+                "peak": peak,
+                "unit": "GB/s",
+                "frac": achieved / peak,
+                "traffic": traffic,
+                "peak_source": f"{peak_kind} hbm_gbs",
+                "alg_bytes_per_launch": ab[dom],
+                "kernel_ms": {k_: round(v, 5) for k_, v in durations.items()},
+            },
+            "log_pred_density": {"value": lpd_pts, "unit": "pts/s", "ms": lpd_ms, "queries": len(Xte),
+                                 "kernels": N, "mean_log_density": float(lpd.mean())},
+            "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "VI iters/s", "h2d_bytes_per_step": X.numel() * 4,
+                    "d2h_bytes_per_step": 8, "elbo": elbo},
+            "gpu_launches": 4 * args.steps,
+            "clocks": clocks.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

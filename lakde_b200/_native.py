@@ -34,6 +34,11 @@ _SIGNATURES = {
         [_c_int, _c_vp, _c_int, _c_vp, _c_int, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64, _c_i64, _c_i64, _c_vp],
         _c_int,
     ),
+    "lakde_mstep": (
+        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_int, _c_vp, _c_int, _c_vp, _c_vp, _c_i64, _c_dbl, _c_vp, _c_vp,
+         _c_vp],
+        _c_int,
+    ),
     "lakde_posterior_factor": (
         [_c_int, _c_i64, _c_i64, _c_vp, _c_vp, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_vp, _c_vp,
          _c_vp, _c_vp, _c_vp, _c_i64, _c_vp, _c_vp],

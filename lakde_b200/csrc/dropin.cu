@@ -94,7 +94,7 @@ template <typename T, typename RP, typename CI, int DP>
 __global__ void __launch_bounds__(256) scatter_cov_warp(const RP *__restrict__ rowptr, const CI *__restrict__ col,
                                                         const T *__restrict__ val, const T *__restrict__ Xn,
                                                         const T *__restrict__ Xm, T *__restrict__ out, int64_t N,
-                                                        int64_t M, int D) {
+                                                        int64_t M, int D, T *__restrict__ nu_out, T nu0) {
   constexpr int TT = DP * (DP + 1) / 2;
   constexpr int KE = (TT + 31) / 32;
   __shared__ T sd[8][32][DP + 1];
@@ -120,6 +120,7 @@ __global__ void __launch_bounds__(256) scatter_cov_warp(const RP *__restrict__ r
   T acc[KE];
 #pragma unroll
   for (int k = 0; k < KE; ++k) acc[k] = T(0);
+  T vsum = T(0);
 
   for (int64_t base = start; base < end; base += 32) {
     const int64_t p = base + lane;
@@ -135,6 +136,7 @@ __global__ void __launch_bounds__(256) scatter_cov_warp(const RP *__restrict__ r
     for (int d = 0; d < DP; ++d)
       sd[warp][lane][d] = (valid && d < D) ? Xm[c * D + d] - Xn[row * D + d] : T(0);
     sv[warp][lane] = v;
+    vsum += v;
     __syncwarp();
     const int cnt = (int)((end - base) < 32 ? (end - base) : 32);
     for (int q = 0; q < cnt; ++q) {
@@ -151,6 +153,10 @@ __global__ void __launch_bounds__(256) scatter_cov_warp(const RP *__restrict__ r
     __syncwarp();
   }
   bad = __any_sync(0xffffffffu, bad);
+  if (nu_out) {
+    vsum = warp_sum(vsum);
+    if (lane == 0) nu_out[row] = bad ? T(NAN) : nu0 + vsum;
+  }
   T *o = out + row * (int64_t)D * D;
 #pragma unroll
   for (int k = 0; k < KE; ++k) {
@@ -182,7 +188,8 @@ struct CtaScatterCfg {
 template <typename T, typename RP, typename CI, int DP>
 __global__ void scatter_cov_cta(const RP *__restrict__ rowptr, const CI *__restrict__ col,
                                 const T *__restrict__ val, const T *__restrict__ Xn, const T *__restrict__ Xm,
-                                T *__restrict__ out, int64_t N, int64_t M, int D) {
+                                T *__restrict__ out, int64_t N, int64_t M, int D, T *__restrict__ nu_out,
+                                T nu0) {
   using C = CtaScatterCfg<T, DP>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *sd = reinterpret_cast<T *>(smem_raw);
@@ -215,6 +222,7 @@ __global__ void scatter_cov_cta(const RP *__restrict__ rowptr, const CI *__restr
 #pragma unroll
     for (int q = 0; q < 4; ++q) acc[p][q] = T(0);
 
+  T vsum = T(0);  // row sum of the weights, accumulated by thread 0
   for (int64_t base = start; base < end; base += C::CH) {
     const int cnt = (int)((end - base) < C::CH ? (end - base) : C::CH);
     for (int pp = tid; pp < C::CH; pp += blockDim.x) {
@@ -233,6 +241,8 @@ __global__ void scatter_cov_cta(const RP *__restrict__ rowptr, const CI *__restr
       sv[pp] = v;
     }
     __syncthreads();
+    if (tid == 0)
+      for (int pp = 0; pp < cnt; ++pp) vsum += sv[pp];
     for (int e = tid; e < C::CH * DP; e += blockDim.x) {
       const int pp = e / DP, d = e % DP;
       sd[pp * C::LD + d] = (pp < cnt && d < D) ? Xm[sc[pp] * D + d] - sxn[d] : T(0);
@@ -256,6 +266,7 @@ __global__ void scatter_cov_cta(const RP *__restrict__ rowptr, const CI *__restr
     __syncthreads();
   }
   __syncthreads();
+  if (nu_out && tid == 0) nu_out[row] = s_bad ? T(NAN) : nu0 + vsum;
   if (bi < 0) return;
   const bool bad = s_bad != 0;
   T *o = out + row * (int64_t)D * D;
@@ -348,24 +359,24 @@ extern "C" int lakde_chol_quad_form(int dtype, const void *W_triu, const int64_t
   });
 }
 
-extern "C" int lakde_W_inv(int dtype, const void *rowptr, int rowptr_dtype, const void *col, int col_dtype,
-                           const void *value, const void *Xn, const void *Xm, void *out, int64_t N, int64_t M,
-                           int64_t D, void *stream) {
+static int scatter_cov_launch(const char *what, int dtype, const void *rowptr, int rowptr_dtype, const void *col,
+                              int col_dtype, const void *value, const void *Xn, const void *Xm, void *out, int64_t N,
+                              int64_t M, int64_t D, void *nu_out, double nu0, void *stream) {
   clear_error();
   if (N < 0 || M < 0 || D < 1) {
-    set_error("W_inv: invalid sizes (N=%lld, M=%lld, D=%lld)", (long long)N, (long long)M, (long long)D);
+    set_error("%s: invalid sizes (N=%lld, M=%lld, D=%lld)", what, (long long)N, (long long)M, (long long)D);
     return LAKDE_EINVAL;
   }
   if (N == 0) return LAKDE_OK;
   if (N > 0x7fffffffLL) {
-    set_error("W_inv: N=%lld exceeds the grid limit", (long long)N);
+    set_error("%s: N=%lld exceeds the grid limit", what, (long long)N);
     return LAKDE_EUNSUPPORTED;
   }
   if (!rowptr || !out || !Xn || (M > 0 && !Xm)) {
-    set_error("W_inv: null pointer");
+    set_error("%s: null pointer", what);
     return LAKDE_EINVAL;
   }
-  if (int st = bind_device("W_inv", {out, rowptr, col, value, Xn, Xm})) return st;
+  if (int st = bind_device(what, {out, rowptr, col, value, Xn, Xm, nu_out})) return st;
   return dispatch_float(dtype, [&](auto t0) {
     using T = decltype(t0);
     return dispatch_index(rowptr_dtype, [&](auto r0) {
@@ -382,18 +393,41 @@ extern "C" int lakde_W_inv(int dtype, const void *rowptr, int rowptr_dtype, cons
           auto op = static_cast<T *>(out);
           if constexpr (DP <= 16) {
             const int64_t blocks = (N + 7) / 8;
-            scatter_cov_warp<T, RP, CI, DP><<<(unsigned)blocks, 256, 0, as_stream(stream)>>>(rp, cp, vp, xn, xm,
-                                                                                               op, N, M, (int)D);
+            scatter_cov_warp<T, RP, CI, DP><<<(unsigned)blocks, 256, 0, as_stream(stream)>>>(
+                rp, cp, vp, xn, xm, op, N, M, (int)D, static_cast<T *>(nu_out), (T)nu0);
           } else {
             using C = CtaScatterCfg<T, DP>;
             auto kern = scatter_cov_cta<T, RP, CI, DP>;
             int st = set_smem(kern, C::smem);
             if (st) return st;
-            kern<<<(unsigned)N, C::THREADS, C::smem, as_stream(stream)>>>(rp, cp, vp, xn, xm, op, N, M, (int)D);
+            kern<<<(unsigned)N, C::THREADS, C::smem, as_stream(stream)>>>(rp, cp, vp, xn, xm, op, N, M, (int)D,
+                                                                          static_cast<T *>(nu_out), (T)nu0);
           }
-          return check_launch("W_inv");
+          return check_launch(what);
         });
       });
     });
   });
+}
+
+extern "C" int lakde_W_inv(int dtype, const void *rowptr, int rowptr_dtype, const void *col, int col_dtype,
+                           const void *value, const void *Xn, const void *Xm, void *out, int64_t N, int64_t M,
+                           int64_t D, void *stream) {
+  return scatter_cov_launch("W_inv", dtype, rowptr, rowptr_dtype, col, col_dtype, value, Xn, Xm, out, N, M, D,
+                            nullptr, 0.0, stream);
+}
+
+extern "C" int lakde_mstep(int dtype, int64_t N, int64_t D, int64_t npts, const void *rowptr, int rowptr_dtype,
+                           const void *col, int col_dtype, const void *r, const void *X, int64_t kernel_offset,
+                           double nu_0, void *S, void *nu, void *stream) {
+  if (kernel_offset < 0 || kernel_offset + N > npts) {
+    clear_error();
+    set_error("mstep: kernel rows [%lld, %lld) outside the %lld points", (long long)kernel_offset,
+              (long long)(kernel_offset + N), (long long)npts);
+    return LAKDE_EINVAL;
+  }
+  const size_t es = dtype == LAKDE_F64 ? 8 : 4;
+  const void *Xn = X ? static_cast<const char *>(X) + (size_t)kernel_offset * (size_t)D * es : nullptr;
+  return scatter_cov_launch("mstep", dtype, rowptr, rowptr_dtype, col, col_dtype, r, Xn, X, S, N, npts, D, nu, nu_0,
+                            stream);
 }

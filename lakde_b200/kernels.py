@@ -158,21 +158,43 @@ def chol_quad_form(W_triu, Xn, Xm):
 # --------------------------------------------------------------------------
 
 
-def posterior_factor(S, jitter, eps, P=None, nu_0=None, a=None, b=None, T=None, want_L=False, info=None, out=None):
+def mstep(rowptr, col, r, X, nu_0, kernel_offset=0, S=None, nu=None):
+    """Scatter covariance S and nu = nu_0 + row sums of r for kernels kernel_offset.. of X."""
+    nat.require_cuda(rowptr, col, r, X, op="mstep")
+    N = rowptr.numel() - 1
+    D = X.size(1)
+    S = X.new_empty(N, D, D) if S is None else S
+    nu = X.new_empty(N) if nu is None else nu
+    nat.check(
+        nat.lib().lakde_mstep(
+            nat.dtype_code(X), N, D, X.size(0), nat.ptr(rowptr), nat.dtype_code(rowptr), nat.ptr(col),
+            nat.dtype_code(col), nat.ptr(r), nat.ptr(X), kernel_offset, float(nu_0), nat.ptr(S), nat.ptr(nu),
+            nat.stream_of(X),
+        ),
+        "mstep",
+    )
+    return S, nu
+
+
+def posterior_factor(S, jitter, eps, P=None, nu_0=None, a=None, b=None, T=None, want_L=False, info=None, out=None,
+                     logdet=None, trace=None, L=None):
     """FP64 jittered Cholesky of A_n = nu_0 a_n / b_n P_n + S_n (see include/lakde_b200.h).
 
     Returns (W_triu, logdet_W, info, L or None, trace or None); ``jitter`` is
     updated in place.  ``P`` and ``T`` may be [D, D] (shared) or [N, D, D].
+    Output buffers may be passed in (out, logdet, info, trace, L).
     """
     nat.require_cuda(S, jitter, P, nu_0, a, b, T, op="posterior_factor")
     N, D, _ = S.shape
     S = S.contiguous()
     dt = S.dtype
     W = torch.empty_like(S) if out is None else out
-    logdet = S.new_empty(N)
+    logdet = S.new_empty(N) if logdet is None else logdet
     info = S.new_empty(N, dtype=torch.int32) if info is None else info
-    L = torch.empty_like(S) if want_L else None
-    trace = S.new_empty(N) if T is not None else None
+    if L is None and want_L:
+        L = torch.empty_like(S)
+    if T is not None and trace is None:
+        trace = S.new_empty(N)
 
     def batch(M):
         if M is None:
