@@ -272,7 +272,6 @@ class FusedHier(FusedVI):
 
     def step(self):
         """lakde/local_hierarchical_kde.py:273-332 at block_size = N."""
-        self._refresh_prior()
         self.mstep()
         self.factor()
         self.estep(mode=1)
@@ -284,6 +283,9 @@ class FusedHier(FusedVI):
                                                  torch.finfo(torch.float64).eps)
         torch.minimum(self.failed, info.min(), out=self.failed)
         self.W_shared_triu.copy_(W_sh[0])
+        # E[Sigma_bar] follows the shared factor at once, so the next step and
+        # log_pred_density both see the current prior
+        self._refresh_prior()
 
     def compute_elbo(self):
         """lakde/local_hierarchical_kde.py:334-461 (terms :25-79), reduced in float64."""
