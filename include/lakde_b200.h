@@ -129,6 +129,19 @@ LAKDE_API int lakde_posterior_factor(int dtype, int64_t N, int64_t D, const void
                            int64_t T_batch_stride, void *trace, void *stream);
 
 /*
+ * Fused-path M-step: the scatter covariance of lakde_W_inv for kernels
+ * n = kernel_offset .. kernel_offset + N - 1 of X (Xn = X[kernel_offset:]) and
+ * nu_n = nu_0 + sum_{p in row n} r[p] in the same pass.  Restates
+ * lakde/local_adaptive_kde.py:66-81 (calc_posterior_contribs).
+ * rowptr [N+1], col [nnz] (I32/I64), r [nnz], X [npts,D], S [N,D,D], nu [N].
+ */
+LAKDE_API int lakde_mstep(int dtype, int64_t N, int64_t D, int64_t npts,
+                          const void *rowptr, int rowptr_dtype, const void *col,
+                          int col_dtype, const void *r, const void *X,
+                          int64_t kernel_offset, double nu_0, void *S, void *nu,
+                          void *stream);
+
+/*
  * Sparse-pair E-step numerators.  For kernel n in [0, N) and every pair p of
  * its CSR row (rowptr over the N kernels, col = point index into X[npts,D]):
  *   logrho[p] = 0.5 (mvdigamma(nu_n / 2, D) + D log 2 + logdet_W_n)
@@ -183,6 +196,27 @@ LAKDE_API int lakde_log_pred_density(int dtype, int64_t N, int64_t Nq, int64_t D
                            const void *log_coeff, const void *Y, void *out,
                            void *workspace, size_t workspace_bytes,
                            void *stream);
+
+/*
+ * lakde_log_pred_density without any device allocation.  This entry point has
+ * no counterpart in the reference.  It is for callers that cannot call
+ * cudaMalloc: hosts that own all device memory themselves (a framework's
+ * caching allocator, a plugin sandbox) or that forbid device allocation once
+ * they are running.  Same arguments and result as lakde_log_pred_density
+ * minus the workspace, which comes from a 16 MiB array built into the library
+ * (each GPU that loads the library holds it until the process exits).  Calls
+ * that would need more than 16 MiB of scratch (see
+ * lakde_log_pred_density_workspace) are rejected with LAKDE_EINVAL; split the
+ * queries.  The first call on each device looks up the array's device address
+ * with that device current; make that first call before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race on it.
+ */
+LAKDE_API int lakde_log_pred_density_noalloc(int dtype, int64_t N, int64_t Nq,
+                                             int64_t D, const void *X,
+                                             const void *W_triu, const void *nu,
+                                             const void *log_coeff,
+                                             const void *Y, void *out,
+                                             void *stream);
 
 #ifdef __cplusplus
 }

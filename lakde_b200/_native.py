@@ -55,6 +55,10 @@ _SIGNATURES = {
     ),
     "lakde_pred_coeff": ([_c_int, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
     "lakde_log_pred_density_workspace": ([_c_int, _c_i64, _c_i64, _c_i64], ctypes.c_size_t),
+    "lakde_log_pred_density_noalloc": (
+        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
+        _c_int,
+    ),
     "lakde_log_pred_density": (
         [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, ctypes.c_size_t, _c_vp],
         _c_int,

@@ -3,6 +3,8 @@
 // online logsumexp.  The kernel axis is split into chunks so the grid fills the
 // 148 SMs; each (query tile, chunk) CTA leaves a (max, sum) pair per query in a
 // caller-provided workspace and a second pass folds the chunks.
+#include <mutex>
+
 #include "common.cuh"
 
 namespace lakde {
@@ -211,6 +213,108 @@ extern "C" int lakde_log_pred_density(int dtype, int64_t N, int64_t Nq, int64_t 
       pred_combine_kernel<T><<<(unsigned)((Nq + 255) / 256), 256, 0, as_stream(stream)>>>(
           ws_m, ws_s, static_cast<T *>(out), Nq, nchunks, (T)log((double)N));
       return check_launch("log_pred_density_combine");
+    });
+  });
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant.  Some callers cannot call cudaMalloc: hosts that own
+// all device memory themselves (a framework's caching allocator, a plugin
+// sandbox) or that forbid device allocation once they are running.  For them
+// the (max, sum) partials live in this file-scope device array instead of a
+// caller workspace.  It is 16 MiB; every GPU that loads the library holds it
+// until the process exits.  All calls share it, and it keeps the contents of the
+// last call: every slot a call reads is written earlier in that same call, so
+// nothing needs clearing, but calls that overlap on the GPU (concurrent
+// streams, or several host threads) race on it.
+// ---------------------------------------------------------------------------
+namespace lakde {
+
+constexpr size_t kNoAllocScratchBytes = 16u << 20;
+static __device__ __align__(256) unsigned char g_pred_scratch[kNoAllocScratchBytes];
+
+// Device address of g_pred_scratch per device, resolved on the first call that
+// runs on that device (with the device current).
+static void *g_pred_scratch_ptr[128];
+static std::mutex g_pred_scratch_mu;
+
+static int pred_scratch_address(void **out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 128) {
+    set_error("log_pred_density_noalloc: cudaGetDevice failed: %s", cudaGetErrorString(e));
+    return LAKDE_ECUDA;
+  }
+  std::lock_guard<std::mutex> lock(g_pred_scratch_mu);
+  if (!g_pred_scratch_ptr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_pred_scratch);
+    if (e != cudaSuccess || !p) {
+      set_error("log_pred_density_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+      return LAKDE_ECUDA;
+    }
+    g_pred_scratch_ptr[dev] = p;
+  }
+  *out = g_pred_scratch_ptr[dev];
+  return LAKDE_OK;
+}
+
+}  // namespace lakde
+
+extern "C" int lakde_log_pred_density_noalloc(int dtype, int64_t N, int64_t Nq, int64_t D, const void *X,
+                                              const void *W_triu, const void *nu, const void *log_coeff,
+                                              const void *Y, void *out, void *stream) {
+  clear_error();
+  if (N < 1 || Nq < 0 || D < 1) {
+    set_error("log_pred_density_noalloc: invalid sizes (N=%lld, Nq=%lld, D=%lld)", (long long)N, (long long)Nq,
+              (long long)D);
+    return LAKDE_EINVAL;
+  }
+  if (Nq == 0) return LAKDE_OK;
+  const size_t need = lakde_log_pred_density_workspace(dtype, N, Nq, D);
+  if (need == 0) {
+    set_error("log_pred_density_noalloc: unsupported dtype %d or D=%lld", dtype, (long long)D);
+    return LAKDE_EUNSUPPORTED;
+  }
+  if (need > kNoAllocScratchBytes) {
+    set_error("log_pred_density_noalloc: %lld queries x %lld kernels need %zu bytes of scratch, more than the "
+              "built-in %zu bytes; split the queries into smaller batches",
+              (long long)Nq, (long long)N, need, kNoAllocScratchBytes);
+    return LAKDE_EINVAL;
+  }
+  if (!X || !W_triu || !nu || !log_coeff || !Y || !out) {
+    set_error("log_pred_density_noalloc: null pointer");
+    return LAKDE_EINVAL;
+  }
+  if (int st = bind_device("log_pred_density_noalloc", {out, X, W_triu, nu, log_coeff, Y})) return st;
+  void *scratch = nullptr;
+  if (int st = pred_scratch_address(&scratch)) return st;
+  return dispatch_float(dtype, [&](auto t0) {
+    using T = decltype(t0);
+    return dispatch_dp(D, [&](auto dp) {
+      constexpr int DP = decltype(dp)::value;
+      using C = PredCfg<T, DP>;
+      const int64_t chunk = pred_chunk(N, Nq, C::KT);
+      const int64_t nchunks = (N + chunk - 1) / chunk;
+      const int64_t q_tiles = (Nq + C::QT - 1) / C::QT;
+      auto kern = pred_partial_kernel<T, DP>;
+      if (C::smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
+        if (e != cudaSuccess) {
+          set_error("log_pred_density_noalloc: %s", cudaGetErrorString(e));
+          return (int)LAKDE_ECUDA;
+        }
+      }
+      T *ws_m = static_cast<T *>(scratch);
+      T *ws_s = ws_m + nchunks * Nq;
+      kern<<<(unsigned)(q_tiles * nchunks), C::QT, C::smem, as_stream(stream)>>>(
+          static_cast<const T *>(X), static_cast<const T *>(W_triu), static_cast<const T *>(nu),
+          static_cast<const T *>(log_coeff), static_cast<const T *>(Y), ws_m, ws_s, N, Nq, (int)D, chunk, q_tiles);
+      int st = check_launch("log_pred_density_noalloc");
+      if (st) return st;
+      pred_combine_kernel<T><<<(unsigned)((Nq + 255) / 256), 256, 0, as_stream(stream)>>>(
+          ws_m, ws_s, static_cast<T *>(out), Nq, nchunks, (T)log((double)N));
+      return check_launch("log_pred_density_noalloc_combine");
     });
   });
 }
