@@ -130,9 +130,11 @@ class ClockSampler:
 
 
 def alg_bytes(N, D, nnz, es=4):
-    """Compulsory bytes per launch of the four kernels of one iteration."""
+    """Compulsory bytes per launch of the kernels of one iteration (each array once)."""
     T = D * D
     return {
+        # rowptr, order, col, r, X, prior P and factor T, per-kernel vectors, logrho
+        "vi_rows": 8 * (N + 1) + 4 * N + 4 * nnz + es * nnz + es * N * D + 2 * es * N * T + 8 * es * N + es * nnz,
         "mstep": 8 * (N + 1) + 4 * nnz + es * nnz + es * N * D + es * N * T + es * N,
         "posterior_factor": 3 * es * N * T + es * N * T + 3 * es * N + 4 * es * N + 4 * N,
         "estep_logrho": 8 * (N + 1) + 4 * nnz + es * N * D + es * N * T + 2 * es * N + es * nnz,
@@ -141,50 +143,50 @@ def alg_bytes(N, D, nnz, es=4):
 
 
 def timed_steps(eng, steps, flush, torch):
-    """Times each fused iteration with CUDA events (L2 flushed before each),
-    and within it the M-step, the factorisation and the E-step."""
+    """Times each VI iteration (the product step) with CUDA events, L2 flushed before each."""
     stream = torch.cuda.current_stream()
-    parts = {"mstep": 0.0, "posterior_factor": 0.0, "estep": 0.0, "updates": 0.0}
     total = 0.0
     for _ in range(steps):
         flush.zero_()
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
-        ev[0].record(stream)
-        eng.mstep()
-        ev[1].record(stream)
-        eng.factor()
-        ev[2].record(stream)
-        eng.estep(mode=1)
-        ev[3].record(stream)
-        torch.mul(eng.nu, eng.trace, out=eng.sigma_0_lambda_mm_trace)
-        torch.add(eng.sigma_0_lambda_mm_trace * (eng.nu_0 / 2), eng.b_0, out=eng.b)
-        ev[4].record(stream)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        eng.step()
+        b.record(stream)
         torch.cuda.synchronize()
-        for i, name in enumerate(parts):
-            parts[name] += ev[i].elapsed_time(ev[i + 1])
-        total += ev[0].elapsed_time(ev[4])
-    return total, parts
+        total += a.elapsed_time(b)
+    return total
 
 
-def split_estep(eng, reps, flush, torch):
-    """Average durations of the two E-step kernels, timed separately."""
+def kernel_split(eng, reps, flush, torch):
+    """Average duration of each library kernel of the iteration, timed one by one."""
     from lakde_b200 import kernels as K
 
     stream = torch.cuda.current_stream()
-    t_lr = t_nm = 0.0
+    p = eng.pattern
+    if eng.D <= 8:
+        launches = {
+            "vi_rows": lambda: K.vi_rows(p.rowptr, p.col, eng.r, eng.X, eng.nu_0, eng.a, eng.b, eng.b_0_f,
+                                         eng.W_inv_jitter, eng.eps, eng.nu, eng.logdet_W, eng.info, eng.logrho,
+                                         P=eng.sigma_0, T=eng.sigma_0_tril, order=p.order,
+                                         mm=eng.sigma_0_lambda_mm_trace),
+        }
+    else:
+        launches = {"mstep": eng.mstep, "posterior_factor": eng.factor,
+                    "estep_logrho": lambda: K.estep_logrho(p.rowptr, p.col, eng.X, eng.U, eng.nu, eng.logdet_W,
+                                                           out=eng.logrho)}
+    launches["estep_normalise"] = lambda: K.estep_normalise(p.cptr, p.pos, eng.logrho, eng.r, eng.c, eng.rsum, 1,
+                                                            eng.threshold)
+    out = {k: 0.0 for k in launches}
     for _ in range(reps):
-        flush.zero_()
-        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-        rowptr, col = eng._tri()
-        e[0].record(stream)
-        K.estep_logrho(rowptr, col, eng.X, eng.U, eng.nu, eng.logdet_W, out=eng.logrho)
-        e[1].record(stream)
-        K.estep_normalise(eng.pattern.cptr, eng.pattern.pos, eng.logrho, eng.r, eng.c, eng.rsum, 1, eng.threshold)
-        e[2].record(stream)
-        torch.cuda.synchronize()
-        t_lr += e[0].elapsed_time(e[1])
-        t_nm += e[1].elapsed_time(e[2])
-    return t_lr / reps, t_nm / reps
+        for name, fn in launches.items():
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            out[name] += a.elapsed_time(b)
+    return {k: v / reps for k, v in out.items()}
 
 
 def cpu_baseline(Xtr, graph, k, thr, budget_s=20.0):
@@ -328,11 +330,11 @@ def main():
 
     clocks.wait_for_samples(3, 20.0, busy)
     n_before = len(clocks.samples)
-    total_ms, per_kernel = timed_steps(eng, args.steps, flush, torch)
+    total_ms = timed_steps(eng, args.steps, flush, torch)
     torch.cuda.synchronize()
     clocks.wait_for_samples(n_before + 2, 20.0, busy)
     clocks.__exit__(None, None, None)
-    t_lr, t_nm = split_estep(eng, max(3, args.steps // 2), flush, torch)
+    durations = kernel_split(eng, max(3, args.steps // 2), flush, torch)
     ms_per_step = total_ms / args.steps
     if world > 1:
         t = torch.tensor([ms_per_step], device=dev)
@@ -340,13 +342,7 @@ def main():
         ms_per_step = float(t)
     value = world * 1000.0 / ms_per_step
 
-    # per-kernel average durations and the roofline of the dominant one
-    durations = {
-        "mstep": per_kernel["mstep"] / args.steps,
-        "posterior_factor": per_kernel["posterior_factor"] / args.steps,
-        "estep_logrho": t_lr,
-        "estep_normalise": t_nm,
-    }
+    # the roofline of the dominant kernel
     dom = max(durations, key=durations.get)
     ab = alg_bytes(N, D, nnz)
     peak, peak_kind = load_peaks()
@@ -432,7 +428,7 @@ def main():
                                  "kernels": N, "mean_log_density": float(lpd.mean())},
             "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "VI iters/s", "h2d_bytes_per_step": X.numel() * 4,
                     "d2h_bytes_per_step": 8, "elbo": elbo},
-            "gpu_launches": 4 * args.steps,
+            "gpu_launches": (2 if D <= 8 else 4) * args.steps,
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
         }

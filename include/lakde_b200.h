@@ -156,6 +156,31 @@ LAKDE_API int lakde_estep_logrho(int dtype, int64_t N, int64_t D, int64_t npts,
                        void *logrho, void *stream);
 
 /*
+ * One VI iteration's per-kernel work for D <= 8 in a single pass, one thread
+ * per kernel row (kernels are the points 0..N-1 of X[npts,D]):
+ *   nu_n = nu_0 + sum_p r_p and S_n = sum_p r_p (x_m - x_n)(x_m - x_n)^T
+ *   L_n = chol(nu_0 a_n / b_n P_n + S_n + jitter_n I) in FP64 with the ladder of
+ *         lakde_posterior_factor (info_n = -1 when it fails)
+ *   logdet_W_n = -2 sum log L_ii; mm_n = nu_n ||L_n^-1 T_n||_F^2 (if T given;
+ *         = nu_n chol_mm_trace(T_n, W_triu_n)) and then b_n = b_0 + nu_0 mm_n / 2
+ *   logrho_p = 0.5 (mvdigamma(nu_n/2, D) + D log 2 + logdet_W_n)
+ *              - nu_n / 2 ||L_n^-1 (x_m - x_n)||^2  (-inf on the self pair)
+ * Restates lakde/local_adaptive_kde.py:66-96 and :36-44 and
+ * lakde/local_knn_kde.py:220-236 for the batch schedule.  rowptr I64 [N+1],
+ * col I32 [nnz], order I32 [N] (visiting order, may be NULL), r / logrho [nnz],
+ * P and T [D,D] blocks with batch strides (0 = shared), a, b (in/out), jitter
+ * (in/out), nu, logdet_W, mm [N] (mm may be NULL), info [N].
+ */
+LAKDE_API int lakde_vi_rows(int dtype, int64_t N, int64_t D, int64_t npts,
+                            const void *rowptr, const void *col,
+                            const void *order, const void *r, const void *X,
+                            double nu_0, const void *P, int64_t P_batch_stride,
+                            const void *T, int64_t T_batch_stride,
+                            const void *a, void *b, double b_0, void *jitter,
+                            double eps, void *nu, void *logdet_W, void *mm,
+                            int32_t *info, void *logrho, void *stream);
+
+/*
  * Per-point normaliser, responsibilities and rebalance over a pair pattern
  * given point-major: pairs of point m are pos[cptr[m] .. cptr[m+1]) (indices
  * into logrho / r).  mode 0 (initial pass): c_m = logsumexp_n logrho.
@@ -196,6 +221,33 @@ LAKDE_API int lakde_log_pred_density(int dtype, int64_t N, int64_t Nq, int64_t D
                            const void *log_coeff, const void *Y, void *out,
                            void *workspace, size_t workspace_bytes,
                            void *stream);
+
+/* Workspace bytes lakde_log_pred_density_bwd needs. */
+LAKDE_API size_t lakde_log_pred_density_bwd_workspace(int dtype, int64_t N,
+                                                      int64_t Nq, int64_t D);
+
+/*
+ * Backward of lakde_log_pred_density for an upstream gradient g [Nq] (new;
+ * the reference's log_pred_density, lakde/local_adaptive_kde.py:200-223, is
+ * not differentiable).  With z = W_triu_n^T (y - x_n), Q = |z|^2,
+ * h_n = (nu_n + 1)/2 and softmax weights w_ny over kernels (recomputed from
+ * the forward output `out`), writes
+ *   grad_Y [Nq, D]  = sum_n g_y w_ny (-2 h_n / (1 + Q)) W_triu_n z      (score)
+ *   cw [N, Nq]      = g_y w_ny / (1 + Q)
+ *   sw [N]          = sum_y g_y w_ny
+ *   S_c [N, D, D]   = sum_y cw_ny (y - x_n)(y - x_n)^T
+ * from which d/dL_n = 2 h_n W_triu_n W_triu_n^T S_c W_triu_n - sw_n diag(1/L_ii)
+ * (lower part) for the Cholesky factor L_n = W_triu_n^-T.  Quad forms are
+ * recomputed, never stored per pair and dimension.
+ */
+LAKDE_API int lakde_log_pred_density_bwd(int dtype, int64_t N, int64_t Nq,
+                                         int64_t D, const void *X,
+                                         const void *W_triu, const void *nu,
+                                         const void *log_coeff, const void *Y,
+                                         const void *out, const void *grad_out,
+                                         void *grad_Y, void *cw, void *sw,
+                                         void *S_c, void *workspace,
+                                         size_t workspace_bytes, void *stream);
 
 /*
  * lakde_log_pred_density without any device allocation.  This entry point has

@@ -49,12 +49,23 @@ _SIGNATURES = {
          _c_vp, _c_vp],
         _c_int,
     ),
+    "lakde_vi_rows": (
+        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_vp, _c_i64, _c_vp, _c_i64,
+         _c_vp, _c_vp, _c_dbl, _c_vp, _c_dbl, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
+        _c_int,
+    ),
     "lakde_estep_normalise": (
         [_c_int, _c_i64, _c_vp, _c_vp, _c_int, _c_vp, _c_vp, _c_vp, _c_vp, _c_int, _c_dbl, _c_vp],
         _c_int,
     ),
     "lakde_pred_coeff": ([_c_int, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
     "lakde_log_pred_density_workspace": ([_c_int, _c_i64, _c_i64, _c_i64], ctypes.c_size_t),
+    "lakde_log_pred_density_bwd_workspace": ([_c_int, _c_i64, _c_i64, _c_i64], ctypes.c_size_t),
+    "lakde_log_pred_density_bwd": (
+        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
+         _c_vp, _c_vp, ctypes.c_size_t, _c_vp],
+        _c_int,
+    ),
     "lakde_log_pred_density_noalloc": (
         [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
         _c_int,

@@ -62,51 +62,108 @@ __global__ void __launch_bounds__(128) estep_logrho_kernel(const RP *__restrict_
   }
 }
 
+// Normaliser, threshold and rebalance of one point from its log rho values
+// (one warp per point).  Points with at most 128 pairs keep their values in
+// registers (four per lane) and read logrho once; longer lists loop.
+template <typename T>
+struct NormParams {
+  int mode;
+  T thr, eps, tiny, big;
+};
+
+template <typename T>
+__device__ __forceinline__ T normaliser_update(T c_old, T rs_old, T lse, int mode) {
+  if (mode == 0) return logaddexp(c_old, lse);
+  const T old_contrib = log(rs_old) + c_old;
+  return logaddexp(logsubexp(c_old, old_contrib), lse);
+}
+
+template <typename T>
+__device__ __forceinline__ T responsibility(T lr, T c_new, T thr) {
+  T rv = exp(lr - c_new);
+  if (thr > T(0) && rv <= thr) rv = T(0);
+  return rv;
+}
+
+template <typename T>
+__device__ __forceinline__ T clamp_coeff(T sum, const NormParams<T> &np, T *c_fin, T c_new) {
+  sum = sum < np.eps ? np.eps : sum;
+  *c_fin = c_new + log(sum);
+  T coeff = T(1) / sum;
+  return coeff < np.tiny ? np.tiny : (coeff > np.big ? np.big : coeff);
+}
+
 template <typename T, typename PI>
 __global__ void __launch_bounds__(256) estep_normalise_kernel(const int64_t *__restrict__ cptr,
                                                               const PI *__restrict__ pos,
                                                               const T *__restrict__ logrho, T *__restrict__ r,
                                                               T *__restrict__ c, T *__restrict__ rsum,
-                                                              int64_t npts, int mode, T thr, T eps, T tiny,
-                                                              T big) {
+                                                              int64_t npts, NormParams<T> np) {
+  constexpr int R = 4;
   const int lane = threadIdx.x & 31;
   const int64_t m = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (m >= npts) return;
   const int64_t s = cptr[m], e = cptr[m + 1];
-  T mx = neg_inf<T>();
-  for (int64_t p = s + lane; p < e; p += 32) mx = fmax(mx, logrho[pos[p]]);
-  mx = warp_max(mx);
-  T se = T(0);
-  if (mx != neg_inf<T>())
-    for (int64_t p = s + lane; p < e; p += 32) se += exp(logrho[pos[p]] - mx);
-  se = warp_sum(se);
-  const T lse = (mx == neg_inf<T>()) ? mx : mx + log(se);
   const T c_old = c[m];
-  T c_new;
-  if (mode == 0) {
-    c_new = logaddexp(c_old, lse);
+  const T rs_old = rsum[m];
+  T c_new, c_fin, coeff, rs = T(0);
+  if (e - s <= 32 * R) {
+    T v[R];
+    int64_t q[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const int64_t p = s + lane + 32 * k;
+      q[k] = p < e ? (int64_t)pos[p] : -1;
+      v[k] = q[k] >= 0 ? logrho[q[k]] : neg_inf<T>();
+    }
+    T mx = v[0];
+#pragma unroll
+    for (int k = 1; k < R; ++k) mx = fmax(mx, v[k]);
+    mx = warp_max(mx);
+    T se = T(0);
+    if (mx != neg_inf<T>()) {
+#pragma unroll
+      for (int k = 0; k < R; ++k)
+        if (q[k] >= 0) se += exp(v[k] - mx);
+    }
+    se = warp_sum(se);
+    const T lse = (mx == neg_inf<T>()) ? mx : mx + log(se);
+    c_new = normaliser_update(c_old, rs_old, lse, np.mode);
+    T sum = T(0);
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      v[k] = q[k] >= 0 ? responsibility(v[k], c_new, np.thr) : T(0);
+      sum += v[k];
+    }
+    sum = warp_sum(sum);
+    coeff = clamp_coeff(sum, np, &c_fin, c_new);
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      if (q[k] >= 0) {
+        const T rv = v[k] * coeff;
+        r[q[k]] = rv;
+        rs += rv;
+      }
+    }
   } else {
-    const T old_contrib = log(rsum[m]) + c_old;
-    c_new = logaddexp(logsubexp(c_old, old_contrib), lse);
-  }
-  T sum = T(0);
-  for (int64_t p = s + lane; p < e; p += 32) {
-    T rv = exp(logrho[pos[p]] - c_new);
-    if (thr > T(0) && rv <= thr) rv = T(0);
-    sum += rv;
-  }
-  sum = warp_sum(sum);
-  sum = sum < eps ? eps : sum;
-  const T c_fin = c_new + log(sum);
-  T coeff = T(1) / sum;
-  coeff = coeff < tiny ? tiny : (coeff > big ? big : coeff);
-  T rs = T(0);
-  for (int64_t p = s + lane; p < e; p += 32) {
-    T rv = exp(logrho[pos[p]] - c_new);
-    if (thr > T(0) && rv <= thr) rv = T(0);
-    rv = rv * coeff;
-    r[pos[p]] = rv;
-    rs += rv;
+    T mx = neg_inf<T>();
+    for (int64_t p = s + lane; p < e; p += 32) mx = fmax(mx, logrho[pos[p]]);
+    mx = warp_max(mx);
+    T se = T(0);
+    if (mx != neg_inf<T>())
+      for (int64_t p = s + lane; p < e; p += 32) se += exp(logrho[pos[p]] - mx);
+    se = warp_sum(se);
+    const T lse = (mx == neg_inf<T>()) ? mx : mx + log(se);
+    c_new = normaliser_update(c_old, rs_old, lse, np.mode);
+    T sum = T(0);
+    for (int64_t p = s + lane; p < e; p += 32) sum += responsibility(logrho[pos[p]], c_new, np.thr);
+    sum = warp_sum(sum);
+    coeff = clamp_coeff(sum, np, &c_fin, c_new);
+    for (int64_t p = s + lane; p < e; p += 32) {
+      const T rv = responsibility(logrho[pos[p]], c_new, np.thr) * coeff;
+      r[pos[p]] = rv;
+      rs += rv;
+    }
   }
   rs = warp_sum(rs);
   if (lane == 0) {
@@ -185,10 +242,10 @@ extern "C" int lakde_estep_normalise(int dtype, int64_t npts, const void *cptr, 
       const T eps = std::is_same<T, float>::value ? (T)1.1920928955078125e-07 : (T)2.220446049250313e-16;
       const T tiny = std::is_same<T, float>::value ? (T)1.1754943508222875e-38 : (T)2.2250738585072014e-308;
       const T big = std::is_same<T, float>::value ? (T)3.4028234663852886e+38 : (T)1.7976931348623157e+308;
+      NormParams<T> np{mode, (T)threshold, eps, tiny, big};
       estep_normalise_kernel<T, PI><<<blocks, 256, 0, as_stream(stream)>>>(
           static_cast<const int64_t *>(cptr), static_cast<const PI *>(pos), static_cast<const T *>(logrho),
-          static_cast<T *>(r), static_cast<T *>(c), static_cast<T *>(rsum), npts, mode, (T)threshold, eps, tiny,
-          big);
+          static_cast<T *>(r), static_cast<T *>(c), static_cast<T *>(rsum), npts, np);
       return check_launch("estep_normalise");
     });
   });

@@ -1,0 +1,278 @@
+// One VI iteration's per-kernel work in a single pass, one thread per kernel
+// row, for small D (D <= 8): everything lives in registers.
+//
+//   M-step     S_n = sum_p r_p (x_m - x_n)(x_m - x_n)^T, nu_n = nu_0 + sum_p r_p
+//              (lakde/local_adaptive_kde.py:66-81)
+//   posterior  A_n = nu_0 a_n / b_n P_n + S_n, FP64 Cholesky with the jitter
+//              ladder (lakde/local_adaptive_kde.py:83-96, lakde/linalg_util.py:109-170)
+//   summaries  logdet_W_n = -2 sum log L_ii, trace_n = ||L_n^-1 T_n||_F^2
+//              (= ||T_n^T W_triu_n||_F^2), mm_n = nu_n trace_n and the new
+//              b_n = b_0 + nu_0 mm_n / 2 (lakde/local_knn_kde.py:220-236)
+//   E-step     log rho_p = 0.5 (mvdigamma(nu_n/2) + D log 2 + logdet_W_n)
+//              - nu_n / 2 ||L_n^-1 (x_m - x_n)||^2, by forward substitution with
+//              L_n (the same quantity as ||W_triu_n^T (x_m - x_n)||^2 with
+//              W_triu = L^-T), -inf on the self pair (lakde/local_adaptive_kde.py:36-44)
+//
+// Rows are visited in a caller-given order (longest first), so the threads of
+// a warp carry rows of similar length.
+#include "common.cuh"
+
+namespace lakde {
+
+template <typename T>
+struct RowArgs {
+  const int64_t *rowptr;
+  const int32_t *col;
+  const int32_t *order;
+  const T *r;
+  const T *X;
+  int64_t npts;
+  T nu0;
+  const T *P;
+  int64_t Pbs;
+  const T *Tm;
+  int64_t Tbs;
+  const T *a;
+  T *b;
+  T b0;
+  T *jitter;
+  double eps;
+  T *nu_out;
+  T *logdet_out;
+  T *mm_out;
+  int32_t *info;
+  T *logrho;
+  int64_t N;
+  int D;
+};
+
+__device__ __forceinline__ float f_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double f_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float f_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double f_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float f_div(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double f_div(double a, double b) { return __ddiv_rn(a, b); }
+
+template <int DP>
+__device__ __forceinline__ constexpr int tix(int i, int j) { return i * (i + 1) / 2 + j; }
+
+// Cholesky of (scale P + S + jit I) in FP64 registers; false if a pivot is
+// not positive.  Padded dimensions are the identity.
+template <typename T, int DP>
+__device__ __forceinline__ bool chol_rows(const T (&S)[DP * (DP + 1) / 2], const T *__restrict__ P, T scale, T jit,
+                                          int D, double (&L)[DP * (DP + 1) / 2]) {
+#pragma unroll
+  for (int i = 0; i < DP; ++i)
+#pragma unroll
+    for (int j = 0; j <= i; ++j) {
+      double v;
+      if (i < D) {
+        T s = S[tix<DP>(i, j)];
+        if (P) s = f_add(f_mul(P[i * D + j], scale), s);
+        if (i == j) s = f_add(s, jit);
+        v = (double)s;
+      } else {
+        v = (i == j) ? 1.0 : 0.0;
+      }
+      L[tix<DP>(i, j)] = v;
+    }
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < DP; ++k) {
+    const double piv = L[tix<DP>(k, k)];
+    ok = ok && (piv > 0.0);
+    const double lkk = sqrt(ok ? piv : 1.0);
+    const double rk = 1.0 / lkk;
+    L[tix<DP>(k, k)] = lkk;
+#pragma unroll
+    for (int i = k + 1; i < DP; ++i) L[tix<DP>(i, k)] *= rk;
+#pragma unroll
+    for (int i = k + 1; i < DP; ++i)
+#pragma unroll
+      for (int j = k + 1; j <= i; ++j) L[tix<DP>(i, j)] -= L[tix<DP>(i, k)] * L[tix<DP>(j, k)];
+  }
+  return ok;
+}
+
+template <typename T, int DP>
+__global__ void __launch_bounds__(128) vi_rows_kernel(RowArgs<T> g) {
+  constexpr int TT = DP * (DP + 1) / 2;
+  const int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (it >= g.N) return;
+  const int64_t n = g.order ? (int64_t)g.order[it] : it;
+  const int D = g.D;
+  const int64_t start = g.rowptr[n], end = g.rowptr[n + 1];
+  bool bad = end < start;
+
+  T xn[DP];
+#pragma unroll
+  for (int d = 0; d < DP; ++d) xn[d] = d < D ? g.X[n * D + d] : T(0);
+
+  // ---------------------------------------------------------------- M-step
+  T S[TT];
+#pragma unroll
+  for (int e = 0; e < TT; ++e) S[e] = T(0);
+  T vsum = T(0);
+  for (int64_t p = start; p < end; ++p) {
+    const int64_t c = g.col[p];
+    const T v = g.r[p];
+    if (c < 0 || c >= g.npts) {
+      bad = true;
+      continue;
+    }
+    T dl[DP];
+#pragma unroll
+    for (int d = 0; d < DP; ++d) dl[d] = d < D ? g.X[c * D + d] - xn[d] : T(0);
+#pragma unroll
+    for (int i = 0; i < DP; ++i) {
+      const T vi = v * dl[i];
+#pragma unroll
+      for (int j = 0; j <= i; ++j) S[tix<DP>(i, j)] = fma(vi, dl[j], S[tix<DP>(i, j)]);
+    }
+    vsum += v;
+  }
+  const T nu = g.nu0 + vsum;
+
+  // ------------------------------------------------------------- posterior
+  const T b_old = g.b[n];
+  const T scale = f_mul(g.nu0, f_div(g.a[n], b_old));
+  const T *P = g.P ? g.P + n * g.Pbs : nullptr;
+  T jit = g.jitter[n];
+  double L[TT];
+  bool ok = chol_rows<T, DP>(S, P, scale, jit, D, L);
+  if (!ok) {
+    T jt = T(0);
+    for (int k = 0; k < 32 && !ok; ++k) {
+      jt = f_add(jt, (T)(g.eps * ldexp(1.0, k)));
+      ok = chol_rows<T, DP>(S, P, scale, jt, D, L);
+      if (ok) jit = jt;
+    }
+  }
+  ok = ok && !bad;
+
+  // logdet of W = 2 sum log W_triu_ii, W_triu_ii = 1 / L_ii (in the model dtype)
+  double ld = 0.0;
+#pragma unroll
+  for (int i = 0; i < DP; ++i)
+    if (i < D) ld += log((double)(T)(1.0 / L[tix<DP>(i, i)]));
+  const T logdet = (T)(2.0 * ld);
+
+  // trace ||L^-1 T_n||_F^2 by forward substitution of each column of T_n
+  double tr = 0.0;
+  if (g.Tm) {
+    const T *Tn = g.Tm + n * g.Tbs;
+    for (int a = 0; a < D; ++a) {
+      double z[DP];
+#pragma unroll
+      for (int i = 0; i < DP; ++i) {
+        double s = i < D ? (double)Tn[i * D + a] : 0.0;
+#pragma unroll
+        for (int j = 0; j < i; ++j) s -= L[tix<DP>(i, j)] * z[j];
+        z[i] = s / L[tix<DP>(i, i)];
+        tr += z[i] * z[i];
+      }
+    }
+  }
+  const T mm = nu * (T)tr;
+  const T nanv = T(NAN);
+  g.jitter[n] = jit;
+  g.info[n] = ok ? 0 : -1;
+  g.nu_out[n] = ok ? nu : nanv;
+  g.logdet_out[n] = ok ? logdet : nanv;
+  if (g.mm_out) g.mm_out[n] = ok ? mm : nanv;
+  if (g.Tm) g.b[n] = ok ? g.b0 + g.nu0 * mm / T(2) : nanv;
+
+  // ---------------------------------------------------------------- E-step
+  T Lf[TT], rinv[DP];
+#pragma unroll
+  for (int i = 0; i < DP; ++i) {
+#pragma unroll
+    for (int j = 0; j < i; ++j) Lf[tix<DP>(i, j)] = (T)L[tix<DP>(i, j)];
+    rinv[i] = (T)(1.0 / L[tix<DP>(i, i)]);
+  }
+  const double e = mvdigamma_d(0.5 * (double)nu, D) + D * 0.69314718055994530942 + (double)logdet;
+  const T cst = (T)(0.5 * e);
+  const T expo = T(-0.5) * nu;
+  for (int64_t p = start; p < end; ++p) {
+    const int64_t c = g.col[p];
+    if (!ok || c < 0 || c >= g.npts) {
+      g.logrho[p] = nanv;
+      continue;
+    }
+    T y[DP];
+    T q = T(0);
+#pragma unroll
+    for (int i = 0; i < DP; ++i) {
+      T s = i < D ? g.X[c * D + i] - xn[i] : T(0);
+#pragma unroll
+      for (int j = 0; j < i; ++j) s = fma(-Lf[tix<DP>(i, j)], y[j], s);
+      y[i] = s * rinv[i];
+      q = fma(y[i], y[i], q);
+    }
+    T lr = f_add(f_mul(q, expo), cst);
+    if (c == n) lr = neg_inf<T>();
+    g.logrho[p] = lr;
+  }
+}
+
+}  // namespace lakde
+
+using namespace lakde;
+
+extern "C" int lakde_vi_rows(int dtype, int64_t N, int64_t D, int64_t npts, const void *rowptr, const void *col,
+                             const void *order, const void *r, const void *X, double nu_0, const void *P,
+                             int64_t P_batch_stride, const void *T, int64_t T_batch_stride, const void *a, void *b,
+                             double b_0, void *jitter, double eps, void *nu, void *logdet_W, void *mm,
+                             int32_t *info, void *logrho, void *stream) {
+  clear_error();
+  if (N < 0 || D < 1 || npts < N) {
+    set_error("vi_rows: invalid sizes (N=%lld, D=%lld, npts=%lld)", (long long)N, (long long)D, (long long)npts);
+    return LAKDE_EINVAL;
+  }
+  if (N == 0) return LAKDE_OK;
+  if (D > 8) {
+    set_error("vi_rows: D=%lld; the register-resident fused kernel covers D <= 8", (long long)D);
+    return LAKDE_EUNSUPPORTED;
+  }
+  if (!rowptr || !col || !r || !X || !a || !b || !jitter || !nu || !logdet_W || !info || !logrho) {
+    set_error("vi_rows: null pointer");
+    return LAKDE_EINVAL;
+  }
+  if (int st = bind_device("vi_rows", {logrho, rowptr, col, order, r, X, P, T, a, b, jitter, nu, logdet_W, mm, info}))
+    return st;
+  return dispatch_float(dtype, [&](auto t0) {
+    using TT = decltype(t0);
+    RowArgs<TT> g;
+    g.rowptr = static_cast<const int64_t *>(rowptr);
+    g.col = static_cast<const int32_t *>(col);
+    g.order = static_cast<const int32_t *>(order);
+    g.r = static_cast<const TT *>(r);
+    g.X = static_cast<const TT *>(X);
+    g.npts = npts;
+    g.nu0 = (TT)nu_0;
+    g.P = static_cast<const TT *>(P);
+    g.Pbs = P_batch_stride;
+    g.Tm = static_cast<const TT *>(T);
+    g.Tbs = T_batch_stride;
+    g.a = static_cast<const TT *>(a);
+    g.b = static_cast<TT *>(b);
+    g.b0 = (TT)b_0;
+    g.jitter = static_cast<TT *>(jitter);
+    g.eps = eps;
+    g.nu_out = static_cast<TT *>(nu);
+    g.logdet_out = static_cast<TT *>(logdet_W);
+    g.mm_out = static_cast<TT *>(mm);
+    g.info = info;
+    g.logrho = static_cast<TT *>(logrho);
+    g.N = N;
+    g.D = (int)D;
+    const unsigned blocks = (unsigned)((N + 127) / 128);
+    if (D <= 2)
+      vi_rows_kernel<TT, 2><<<blocks, 128, 0, as_stream(stream)>>>(g);
+    else if (D <= 4)
+      vi_rows_kernel<TT, 4><<<blocks, 128, 0, as_stream(stream)>>>(g);
+    else
+      vi_rows_kernel<TT, 8><<<blocks, 128, 0, as_stream(stream)>>>(g);
+    return check_launch("vi_rows");
+  });
+}

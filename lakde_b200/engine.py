@@ -44,6 +44,7 @@ class FusedVI:
         self.nu_0_t = torch.full((1,), self.nu_0, dtype=self.dtype, device=self.device)
         self.a_0 = a_0
         self.b_0 = b_0
+        self.b_0_f = float(b_0)  # host copy: no device read inside a captured step
         self.threshold = float(threshold or 0.0)
         self.eps = torch.finfo(self.dtype).eps
         N, D = self.N, self.D
@@ -195,6 +196,15 @@ class FusedKNN(FusedVI):
 
     def step(self):
         """lakde/local_knn_kde.py:209-254 at block_size = N."""
+        if self.D <= 8:
+            # M-step, factorisation, summaries, b update and log rho in one pass
+            p = self.pattern
+            K.vi_rows(p.rowptr, p.col, self.r, self.X, self.nu_0, self.a, self.b, self.b_0_f, self.W_inv_jitter,
+                      self.eps, self.nu, self.logdet_W, self.info, self.logrho, P=self.sigma_0, T=self.sigma_0_tril,
+                      order=p.order, mm=self.sigma_0_lambda_mm_trace)
+            torch.minimum(self.failed, self.info.min(), out=self.failed)
+            K.estep_normalise(p.cptr, p.pos, self.logrho, self.r, self.c, self.rsum, 1, self.threshold)
+            return
         self.mstep()
         self.factor()
         self.estep(mode=1)

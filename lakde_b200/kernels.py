@@ -238,6 +238,27 @@ def estep_logrho(rowptr, col, X, W_triu, nu, logdet_W, kernel_offset=0, out=None
     return out
 
 
+def vi_rows(rowptr, col, r, X, nu_0, a, b, b_0, jitter, eps, nu, logdet_W, info, logrho, P=None, T=None,
+            order=None, mm=None):
+    """Fused per-kernel pass of one VI iteration for D <= 8 (see include/lakde_b200.h)."""
+    nat.require_cuda(rowptr, col, r, X, a, b, jitter, nu, logdet_W, info, logrho, P, T, order, mm, op="vi_rows")
+    N = rowptr.numel() - 1
+    D = X.size(1)
+    assert rowptr.dtype == torch.int64 and col.dtype == torch.int32
+    assert order is None or order.dtype == torch.int32
+    pbs = 0 if P is None or P.dim() == 2 else D * D
+    tbs = 0 if T is None or T.dim() == 2 else D * D
+    nat.check(
+        nat.lib().lakde_vi_rows(
+            nat.dtype_code(X), N, D, X.size(0), nat.ptr(rowptr), nat.ptr(col), nat.ptr(order), nat.ptr(r),
+            nat.ptr(X), float(nu_0), nat.ptr(P), pbs, nat.ptr(T), tbs, nat.ptr(a), nat.ptr(b), float(b_0),
+            nat.ptr(jitter), float(eps), nat.ptr(nu), nat.ptr(logdet_W), nat.ptr(mm), nat.ptr(info), nat.ptr(logrho),
+            nat.stream_of(X),
+        ),
+        "vi_rows",
+    )
+
+
 def estep_normalise(cptr, pos, logrho, r, c, rsum, mode, threshold):
     """Per-point normaliser, responsibilities and rebalance (see include/lakde_b200.h)."""
     nat.require_cuda(cptr, pos, logrho, r, c, rsum, op="estep_normalise")
@@ -287,3 +308,31 @@ def log_pred_density(X, W_triu, nu, log_coeff, Y, out=None, workspace=None):
         "log_pred_density",
     )
     return out
+
+
+def log_pred_density_bwd(X, W_triu, nu, log_coeff, Y, out, grad_out):
+    """Pair pass of the predictive-density backward (see include/lakde_b200.h).
+
+    Returns (grad_Y [Nq, D], sw [N], S_c [N, D, D]); the [N, Nq] weights are a
+    temporary of the call.
+    """
+    nat.require_cuda(X, W_triu, nu, log_coeff, Y, out, grad_out, op="log_pred_density_bwd")
+    N, D = X.shape
+    Nq = Y.size(0)
+    Y = Y.contiguous()
+    grad_out = grad_out.contiguous()
+    gY = torch.empty_like(Y)
+    cw = X.new_empty(N, Nq)
+    sw = X.new_empty(N)
+    S_c = X.new_empty(N, D, D)
+    need = int(nat.lib().lakde_log_pred_density_bwd_workspace(nat.dtype_code(X), N, Nq, D))
+    ws = torch.empty(max(need, 1), dtype=torch.uint8, device=X.device)
+    nat.check(
+        nat.lib().lakde_log_pred_density_bwd(
+            nat.dtype_code(X), N, Nq, D, nat.ptr(X), nat.ptr(W_triu), nat.ptr(nu), nat.ptr(log_coeff), nat.ptr(Y),
+            nat.ptr(out), nat.ptr(grad_out), nat.ptr(gY), nat.ptr(cw), nat.ptr(sw), nat.ptr(S_c), nat.ptr(ws),
+            ws.numel(), nat.stream_of(X),
+        ),
+        "log_pred_density_bwd",
+    )
+    return gY, sw, S_c

@@ -73,6 +73,10 @@ class PairPattern:
         self.n_kernels = n_kernels
         self.n_points = n_points
         self.rank = rank
+        # kernel rows longest first: the fused per-row kernel walks rows in this
+        # order so the threads of a warp carry rows of similar length
+        lengths = rowptr[1:] - rowptr[:-1]
+        self.order = torch.argsort(lengths, descending=True, stable=True).to(torch.int32)
 
     @property
     def nnz(self):

@@ -285,3 +285,58 @@ def test_log_pred_density(K, D, dtype):
                                           nu.astype(np.float64), logdet.astype(np.float64))
     atol = 2e-4 if dtype == np.float32 else 1e-9
     np.testing.assert_allclose(out, ref, rtol=0, atol=atol * max(1, D / 8))
+
+
+# ------------------------------------------------------- fused per-row pass
+@pytest.mark.parametrize("D", [2, 5, 8])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_vi_rows_matches_unfused_composition(K, D, dtype):
+    rng = np.random.default_rng(10 + D)
+    N = 400
+    X = rng.standard_normal((N, D)).astype(dtype)
+    graph = O.knn_graph(X, 12)
+    ((rows, cols),) = O.knn_pattern(graph)
+    rowptr = O.ind2ptr(rows, N)
+    r = rng.uniform(0.01, 1, size=len(cols)).astype(dtype)
+    P = spd(rng, N, D, cond=10).astype(dtype) * 0.1
+    # rows 0..6: no prior and a single weighted pair, so S is rank one and
+    # the jitter ladder has to run
+    P[:7] = 0
+    for n in range(7):
+        r[rowptr[n] + 1 : rowptr[n + 1]] = 0
+    Tm = np.linalg.cholesky(P.astype(np.float64) + np.eye(D) * 1e-3).astype(dtype)
+    a = rng.uniform(2, 4, N).astype(dtype)
+    b = rng.uniform(1, 3, N).astype(dtype)
+    nu0, b0 = D + 0.5, 1e-6
+    eps = np.finfo(dtype).eps
+    # unfused reference composition
+    rp, cl, rr, Xt = t(rowptr), t(cols, torch.int32), t(r), t(X)
+    S, nu = K.mstep(rp, cl, rr, Xt, nu0)
+    jit1 = torch.zeros(N, dtype=Xt.dtype, device=DEV)
+    W, logdet, info, _, trace = K.posterior_factor(S, jit1, eps, P=t(P), nu_0=torch.tensor(nu0, device=DEV),
+                                                   a=t(a), b=t(b), T=t(Tm))
+    lr_ref = K.estep_logrho(rp, cl, Xt, W, nu, logdet)
+    mm_ref = nu * trace
+    b_ref = b0 + nu0 * mm_ref / 2
+    # fused
+    bt = t(b)
+    jit2 = torch.zeros_like(jit1)
+    nu2, ld2, mm2 = torch.empty_like(nu), torch.empty_like(nu), torch.empty_like(nu)
+    info2 = torch.empty(N, dtype=torch.int32, device=DEV)
+    lr2 = torch.empty_like(lr_ref)
+    pattern_order = torch.argsort(torch.tensor(np.diff(rowptr), device=DEV), descending=True).to(torch.int32)
+    K.vi_rows(rp, cl, rr, Xt, nu0, t(a), bt, b0, jit2, eps, nu2, ld2, info2, lr2, P=t(P), T=t(Tm),
+              order=pattern_order, mm=mm2)
+    assert (info2 == 0).all() and (info == 0).all()
+    # rank-one rows mostly need the ladder (a 2 x 2 one may factor by rounding)
+    assert (jit1[:7] > 0).any()
+    torch.testing.assert_close(jit2, jit1, rtol=0, atol=0)
+    rtol = 1e-4 if dtype == np.float32 else 1e-9
+    torch.testing.assert_close(nu2, nu, rtol=rtol, atol=0)
+    torch.testing.assert_close(ld2, logdet, rtol=rtol, atol=rtol * 10)
+    torch.testing.assert_close(mm2, mm_ref, rtol=10 * rtol, atol=rtol)
+    torch.testing.assert_close(bt, b_ref, rtol=10 * rtol, atol=rtol)
+    fin = torch.isfinite(lr_ref)
+    assert torch.equal(fin, torch.isfinite(lr2))
+    scale = lr_ref[fin].abs().max()
+    torch.testing.assert_close(lr2[fin], lr_ref[fin], rtol=10 * rtol, atol=10 * rtol * scale)
