@@ -129,10 +129,19 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+def alg_flops(N, D, nnz):
+    """Algorithmic flops per launch: nnz 2T for the triangular quad forms and for
+    the rank-one scatter (T = D (D + 1) / 2), D^3 / 3 each for the FP64 Cholesky,
+    inverse and trace products."""
+    T = D * (D + 1) // 2
+    return {"mstep": 2 * T * nnz, "mstep_tc": 2 * T * nnz, "estep_logrho": 2 * T * nnz, "estep_tc": 2 * T * nnz,
+            "posterior_factor": N * D ** 3}
+
+
 def alg_bytes(N, D, nnz, es=4):
     """Compulsory bytes per launch of the kernels of one iteration (each array once)."""
     T = D * D
-    return {
+    b = {
         # rowptr, order, col, r, X, prior P and factor T, per-kernel vectors, logrho
         "vi_rows": 8 * (N + 1) + 4 * N + 4 * nnz + es * nnz + es * N * D + 2 * es * N * T + 8 * es * N + es * nnz,
         "mstep": 8 * (N + 1) + 4 * nnz + es * nnz + es * N * D + es * N * T + es * N,
@@ -140,6 +149,9 @@ def alg_bytes(N, D, nnz, es=4):
         "estep_logrho": 8 * (N + 1) + 4 * nnz + es * N * D + es * N * T + 2 * es * N + es * nnz,
         "estep_normalise": 8 * (N + 1) + 4 * nnz + es * nnz + es * nnz + 4 * es * N,
     }
+    b["mstep_tc"] = b["mstep"]
+    b["estep_tc"] = b["estep_logrho"]
+    return b
 
 
 def timed_steps(eng, steps, flush, torch):
@@ -171,9 +183,12 @@ def kernel_split(eng, reps, flush, torch):
                                          mm=eng.sigma_0_lambda_mm_trace),
         }
     else:
-        launches = {"mstep": eng.mstep, "posterior_factor": eng.factor,
-                    "estep_logrho": lambda: K.estep_logrho(p.rowptr, p.col, eng.X, eng.U, eng.nu, eng.logdet_W,
-                                                           out=eng.logrho)}
+        tcs = "_tc" if eng.precision == "mixed" else ""
+        launches = {"mstep" + tcs: eng.mstep, "posterior_factor": eng.factor,
+                    "estep" + (tcs or "_logrho"): lambda: (
+                        K.estep_tc(p.rowptr, p.col, eng.X, eng.U, eng.nu, eng.logdet_W, eng.err, order=p.order,
+                                   out=eng.logrho) if eng.precision == "mixed" else
+                        K.estep_logrho(p.rowptr, p.col, eng.X, eng.U, eng.nu, eng.logdet_W, out=eng.logrho))}
     launches["estep_normalise"] = lambda: K.estep_normalise(p.cptr, p.pos, eng.logrho, eng.r, eng.c, eng.rsum, 1,
                                                             eng.threshold)
     out = {k: 0.0 for k in launches}
@@ -190,39 +205,47 @@ def kernel_split(eng, reps, flush, torch):
 
 
 def cpu_baseline(Xtr, graph, k, thr, budget_s=20.0):
-    """The reference algorithm (oracle port, numpy) timed on a bounded sample:
-    one partial step (kernel block of 512, dense E-step against every point)
-    of the block schedule, extrapolated to one VI iteration over all blocks."""
+    """The reference algorithm (oracle port, numpy) timed on a bounded sample of
+    one VI iteration of its block schedule (blocks of 512 kernels, dense E-step
+    against every point): the posterior of one kernel block, then as many of
+    its point blocks of the dense E-step as fit the time budget; extrapolated
+    to all point blocks and all kernel blocks."""
     from oracle import lakde_oracle as O
 
     N, D = Xtr.shape
     B = 512
     m = O.KNNKDEOracle(k=graph.astype(np.int64), block_size=B)
     m.init_parameters_(Xtr, thr)
-    # state after initialisation without the two dense initial epochs (they do
-    # not change the cost of a step): unit normalisers and the prior posterior
     m.rnm_log_consts[:] = 0.0
-    m.nu[:] = float(m.nu_0)
-    m.logdet_W[:] = 0.0
-    m.logdet_sigma_0[:] = 0.0
-    m.sigma_0_lambda_mm_trace[:] = 1.0
     t0 = time.perf_counter()
-    steps = 0
-    while True:
-        m.partial_step_(Xtr, steps % ((N - 1) // B + 1), thr)
-        steps += 1
-        if time.perf_counter() - t0 > budget_s or steps >= 2:
-            break
-    per_step = (time.perf_counter() - t0) / steps
-    n_blocks = (N - 1) // B + 1
-    iters_per_s = 1.0 / (per_step * n_blocks)
+    S, nu = m._posterior_contribs(Xtr, 0)
+    sigma_0, _ = m.prior_cov(Xtr, 0)
+    W = m._posterior(0, N, sigma_0, S)
+    t_post = time.perf_counter() - t0
+    logdet = O.chol_logdet(W)
+    n_pb = (N - 1) // B + 1
+    done = 0
+    t1 = time.perf_counter()
+    while done < n_pb and (done < 1 or time.perf_counter() - t1 < budget_s):
+        js = done * B
+        lr = O.calc_log_rho_block(Xtr[js:js + B], Xtr[:B], nu, W, logdet)
+        c = O.logsumexp0(lr)
+        r = np.exp(lr - c[None, :])
+        if thr:
+            r = np.where(r > thr, r, 0)
+        np.nonzero(r)
+        done += 1
+    t_block = (time.perf_counter() - t1) / done
+    per_step = t_post + n_pb * t_block
+    n_kb = (N - 1) // B + 1
     return {
-        "value": iters_per_s,
+        "value": 1.0 / (per_step * n_kb),
         "unit": "VI iters/s",
         "cores": os.cpu_count(),
         "kind": "port",
-        "sample": f"{steps} partial step(s) of the block schedule (block 512 of {N} kernels, dense E-step over all "
-                  f"{N} points, numpy oracle) at {per_step:.2f} s each, extrapolated x{n_blocks} blocks",
+        "sample": (f"posterior of one 512-kernel block ({t_post:.2f} s) + {done} of {n_pb} point blocks of its "
+                   f"dense E-step ({t_block:.3f} s each), numpy oracle; extrapolated to {n_pb} point blocks x "
+                   f"{n_kb} kernel blocks"),
     }
 
 
@@ -241,7 +264,7 @@ def run_reference(args):
     # get random neighbours (they do not enter the timed work)
     graph[:] = rng.integers(0, N, size=(N, k))
     graph[:1024] = O.knn_graph(Xtr, k)[:1024] if N <= 1024 else _block_knn(Xtr, k, 1024)
-    # each timed step is one bounded sample (about 10-30 s); stop after ~90 s
+    # each timed step is one bounded sample; stop after ~90 s
     vals = []
     t0 = time.perf_counter()
     for _ in range(max(1, args.steps)):
@@ -283,6 +306,7 @@ def main():
     ap.add_argument("--workload", default="gas8", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="auto", choices=["auto", "mixed", "fp32"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -305,7 +329,7 @@ def main():
     Xtr, Xte, k, thr, desc = make_data(args.workload)
     X = torch.tensor(Xtr, device=dev)
     Y = torch.tensor(Xte, device=dev)
-    model = LocalKNearestKDE(k_or_knn_graph=k, fused=True, cuda_graph=False)
+    model = LocalKNearestKDE(k_or_knn_graph=k, fused=True, cuda_graph=False, precision=args.precision)
     t_init = time.perf_counter()
     model.fit(X, iterations=0, sparsity_threshold=thr)
     torch.cuda.synchronize()
@@ -316,6 +340,7 @@ def main():
     for _ in range(args.warmup):
         eng.step()
     torch.cuda.synchronize()
+    snap = eng.snapshot()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
 
     if world > 1:
@@ -342,12 +367,41 @@ def main():
         ms_per_step = float(t)
     value = world * 1000.0 / ms_per_step
 
-    # the roofline of the dominant kernel
+    # the roofline of the dominant kernel (HBM: compulsory bytes; the quad
+    # forms and the scatter at large D are gathers of whole point rows, so
+    # they are bound by memory, not by the tensor pipe)
     dom = max(durations, key=durations.get)
     ab = alg_bytes(N, D, nnz)
     peak, peak_kind = load_peaks()
     achieved = ab[dom] / (durations[dom] * 1e-3) / 1e9
     traffic = load_traffic(dom, args.workload)
+    tflops = {k_: alg_flops(N, D, nnz).get(k_, 0) / (v * 1e-3) / 1e12 for k_, v in durations.items()}
+
+    # plain FP32 against mixed precision: the same number of iterations from the
+    # same saved state, timed the same way (large D only)
+    plain = None
+    if D > 8 and eng.precision == "mixed":
+        n_cmp = max(3, args.steps // 2)
+        lpd = {}
+        ms = {}
+        for prec in ("mixed", "fp32"):
+            eng.restore(snap)
+            eng.precision = prec
+            ms[prec] = timed_steps(eng, n_cmp, flush, torch) / n_cmp
+            lpd[prec] = model.log_pred_density(X, Y).double()
+        plain_split = kernel_split(eng, 3, flush, torch)
+        eng.precision = "mixed"
+        plain = {
+            "value": 1000.0 / ms["fp32"], "unit": "VI iters/s", "ms_per_step": ms["fp32"],
+            "kernel_ms": {k_: round(v, 4) for k_, v in plain_split.items()},
+            "mixed_speedup": ms["fp32"] / ms["mixed"],
+            "held_out_mean_log_density": {
+                "iterations_from_same_state": n_cmp,
+                "mixed": float(lpd["mixed"].mean()), "plain_fp32": float(lpd["fp32"].mean()),
+                "abs_diff_nats": float((lpd["mixed"].mean() - lpd["fp32"].mean()).abs()),
+                "max_abs_diff_per_query": float((lpd["mixed"] - lpd["fp32"]).abs().max()),
+            },
+        }
 
     # log_pred_density throughput (queries resident in HBM)
     for _ in range(2):
@@ -402,7 +456,8 @@ def main():
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic",
-            "precision": "fp32 (plain FP32 GPU kernels; FP64 factorisations)",
+            "precision": (f"{eng.precision} (FP64 factorisations)" if D > 8 else
+                          "fp32 (plain FP32 GPU kernels; FP64 factorisations)"),
             "config": {
                 "workload": f"{args.workload}: {desc}",
                 "schedule": "fused batch VI (block_size=N) on the kNN candidate pattern",
@@ -423,7 +478,9 @@ def main():
                 "peak_source": f"{peak_kind} hbm_gbs",
                 "alg_bytes_per_launch": ab[dom],
                 "kernel_ms": {k_: round(v, 5) for k_, v in durations.items()},
+                "kernel_alg_tflops": {k_: round(v, 3) for k_, v in tflops.items()},
             },
+            "plain_fp32": plain,
             "log_pred_density": {"value": lpd_pts, "unit": "pts/s", "ms": lpd_ms, "queries": len(Xte),
                                  "kernels": N, "mean_log_density": float(lpd.mean())},
             "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "VI iters/s", "h2d_bytes_per_step": X.numel() * 4,

@@ -181,6 +181,46 @@ LAKDE_API int lakde_vi_rows(int dtype, int64_t N, int64_t D, int64_t npts,
                             int32_t *info, void *logrho, void *stream);
 
 /*
+ * The same per-kernel pass as lakde_vi_rows for 8 < D <= 64 (float32 values),
+ * one CTA per kernel row: differences gathered once per chunk of 128 pairs
+ * into shared memory, M-step by 4x4 register blocks, FP64 Cholesky, inverse
+ * and trace in shared memory, E-step quad forms against the packed W_triu.
+ */
+LAKDE_API int lakde_vi_cta(int dtype, int64_t N, int64_t D, int64_t npts,
+                           const void *rowptr, const void *col,
+                           const void *order, const void *r, const void *X,
+                           double nu_0, const void *P, int64_t P_batch_stride,
+                           const void *T, int64_t T_batch_stride, const void *a,
+                           void *b, double b_0, void *jitter, double eps,
+                           void *nu, void *logdet_W, void *mm, int32_t *info,
+                           void *logrho, void *stream);
+
+/*
+ * Mixed-precision tensor-core E-step (tcgen05, bf16 hi + lo split, fp32
+ * accumulation in tensor memory), D <= 64, float32 values: the logrho of
+ * lakde_estep_logrho for kernels 0..N-1 of X (no kernel offset), rows visited in
+ * `order` (may be NULL).  *err is set to 1 if a tensor-core completion wait
+ * times out (the affected rows are left unwritten).
+ */
+LAKDE_API int lakde_estep_tc(int dtype, int64_t N, int64_t D, int64_t npts,
+                             const void *rowptr, const void *col,
+                             const void *order, const void *X,
+                             const void *W_triu, const void *nu,
+                             const void *logdet_W, void *logrho, int32_t *err,
+                             void *stream);
+
+/*
+ * Mixed-precision tensor-core M-step (tcgen05): S_n and nu_n of lakde_mstep
+ * for kernels 0..N-1 of X, D <= 64, float32 values (S is symmetric up to the
+ * order of the fp32 accumulation).  *err as in lakde_estep_tc.
+ */
+LAKDE_API int lakde_mstep_tc(int dtype, int64_t N, int64_t D, int64_t npts,
+                             const void *rowptr, const void *col,
+                             const void *order, const void *r, const void *X,
+                             double nu_0, void *S, void *nu, int32_t *err,
+                             void *stream);
+
+/*
  * Per-point normaliser, responsibilities and rebalance over a pair pattern
  * given point-major: pairs of point m are pos[cptr[m] .. cptr[m+1]) (indices
  * into logrho / r).  mode 0 (initial pass): c_m = logsumexp_n logrho.

@@ -36,13 +36,11 @@ __global__ void __launch_bounds__(128) estep_logrho_kernel(const RP *__restrict_
   load_tri<T, DP>(sU, W + n * (int64_t)D * D, D, 1, D, true, lane, 32);
   const int64_t self = n + koff;
   for (int d = lane; d < DP; d += 32) sxn[d] = (d < D && self < npts) ? X[self * D + d] : T(0);
-  T cst = T(0);
-  if (lane == 0) {
-    const T nv = nu[n];
-    const double e = mvdigamma_d(0.5 * (double)nv, D) + D * 0.69314718055994530942 + (double)logdet[n];
-    cst = (T)(0.5 * e);
-  }
-  cst = __shfl_sync(0xffffffffu, cst, 0);
+  // multivariate digamma, one term per lane
+  double md = 0.0;
+  for (int i = 1 + lane; i <= D; i += 32) md += digamma_d(0.5 * (double)nu[n] + 0.5 * (1 - i));
+  md = warp_sum(md);
+  const T cst = (T)(0.5 * (md + D * 0.69314718055994530942 + (double)logdet[n]));
   const T expo = T(-0.5) * nu[n];
   __syncwarp();
   const int64_t start = (int64_t)rowptr[n], end = (int64_t)rowptr[n + 1];

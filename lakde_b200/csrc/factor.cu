@@ -5,10 +5,12 @@
 // term ||T_n^T W_triu_n||_F^2 (lakde/linalg_util.py:30-37).
 //
 // D <= 8: one thread per matrix, everything in registers.
-// D in (8, 64]: one warp per matrix, the matrix in shared memory (FP64),
-// right-looking column Cholesky with the trailing update spread over lanes by
-// row, then per-lane forward substitution for the inverse (lanes own columns).
+// D in (8, 64]: one warp per matrix on the FP64 tensor cores (mma.sync
+// m8n8k4 f64): blocked right-looking Cholesky over 8 x 8 lower tiles in shared
+// memory, in-place blocked triangular inverse, trace by tile products
+// (factor_dmma.cuh).
 #include "common.cuh"
+#include "factor_dmma.cuh"
 
 namespace lakde {
 
@@ -163,81 +165,60 @@ __global__ void __launch_bounds__(128) factor_thread_kernel(FactorArgs<T> g) {
   }
 }
 
-// ------------------------------ warp per matrix ----------------------------
+// ------------------------- warp per matrix, FP64 tensor cores --------------
 template <int DP>
-struct WarpFactorCfg {
-  static constexpr int WPB = DP <= 32 ? 4 : (DP <= 48 ? 2 : 1);
-  static constexpr int LDM = DP + 1;
-  static constexpr int per_warp = DP * LDM + DP;
+struct DmmaCfg {
+  static constexpr int NT = DP / 8;
+  static constexpr int NTILE = NT * (NT + 1) / 2;
+  static constexpr int WPB = DP >= 48 ? 2 : 4;
+  static constexpr int per_warp = NTILE * 64 + 64 + DP + NT * 64;  // tiles, scratch, diag(L), T column block
   static constexpr size_t smem = (size_t)WPB * per_warp * sizeof(double);
 };
 
 template <typename T, int DP>
-__device__ __forceinline__ void assemble_warp(const FactorArgs<T> &g, int64_t n, T scale, T jit, double *sm,
-                                              int lane) {
-  constexpr int LDM = WarpFactorCfg<DP>::LDM;
-  const int D = g.D;
-  for (int e = lane; e < D * D; e += 32) {
-    const int i = e / D, j = e % D;
-    if (j <= i) sm[i * LDM + j] = assembled(g, n, scale, i, j, jit);
-  }
-  __syncwarp();
-}
-
-template <int DP>
-__device__ __forceinline__ bool factor_warp(double *sm, int D, int lane) {
-  constexpr int LDM = WarpFactorCfg<DP>::LDM;
-  for (int k = 0; k < D; ++k) {
-    const double piv = sm[k * LDM + k];
-    __syncwarp();
-    if (!(piv > 0.0)) return false;
-    const double lkk = sqrt(piv);
-    const double r = 1.0 / lkk;
-    if (lane == 0) sm[k * LDM + k] = lkk;
-    for (int i = k + 1 + lane; i < D; i += 32) sm[i * LDM + k] *= r;
-    __syncwarp();
-    for (int i = k + 1 + lane; i < D; i += 32) {
-      const double lik = sm[i * LDM + k];
-      for (int j = k + 1; j <= i; ++j) sm[i * LDM + j] -= lik * sm[j * LDM + k];
-    }
-    __syncwarp();
-  }
-  return true;
-}
-
-template <typename T, int DP>
-__global__ void factor_warp_kernel(FactorArgs<T> g) {
-  using C = WarpFactorCfg<DP>;
-  constexpr int LDM = C::LDM;
+__global__ void __launch_bounds__(128) factor_dmma_kernel(FactorArgs<T> g) {
+  using C = DmmaCfg<DP>;
+  constexpr int NT = C::NT;
   extern __shared__ double smem_d[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t n = (int64_t)blockIdx.x * C::WPB + warp;
   if (n >= g.N) return;
-  double *sm = smem_d + warp * C::per_warp;
-  double *dinv = sm + DP * LDM;
+  double *M = smem_d + warp * C::per_warp;
+  double *scratch = M + C::NTILE * 64;
+  double *ldiag = scratch + 64;
+  double *tcol = ldiag + DP;  // one 8-column block of T_n, NT tiles
   const int D = g.D;
   const T scale = posterior_scale(g, n);
   T jit = g.jitter[n];
-  assemble_warp<T, DP>(g, n, scale, jit, sm, lane);
-  bool ok = factor_warp<DP>(sm, D, lane);
-  if (!ok) {
-    T jt = T(0);
-    for (int k = 0; k < 32 && !ok; ++k) {
-      jt = add_rn(jt, (T)(g.eps * ldexp(1.0, k)));
-      assemble_warp<T, DP>(g, n, scale, jt, sm, lane);
-      ok = factor_warp<DP>(sm, D, lane);
-      if (ok) jit = jt;
+  T *lout = g.L ? g.L + n * (int64_t)D * D : nullptr;
+  bool ok = false;
+  for (int attempt = 0; attempt <= 32 && !ok; ++attempt) {
+    T jt = jit;
+    if (attempt > 0) {
+      jt = T(0);
+      for (int k = 0; k < attempt; ++k) jt = add_rn(jt, (T)(g.eps * ldexp(1.0, k)));
     }
+    for (int e = lane; e < DP * DP; e += 32) {
+      const int i = e / DP, j = e % DP;
+      if (j > i) continue;
+      const double v = (i < D) ? assembled(g, n, scale, i, j, jt) : (i == j ? 1.0 : 0.0);
+      M[dmma::tix(i >> 3, j >> 3) + (i & 7) * 8 + (j & 7)] = v;
+    }
+    __syncwarp();
+    ok = dmma::chol_blocked<T>(M, scratch, ldiag, NT, lane, lout, D);
+    if (ok) jit = jt;
+    __syncwarp();
   }
   if (lane == 0) {
     g.jitter[n] = jit;
     g.info[n] = ok ? 0 : -1;
   }
   const T nanv = T(NAN);
+  T *W = g.W + n * (int64_t)D * D;
   if (!ok) {
     for (int e = lane; e < D * D; e += 32) {
-      g.W[n * (int64_t)D * D + e] = nanv;
-      if (g.L) g.L[n * (int64_t)D * D + e] = nanv;
+      W[e] = nanv;
+      if (lout) lout[e] = nanv;
     }
     if (lane == 0) {
       g.logdet[n] = nanv;
@@ -245,50 +226,52 @@ __global__ void factor_warp_kernel(FactorArgs<T> g) {
     }
     return;
   }
-  // inverse: lane owns columns c = lane, lane + 32; Linv[i][c] is stored
-  // transposed in the strict upper triangle (sm[c][i]) and the diagonal in dinv.
-  for (int c = lane; c < D; c += 32) dinv[c] = 1.0 / sm[c * LDM + c];
-  __syncwarp();
-  const int c0 = lane, c1 = lane + 32;
-  for (int i = 1; i < D; ++i) {
-    double s0 = 0.0, s1 = 0.0;
-    for (int k = 0; k < i; ++k) {
-      const double lik = sm[i * LDM + k];
-      if (c0 <= k) s0 += lik * (k == c0 ? dinv[c0] : sm[c0 * LDM + k]);
-      if (c1 < D && c1 <= k) s1 += lik * (k == c1 ? dinv[c1] : sm[c1 * LDM + k]);
-    }
-    if (c0 < i) sm[c0 * LDM + i] = -s0 * dinv[i];
-    if (c1 < i) sm[c1 * LDM + i] = -s1 * dinv[i];
-  }
-  __syncwarp();
-  T *W = g.W + n * (int64_t)D * D;
-  for (int e = lane; e < D * D; e += 32) {
-    const int r = e / D, c = e % D;
-    const double u = r < c ? sm[r * LDM + c] : (r == c ? dinv[r] : 0.0);
-    W[e] = (T)u;
-  }
-  if (g.L) {
-    T *Lo = g.L + n * (int64_t)D * D;
+  if (lout) {
+    // the factor's strictly upper blocks are not touched by the tile loops
     for (int e = lane; e < D * D; e += 32) {
       const int r = e / D, c = e % D;
-      Lo[e] = (T)(r >= c ? sm[r * LDM + c] : 0.0);
+      if ((c >> 3) > (r >> 3)) lout[e] = T(0);
     }
   }
+  dmma::trtri_blocked(M, scratch, NT, lane);
+  // W_triu = X^T (upper): W[r][c] = X[c][r], r <= c
+  for (int e = lane; e < D * D; e += 32) {
+    const int r = e / D, c = e % D;
+    const double v = (r <= c) ? M[dmma::tix(c >> 3, r >> 3) + (c & 7) * 8 + (r & 7)] : 0.0;
+    W[e] = (T)v;
+  }
   double ld = 0.0;
-  for (int i = lane; i < D; i += 32) ld += log((double)(T)dinv[i]);
+  for (int i = lane; i < D; i += 32) ld += log((double)(T)(1.0 / ldiag[i]));
   ld = warp_sum(ld);
   if (lane == 0) g.logdet[n] = (T)(2.0 * ld);
   if (g.Tm) {
-    const T *Tm = g.Tm + n * g.Tbs;
+    // ||X T_n||_F^2 with X lower: (X T)_IA = sum_{K <= I} X_IK T_KA.  Each
+    // 8-column block A of T_n is staged in shared memory (coalesced rows) and
+    // its all-zero 8 x 8 tiles (the upper part of a triangular T) are skipped.
+    const T *Tn = g.Tm + n * g.Tbs;
     double acc = 0.0;
-    for (int a = lane; a < D; a += 32) {
-      for (int bcol = 0; bcol < D; ++bcol) {
-        double s = 0.0;
-        for (int k = 0; k <= bcol; ++k) {
-          const double u = k < bcol ? sm[k * LDM + bcol] : dinv[bcol];
-          s += (double)Tm[k * D + a] * u;
+    for (int Ac = 0; Ac < NT; ++Ac) {
+      __syncwarp();
+      for (int e = lane; e < NT * 64; e += 32) {
+        const int row = e >> 3, col = 8 * Ac + (e & 7);
+        tcol[e] = (row < D && col < D) ? (double)Tn[row * D + col] : 0.0;
+      }
+      __syncwarp();
+      unsigned nonzero = 0;  // bit K: tile K of this column block has a non-zero
+      for (int K = 0; K < NT; ++K) {
+        const bool nz = tcol[K * 64 + lane] != 0.0 || tcol[K * 64 + 32 + lane] != 0.0;
+        if (__any_sync(0xffffffffu, nz)) nonzero |= 1u << K;
+      }
+      for (int I = 0; I < NT; ++I) {
+        double c0 = 0.0, c1 = 0.0;
+        for (int K = 0; K <= I; ++K) {
+          if (!((nonzero >> K) & 1u)) continue;
+          const double *x = M + dmma::tix(I, K);
+          const double *tk = tcol + K * 64;
+#pragma unroll
+          for (int s = 0; s < 2; ++s) dmma::mma(c0, c1, dmma::afrag(x, s, lane), dmma::bfrag(tk, s, lane));
         }
-        acc += s * s;
+        acc += c0 * c0 + c1 * c1;
       }
     }
     acc = warp_sum(acc);
@@ -346,8 +329,8 @@ extern "C" int lakde_posterior_factor(int dtype, int64_t N, int64_t D, const voi
       if constexpr (DP <= 8) {
         factor_thread_kernel<TT, DP><<<(unsigned)((N + 127) / 128), 128, 0, as_stream(stream)>>>(g);
       } else {
-        using C = WarpFactorCfg<DP>;
-        auto kern = factor_warp_kernel<TT, DP>;
+        using C = DmmaCfg<DP>;
+        auto kern = factor_dmma_kernel<TT, DP>;
         if (C::smem > 48 * 1024) {
           cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
           if (e != cudaSuccess) {

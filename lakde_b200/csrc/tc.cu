@@ -1,0 +1,570 @@
+// Mixed-precision tensor-core (tcgen05) kernels of the large-D VI path.
+//
+// Grouping pairs by kernel makes two dense contractions per kernel row n with
+// m_n pairs, Delta = [x_m - x_n] (m_n x D):
+//   E-step  Y = Delta W_triu_n          (m_n x D), Q_p = |Y_p|^2   (lakde/local_adaptive_kde.py:36-44)
+//   M-step  S_n = G^T G, G = sqrt(r) Delta                          (lakde/local_adaptive_kde.py:66-81)
+// Both run as tcgen05.mma kind::f16 on bf16 operands with fp32 accumulation in
+// tensor memory.  A split x = hi + lo (hi = bf16(x), lo = bf16(x - hi)) keeps
+// ~16 significant bits: each product is hi*hi + lo*hi + hi*lo.  The
+// differences are centred on the kernel in fp32 before the split, so the
+// cancellation near each kernel centre happens in fp32, not in bf16.
+//
+// Operands are staged by the CTA's threads into shared memory in the canonical
+// no-swizzle core-matrix layout (8 rows x 16 bytes per core matrix).  One
+// thread issues the MMAs; completion is signalled through an mbarrier whose
+// waits are bounded (on timeout the kernel raises an error flag and stops).
+// D is padded to 64 (zero rows and columns).
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+
+namespace lakde {
+namespace tc {
+
+constexpr int DP = 64;       // padded dimension
+constexpr int KG = DP / 8;   // 8-element groups along D
+constexpr int MT = 128;      // pairs per tile (MMA M for the E-step)
+constexpr uint32_t kSpinLimit = 1u << 24;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor: no swizzle, version 1 (sm_100).
+__device__ __forceinline__ uint64_t desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+
+// Instruction descriptor, kind::f16: bf16 x bf16 -> f32, M x N, operand majors.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, int a_mn_major, int b_mn_major) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn_major << 15) | ((uint32_t)b_mn_major << 16) |
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void commit(uint64_t *mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *mbar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity) {
+  const uint32_t addr = smem_u32(mbar);
+  for (uint32_t it = 0; it < kSpinLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_alloc(uint32_t *slot, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)), "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// 16 consecutive fp32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// hi = bf16(x), lo = bf16(x - hi), packed pairwise
+__device__ __forceinline__ void split2(float x0, float x1, uint32_t &hi, uint32_t &lo) {
+  const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
+  const __nv_bfloat16 l0 = __float2bfloat16_rn(x0 - __bfloat162float(h0));
+  const __nv_bfloat16 l1 = __float2bfloat16_rn(x1 - __bfloat162float(h1));
+  hi = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+  lo = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+}
+
+// byte offset of element (row, d) of a [rows x DP] bf16 operand in core-matrix
+// layout with the 8-row groups `rstride` bytes apart and the 8-column groups
+// 128 bytes apart:  core (row / 8, d / 8) + 16 (row % 8) + 2 (d % 8)
+__device__ __forceinline__ uint32_t core_off(int row, int d, uint32_t rstride) {
+  return (uint32_t)(row >> 3) * rstride + (uint32_t)(d >> 3) * 128u + (uint32_t)(row & 7) * 16u + (uint32_t)(d & 7) * 2u;
+}
+
+struct TcArgs {
+  const int64_t *rowptr;
+  const int32_t *col;
+  const int32_t *order;
+  const float *r;
+  const float *X;
+  const float *W;       // W_triu [N, D, D]
+  const float *nu;      // E-step: per-kernel nu
+  const float *logdet;  // E-step
+  float *logrho;        // E-step output
+  float *S;             // M-step output [N, D, D]
+  float *nu_out;        // M-step output
+  float nu0;
+  int64_t npts;
+  int64_t N;
+  int D;
+  int *err;
+};
+
+// --------------------------------------------------------------------- E-step
+// smem: A_hi, A_lo [MT x DP] (K-major: pair rows), B_hi, B_lo [DP x DP] (MN-major:
+// rows of W_triu), cidx[MT], mbarrier, tmem slot.
+struct EsmCfg {
+  static constexpr uint32_t A_BYTES = MT * DP * 2;   // 16 KB
+  static constexpr uint32_t B_BYTES = DP * DP * 2;   // 8 KB
+  static constexpr uint32_t off_Ahi = 0, off_Alo = A_BYTES, off_Bhi = 2 * A_BYTES, off_Blo = 2 * A_BYTES + B_BYTES;
+  static constexpr uint32_t off_c = 2 * A_BYTES + 2 * B_BYTES;
+  static constexpr uint32_t bytes = off_c + MT * 4 + 128;
+};
+
+__global__ void __launch_bounds__(128) estep_tc_kernel(TcArgs g) {
+  using C = EsmCfg;
+  extern __shared__ __align__(128) unsigned char sm[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t s_tmem;
+  __shared__ float s_cst, s_expo;
+  __shared__ float s_xn[DP];
+  unsigned char *Ahi = sm + C::off_Ahi, *Alo = sm + C::off_Alo, *Bhi = sm + C::off_Bhi, *Blo = sm + C::off_Blo;
+  int32_t *cidx = reinterpret_cast<int32_t *>(sm + C::off_c);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int D = g.D;
+
+  if (warp == 0) tmem_alloc(&s_tmem, 64);
+  if (tid == 0) mbar_init(&mbar);
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = s_tmem;
+  uint32_t phase = 0;
+  bool alive = true;
+
+  // A: K-major, pair groups 8 * 128 bytes apart (SBO), K groups 128 bytes apart (LBO)
+  // B: MN-major, N groups 128 bytes apart (SBO), K groups 8 * 128 bytes apart (LBO)
+  constexpr uint32_t A_SBO = KG * 128, A_LBO = 128;
+  constexpr uint32_t B_SBO = 128, B_LBO = KG * 128;
+  const uint32_t idesc = idesc_bf16(MT, DP, 0, 1);
+
+  for (int64_t it = blockIdx.x; it < g.N && alive; it += gridDim.x) {
+    const int64_t n = g.order ? (int64_t)g.order[it] : it;
+    const int64_t start = g.rowptr[n], end = g.rowptr[n + 1];
+    // stage W_triu[n] (rows j, columns i) as B = [K = j][N = i], hi and lo
+    const float *Wn = g.W + n * (int64_t)D * D;
+    // lane -> row j = 8 jg + lane / 4, columns i = 8 ig + 2 (lane % 4), + 1 (bank-conflict-free stores)
+    for (int e = tid; e < DP * DP / 2; e += 128) {
+      const int q = e >> 5, ln = e & 31;  // q: (jg, ig) block of 8 x 8
+      const int j = 8 * (q / KG) + (ln >> 2), i = 8 * (q % KG) + 2 * (ln & 3);
+      const float w0 = (j < D && i < D) ? Wn[j * D + i] : 0.f;
+      const float w1 = (j < D && i + 1 < D) ? Wn[j * D + i + 1] : 0.f;
+      uint32_t hi, lo;
+      split2(w0, w1, hi, lo);
+      // B is MN-major: core (k group j/8, n group i/8), 16-byte line = row j of 8 n's
+      const uint32_t o = (uint32_t)(j >> 3) * B_LBO + (uint32_t)(i >> 3) * B_SBO + (uint32_t)(j & 7) * 16u +
+                         (uint32_t)(i & 7) * 2u;
+      *reinterpret_cast<uint32_t *>(Bhi + o) = hi;
+      *reinterpret_cast<uint32_t *>(Blo + o) = lo;
+    }
+    for (int d = tid; d < DP; d += 128) s_xn[d] = d < D ? g.X[n * D + d] : 0.f;
+    if (warp == 0) {
+      // multivariate digamma, one term per lane
+      const float nv = g.nu[n];
+      double md = 0.0;
+      for (int i = 1 + (tid & 31); i <= D; i += 32) md += digamma_d(0.5 * (double)nv + 0.5 * (1 - i));
+      md = warp_sum(md);
+      if (tid == 0) {
+        s_cst = (float)(0.5 * (md + D * 0.69314718055994530942 + (double)g.logdet[n]));
+        s_expo = -0.5f * nv;
+      }
+    }
+    __syncthreads();
+    for (int64_t base = start; base < end; base += MT) {
+      const int cnt = (int)((end - base) < MT ? (end - base) : MT);
+      // gather: warp w takes the 8-row batches w, w + 4, ...; lane l the row
+      // 8 b + l / 4 and, for each 8-dimension group k, dimensions 8 k + 2 (l % 4)
+      // and + 1.  Every store instruction then covers 8 rows of one core-matrix
+      // column (32 distinct banks) and every load 8 whole 32-byte sectors.
+      for (int bt = warp; bt < MT / 8; bt += 4) {
+        const int p = 8 * bt + (lane >> 2);
+        int32_t c = -1;
+        if (p < cnt) {
+          c = g.col[base + p];
+          if (c < 0 || c >= g.npts) c = -1;
+        }
+        if ((lane & 3) == 0) cidx[p] = c;
+        const float *xm = g.X + (int64_t)(c < 0 ? 0 : c) * D;
+        float v[KG][2];
+#pragma unroll
+        for (int k = 0; k < KG; ++k) {
+          const int d0 = 8 * k + 2 * (lane & 3);
+          v[k][0] = (c >= 0 && d0 < D) ? xm[d0] : 0.f;
+          v[k][1] = (c >= 0 && d0 + 1 < D) ? xm[d0 + 1] : 0.f;
+        }
+#pragma unroll
+        for (int k = 0; k < KG; ++k) {
+          const int d0 = 8 * k + 2 * (lane & 3);
+          const float x0 = (c >= 0 && d0 < D) ? v[k][0] - s_xn[d0] : 0.f;
+          const float x1 = (c >= 0 && d0 + 1 < D) ? v[k][1] - s_xn[d0 + 1] : 0.f;
+          uint32_t hi, lo;
+          split2(x0, x1, hi, lo);
+          const uint32_t o = core_off(p, d0, A_SBO);
+          *reinterpret_cast<uint32_t *>(Ahi + o) = hi;
+          *reinterpret_cast<uint32_t *>(Alo + o) = lo;
+        }
+      }
+      fence_async_smem();
+      fence_before();
+      __syncthreads();
+      if (tid == 0) {
+        fence_after();
+        const uint32_t ahi = smem_u32(Ahi), alo = smem_u32(Alo), bhi = smem_u32(Bhi), blo = smem_u32(Blo);
+#pragma unroll
+        for (int s = 0; s < DP / 16; ++s) {
+          const uint32_t ao = 2 * s * A_LBO, bo = 2 * s * B_LBO;
+          mma(tmem, desc(ahi + ao, A_LBO, A_SBO), desc(bhi + bo, B_LBO, B_SBO), idesc, s > 0);
+          mma(tmem, desc(alo + ao, A_LBO, A_SBO), desc(bhi + bo, B_LBO, B_SBO), idesc, 1);
+          mma(tmem, desc(ahi + ao, A_LBO, A_SBO), desc(blo + bo, B_LBO, B_SBO), idesc, 1);
+        }
+        commit(&mbar);
+      }
+      // the outcome is made uniform across the CTA: the TMEM loads below are
+      // warp-collective
+      const bool ok = __syncthreads_and(mbar_wait(&mbar, phase) ? 1 : 0) != 0;
+      phase ^= 1;
+      fence_after();
+      if (!ok) {
+        if (tid == 0) atomicExch(g.err, 1);
+        alive = false;
+      }
+      // epilogue: lane = pair row
+      float q = 0.f;
+      if (ok) {
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+        for (int c0 = 0; c0 < DP; c0 += 16) {
+          float v[16];
+          tmem_ld16(taddr + c0, v);
+#pragma unroll
+          for (int k = 0; k < 16; ++k) q = fmaf(v[k], v[k], q);
+        }
+      }
+      if (tid < cnt) {
+        const int32_t c = cidx[tid];
+        float lr = NAN;
+        if (ok && c >= 0) {
+          lr = __fadd_rn(__fmul_rn(q, s_expo), s_cst);
+          if ((int64_t)c == n) lr = -INFINITY;
+        }
+        g.logrho[base + tid] = lr;
+      }
+      fence_before();
+      __syncthreads();
+      if (!ok) break;
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  fence_after();
+  if (warp == 0) tmem_dealloc(tmem, 64);
+}
+
+// --------------------------------------------------------------------- M-step
+// smem: G = [MT pairs x (hi | lo) 2 DP] bf16 (core rows of 16 groups),
+// reduction buffer [DP x DP] fp32 reusing G after the MMAs, mbarrier, slot.
+struct MsmCfg {
+  static constexpr uint32_t G_BYTES = MT * 2 * DP * 2;  // 32 KB
+  static constexpr uint32_t bytes = G_BYTES + 128;
+};
+
+__global__ void __launch_bounds__(128) mstep_tc_kernel(TcArgs g) {
+  using C = MsmCfg;
+  extern __shared__ __align__(128) unsigned char sm[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t s_tmem;
+  __shared__ float s_xn[DP];
+  __shared__ float s_rs[4];
+  unsigned char *G = sm;
+  float *red = reinterpret_cast<float *>(sm);  // [DP][DP + 1] after the MMAs
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int D = g.D;
+
+  if (warp == 0) tmem_alloc(&s_tmem, 128);
+  if (tid == 0) mbar_init(&mbar);
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = s_tmem;
+  uint32_t phase = 0;
+  bool alive = true;
+
+  // G rows are pairs: core (pair group, dim group 0..15), dim groups 0-7 hi, 8-15 lo.
+  // As A = [G_hi^T; G_lo^T] (M = 128 dims, K = pairs) and B = G_hi or G_lo
+  // (K = pairs, N = 64 dims) both are MN-major: MN groups 128 bytes apart (SBO),
+  // K (pair) groups 16 * 128 bytes apart (LBO).
+  constexpr uint32_t RS = 2 * KG * 128;  // pair-group stride
+  constexpr uint32_t SBO = 128, LBO = RS;
+  const uint32_t idesc = idesc_bf16(128, DP, 1, 1);
+
+  for (int64_t it = blockIdx.x; it < g.N && alive; it += gridDim.x) {
+    const int64_t n = g.order ? (int64_t)g.order[it] : it;
+    const int64_t start = g.rowptr[n], end = g.rowptr[n + 1];
+    for (int d = tid; d < DP; d += 128) s_xn[d] = d < D ? g.X[n * D + d] : 0.f;
+    __syncthreads();
+    float rsum = 0.f;
+    bool bad = end < start;
+    int ntile = 0;
+    for (int64_t base = start; base < end; base += MT, ++ntile) {
+      const int cnt = (int)((end - base) < MT ? (end - base) : MT);
+      // gather: as in the E-step, warp w takes the 8-row batches w, w + 4, ...;
+      // lane l the row 8 b + l / 4 and the dimension pairs 8 k + 2 (l % 4)
+      for (int bt = warp; bt < MT / 8; bt += 4) {
+        const int p = 8 * bt + (lane >> 2);
+        int32_t c = -1;
+        float rv = 0.f;
+        if (p < cnt) {
+          c = g.col[base + p];
+          rv = g.r[base + p];
+          if (c < 0 || c >= g.npts) {
+            bad = true;
+            c = -1;
+            rv = 0.f;
+          }
+        }
+        if ((lane & 3) == 0) rsum += rv;
+        const float w = sqrtf(rv > 0.f ? rv : 0.f);
+        const float *xm = g.X + (int64_t)(c < 0 ? 0 : c) * D;
+        float v[KG][2];
+#pragma unroll
+        for (int k = 0; k < KG; ++k) {
+          const int d0 = 8 * k + 2 * (lane & 3);
+          v[k][0] = (c >= 0 && d0 < D) ? xm[d0] : 0.f;
+          v[k][1] = (c >= 0 && d0 + 1 < D) ? xm[d0 + 1] : 0.f;
+        }
+#pragma unroll
+        for (int k = 0; k < KG; ++k) {
+          const int d0 = 8 * k + 2 * (lane & 3);
+          const float x0 = (c >= 0 && d0 < D) ? w * (v[k][0] - s_xn[d0]) : 0.f;
+          const float x1 = (c >= 0 && d0 + 1 < D) ? w * (v[k][1] - s_xn[d0 + 1]) : 0.f;
+          uint32_t hi, lo;
+          split2(x0, x1, hi, lo);
+          *reinterpret_cast<uint32_t *>(G + core_off(p, d0, RS)) = hi;
+          *reinterpret_cast<uint32_t *>(G + core_off(p, d0 + DP, RS)) = lo;
+        }
+      }
+      fence_async_smem();
+      fence_before();
+      __syncthreads();
+      if (tid == 0) {
+        fence_after();
+        const uint32_t g0 = smem_u32(G);
+#pragma unroll
+        for (int s = 0; s < MT / 16; ++s) {
+          const uint32_t ko = 2 * s * LBO;
+          const uint32_t acc = (ntile > 0 || s > 0) ? 1u : 0u;
+          // D1 += [G_hi; G_lo]^T G_hi, D2 += [G_hi; G_lo]^T G_lo
+          mma(tmem, desc(g0 + ko, LBO, SBO), desc(g0 + ko, LBO, SBO), idesc, acc);
+          mma(tmem + 64, desc(g0 + ko, LBO, SBO), desc(g0 + ko + KG * 128, LBO, SBO), idesc, acc);
+        }
+        commit(&mbar);
+      }
+      const bool ok = __syncthreads_and(mbar_wait(&mbar, phase) ? 1 : 0) != 0;
+      phase ^= 1;
+      fence_after();
+      if (!ok) {
+        if (tid == 0) atomicExch(g.err, 1);
+        alive = false;
+        break;
+      }
+      fence_before();
+      __syncthreads();
+    }
+    if (!alive) break;
+    // nu = nu0 + sum r (pairs in CSR order within warps, then warps)
+    rsum = warp_sum(rsum);
+    const bool any_bad = __syncthreads_or(bad ? 1 : 0);
+    if (lane == 0) s_rs[warp] = rsum;
+    // S = D1[0:64] + D1[64:128] + D2[0:64]; rows 64..127 go through shared memory
+    float v1[16], v2[16];
+    const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+    if (end > start) {
+      if (warp >= 2) {
+        const int i = tid - 64;
+#pragma unroll
+        for (int c0 = 0; c0 < DP; c0 += 16) {
+          tmem_ld16(taddr + c0, v1);
+#pragma unroll
+          for (int k = 0; k < 16; ++k) red[i * (DP + 1) + c0 + k] = v1[k];
+        }
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      const float nv = g.nu0 + (s_rs[0] + s_rs[1] + s_rs[2] + s_rs[3]);
+      g.nu_out[n] = any_bad ? NAN : nv;
+    }
+    if (warp < 2) {
+      const int i = tid;
+      float *Srow = g.S + n * (int64_t)D * D + (int64_t)i * D;
+#pragma unroll
+      for (int c0 = 0; c0 < DP; c0 += 16) {
+        if (end > start) {
+          tmem_ld16(taddr + c0, v1);
+          tmem_ld16(taddr + 64 + c0, v2);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 16; ++k) v1[k] = v2[k] = 0.f;
+        }
+        if (i < D) {
+#pragma unroll
+          for (int k = 0; k < 16; ++k) {
+            const int j = c0 + k;
+            const float s = (end > start) ? v1[k] + red[i * (DP + 1) + j] + v2[k] : 0.f;
+            if (j < D) Srow[j] = any_bad ? NAN : s;
+          }
+        }
+      }
+    }
+    fence_before();
+    __syncthreads();
+  }
+  __syncthreads();
+  fence_after();
+  if (warp == 0) tmem_dealloc(tmem, 128);
+}
+
+}  // namespace tc
+}  // namespace lakde
+
+using namespace lakde;
+
+static int tc_common_checks(const char *what, int dtype, int64_t N, int64_t D, int64_t npts) {
+  if (dtype != LAKDE_F32) {
+    set_error("%s: float32 values only", what);
+    return LAKDE_EDTYPE;
+  }
+  if (N < 0 || D < 1 || npts < N) {
+    set_error("%s: invalid sizes", what);
+    return LAKDE_EINVAL;
+  }
+  if (D > 64) {
+    set_error("%s: D=%lld exceeds 64", what, (long long)D);
+    return LAKDE_EUNSUPPORTED;
+  }
+  return LAKDE_OK;
+}
+
+// Persistent grid: CTAs per SM limited by shared memory (228 KB per SM, 1 KB
+// reserved per CTA) and tensor memory (512 columns per SM).
+static int tc_grid(size_t smem, int tmem_cols, int64_t N, unsigned *grid) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
+  int per_sm = (int)((228u * 1024u) / (smem + 1024u + 512u));
+  if (per_sm > 512 / tmem_cols) per_sm = 512 / tmem_cols;
+  if (per_sm > 8) per_sm = 8;
+  if (per_sm < 1) per_sm = 1;
+  int64_t g = (int64_t)sms * per_sm;
+  if (g > N) g = N;
+  *grid = (unsigned)(g < 1 ? 1 : g);
+  return LAKDE_OK;
+}
+
+extern "C" int lakde_estep_tc(int dtype, int64_t N, int64_t D, int64_t npts, const void *rowptr, const void *col,
+                              const void *order, const void *X, const void *W_triu, const void *nu,
+                              const void *logdet_W, void *logrho, int32_t *err, void *stream) {
+  clear_error();
+  if (int st = tc_common_checks("estep_tc", dtype, N, D, npts)) return st;
+  if (N == 0) return LAKDE_OK;
+  if (!rowptr || !col || !X || !W_triu || !nu || !logdet_W || !logrho || !err) {
+    set_error("estep_tc: null pointer");
+    return LAKDE_EINVAL;
+  }
+  if (int st = bind_device("estep_tc", {logrho, rowptr, col, order, X, W_triu, nu, logdet_W, err})) return st;
+  tc::TcArgs g{};
+  g.rowptr = static_cast<const int64_t *>(rowptr);
+  g.col = static_cast<const int32_t *>(col);
+  g.order = static_cast<const int32_t *>(order);
+  g.X = static_cast<const float *>(X);
+  g.W = static_cast<const float *>(W_triu);
+  g.nu = static_cast<const float *>(nu);
+  g.logdet = static_cast<const float *>(logdet_W);
+  g.logrho = static_cast<float *>(logrho);
+  g.npts = npts;
+  g.N = N;
+  g.D = (int)D;
+  g.err = err;
+  const size_t smem = tc::EsmCfg::bytes;
+  cudaError_t e = cudaFuncSetAttribute(tc::estep_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) {
+    set_error("estep_tc: %s", cudaGetErrorString(e));
+    return LAKDE_ECUDA;
+  }
+  unsigned grid;
+  tc_grid(smem, 64, N, &grid);
+  tc::estep_tc_kernel<<<grid, 128, smem, as_stream(stream)>>>(g);
+  return check_launch("estep_tc");
+}
+
+extern "C" int lakde_mstep_tc(int dtype, int64_t N, int64_t D, int64_t npts, const void *rowptr, const void *col,
+                              const void *order, const void *r, const void *X, double nu_0, void *S, void *nu,
+                              int32_t *err, void *stream) {
+  clear_error();
+  if (int st = tc_common_checks("mstep_tc", dtype, N, D, npts)) return st;
+  if (N == 0) return LAKDE_OK;
+  if (!rowptr || !col || !r || !X || !S || !nu || !err) {
+    set_error("mstep_tc: null pointer");
+    return LAKDE_EINVAL;
+  }
+  if (int st = bind_device("mstep_tc", {S, rowptr, col, order, r, X, nu, err})) return st;
+  tc::TcArgs g{};
+  g.rowptr = static_cast<const int64_t *>(rowptr);
+  g.col = static_cast<const int32_t *>(col);
+  g.order = static_cast<const int32_t *>(order);
+  g.r = static_cast<const float *>(r);
+  g.X = static_cast<const float *>(X);
+  g.S = static_cast<float *>(S);
+  g.nu_out = static_cast<float *>(nu);
+  g.nu0 = (float)nu_0;
+  g.npts = npts;
+  g.N = N;
+  g.D = (int)D;
+  g.err = err;
+  const size_t smem = tc::MsmCfg::bytes;
+  cudaError_t e = cudaFuncSetAttribute(tc::mstep_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) {
+    set_error("mstep_tc: %s", cudaGetErrorString(e));
+    return LAKDE_ECUDA;
+  }
+  unsigned grid;
+  tc_grid(smem, 128, N, &grid);
+  tc::mstep_tc_kernel<<<grid, 128, smem, as_stream(stream)>>>(g);
+  return check_launch("mstep_tc");
+}

@@ -34,7 +34,7 @@ LOG2 = math.log(2.0)
 class FusedVI:
     """State and iteration of the locally adaptive models on a pair pattern."""
 
-    def __init__(self, X, pattern, nu_0, a_0, b_0, threshold, init_k, init_graph):
+    def __init__(self, X, pattern, nu_0, a_0, b_0, threshold, init_k, init_graph, precision="auto"):
         self.X = X
         self.N, self.D = X.shape
         self.dtype = X.dtype
@@ -64,6 +64,14 @@ class FusedVI:
         self.a = (a_0 + nu_0 * D / 2).expand(N).contiguous()
         self.b = self.a.clone()
         self.graph = None
+        self.err = torch.zeros(1, dtype=torch.int32, device=self.device)
+        # "mixed": tensor-core (tcgen05, bf16 hi + lo) contractions for 8 < D <= 64;
+        # "fp32": the plain FP32 kernels.  Factorisations are FP64 either way.
+        if precision == "auto":
+            precision = "mixed" if (8 < D <= 64 and self.dtype == torch.float32) else "fp32"
+        if precision == "mixed" and not (D <= 64 and self.dtype == torch.float32):
+            raise ValueError("precision='mixed' needs float32 data with D <= 64")
+        self.precision = precision
 
     # ------------------------------------------------------------------ setup
     def _initial_responsibilities(self, init_graph, init_k):
@@ -92,7 +100,10 @@ class FusedVI:
     # --------------------------------------------------------------- kernels
     def mstep(self):
         rowptr, col = self._tri()
-        K.mstep(rowptr, col, self.r, self.X, self.nu_0, S=self.S, nu=self.nu)
+        if self.precision == "mixed":
+            K.mstep_tc(rowptr, col, self.r, self.X, self.nu_0, self.err, order=self.pattern.order, S=self.S, nu=self.nu)
+        else:
+            K.mstep(rowptr, col, self.r, self.X, self.nu_0, S=self.S, nu=self.nu)
 
     def factor(self, with_trace=True):
         P, T = self._prior()
@@ -105,13 +116,30 @@ class FusedVI:
 
     def estep(self, mode):
         rowptr, col = self._tri()
-        K.estep_logrho(rowptr, col, self.X, self.U, self.nu, self.logdet_W, out=self.logrho)
+        if self.precision == "mixed":
+            K.estep_tc(rowptr, col, self.X, self.U, self.nu, self.logdet_W, self.err, order=self.pattern.order,
+                       out=self.logrho)
+        else:
+            K.estep_logrho(rowptr, col, self.X, self.U, self.nu, self.logdet_W, out=self.logrho)
         K.estep_normalise(self.pattern.cptr, self.pattern.pos, self.logrho, self.r, self.c, self.rsum, mode,
                           self.threshold)
+
+    _STATE = ("r", "c", "rsum", "b", "W_inv_jitter", "nu", "logdet_W")
+
+    def snapshot(self):
+        """Copies of the iteration state (to rerun iterations from one point)."""
+        keys = self._STATE + tuple(k for k in ("sigma_0_lambda_mm_trace", "W_shared_triu") if hasattr(self, k))
+        return {k: getattr(self, k).clone() for k in keys}
+
+    def restore(self, snap):
+        for k, v in snap.items():
+            getattr(self, k).copy_(v)
 
     def check_errors(self):
         if int(self.failed) != 0:
             raise RuntimeError("Stabilization did not converge")
+        if int(self.err) != 0:
+            raise RuntimeError("a tensor-core completion wait timed out; results of this fit are invalid")
 
     # ------------------------------------------------------------ prediction
     def log_pred_density(self, Y):
@@ -120,10 +148,14 @@ class FusedVI:
         S = torch.empty_like(self.S)
         nu = torch.empty_like(self.nu)
         rowptr, col = self._tri()
-        K.mstep(rowptr, col, self.r, self.X, self.nu_0, S=S, nu=nu)
+        if self.precision == "mixed":
+            K.mstep_tc(rowptr, col, self.r, self.X, self.nu_0, self.err, order=self.pattern.order, S=S, nu=nu)
+        else:
+            K.mstep(rowptr, col, self.r, self.X, self.nu_0, S=S, nu=nu)
         P, _ = self._prior()
         W, logdet, info, _, _ = K.posterior_factor(S, self.W_inv_jitter, self.eps, P=P, nu_0=self.nu_0_t, a=self.a,
                                                    b=self.b)
+        del S
         torch.minimum(self.failed, info.min(), out=self.failed)
         lc = K.pred_coeff(nu, logdet, self.D)
         return K.log_pred_density(self.X, W, nu, lc, Y.to(self.dtype))
@@ -162,8 +194,8 @@ class FusedVI:
 class FusedKNN(FusedVI):
     """LocalKNearestKDE on a pair pattern (lakde/local_knn_kde.py)."""
 
-    def __init__(self, X, knn_graph, pattern, nu_0, a_0, b_0, threshold, init_k):
-        super().__init__(X, pattern, nu_0, a_0, b_0, threshold, init_k, knn_graph[:, :init_k])
+    def __init__(self, X, knn_graph, pattern, nu_0, a_0, b_0, threshold, init_k, precision="auto"):
+        super().__init__(X, pattern, nu_0, a_0, b_0, threshold, init_k, knn_graph[:, :init_k], precision)
         self.knn_graph = knn_graph
         N, D = self.N, self.D
         self.sigma_0_jitter = torch.zeros(N, dtype=self.dtype, device=self.device)
@@ -237,8 +269,8 @@ class FusedKNN(FusedVI):
 class FusedHier(FusedVI):
     """LocalHierarchicalKDE on a pair pattern (lakde/local_hierarchical_kde.py)."""
 
-    def __init__(self, X, knn_graph, pattern, nu_0, a_0, b_0, threshold, init_k, nu_shared_0):
-        super().__init__(X, pattern, nu_0, a_0, b_0, threshold, init_k, knn_graph[:, :init_k])
+    def __init__(self, X, knn_graph, pattern, nu_0, a_0, b_0, threshold, init_k, nu_shared_0, precision="auto"):
+        super().__init__(X, pattern, nu_0, a_0, b_0, threshold, init_k, knn_graph[:, :init_k], precision)
         self.nu_shared_0 = float(nu_shared_0)
         N, D = self.N, self.D
         self.W_shared_inv_jitter = torch.zeros(1, dtype=torch.float64, device=self.device)

@@ -240,8 +240,11 @@ def estep_logrho(rowptr, col, X, W_triu, nu, logdet_W, kernel_offset=0, out=None
 
 def vi_rows(rowptr, col, r, X, nu_0, a, b, b_0, jitter, eps, nu, logdet_W, info, logrho, P=None, T=None,
             order=None, mm=None):
-    """Fused per-kernel pass of one VI iteration for D <= 8 (see include/lakde_b200.h)."""
+    """Fused per-kernel pass of one VI iteration (see include/lakde_b200.h):
+    one thread per row for D <= 8 (lakde_vi_rows), one CTA per row for
+    8 < D <= 64 (lakde_vi_cta, float32)."""
     nat.require_cuda(rowptr, col, r, X, a, b, jitter, nu, logdet_W, info, logrho, P, T, order, mm, op="vi_rows")
+    entry = nat.lib().lakde_vi_rows if X.size(1) <= 8 else nat.lib().lakde_vi_cta
     N = rowptr.numel() - 1
     D = X.size(1)
     assert rowptr.dtype == torch.int64 and col.dtype == torch.int32
@@ -249,7 +252,7 @@ def vi_rows(rowptr, col, r, X, nu_0, a, b, b_0, jitter, eps, nu, logdet_W, info,
     pbs = 0 if P is None or P.dim() == 2 else D * D
     tbs = 0 if T is None or T.dim() == 2 else D * D
     nat.check(
-        nat.lib().lakde_vi_rows(
+        entry(
             nat.dtype_code(X), N, D, X.size(0), nat.ptr(rowptr), nat.ptr(col), nat.ptr(order), nat.ptr(r),
             nat.ptr(X), float(nu_0), nat.ptr(P), pbs, nat.ptr(T), tbs, nat.ptr(a), nat.ptr(b), float(b_0),
             nat.ptr(jitter), float(eps), nat.ptr(nu), nat.ptr(logdet_W), nat.ptr(mm), nat.ptr(info), nat.ptr(logrho),
@@ -336,3 +339,37 @@ def log_pred_density_bwd(X, W_triu, nu, log_coeff, Y, out, grad_out):
         "log_pred_density_bwd",
     )
     return gY, sw, S_c
+
+
+def estep_tc(rowptr, col, X, W_triu, nu, logdet_W, err, order=None, out=None):
+    """Tensor-core (bf16 hi + lo) E-step numerators, D <= 64 (see include/lakde_b200.h)."""
+    nat.require_cuda(rowptr, col, X, W_triu, nu, logdet_W, err, order, op="estep_tc")
+    assert rowptr.dtype == torch.int64 and col.dtype == torch.int32 and err.dtype == torch.int32
+    N = rowptr.numel() - 1
+    out = X.new_empty(col.numel()) if out is None else out
+    nat.check(
+        nat.lib().lakde_estep_tc(
+            nat.dtype_code(X), N, X.size(1), X.size(0), nat.ptr(rowptr), nat.ptr(col), nat.ptr(order), nat.ptr(X),
+            nat.ptr(W_triu), nat.ptr(nu), nat.ptr(logdet_W), nat.ptr(out), nat.ptr(err), nat.stream_of(X),
+        ),
+        "estep_tc",
+    )
+    return out
+
+
+def mstep_tc(rowptr, col, r, X, nu_0, err, order=None, S=None, nu=None):
+    """Tensor-core (bf16 hi + lo) M-step S and nu, D <= 64 (see include/lakde_b200.h)."""
+    nat.require_cuda(rowptr, col, r, X, err, order, op="mstep_tc")
+    assert rowptr.dtype == torch.int64 and col.dtype == torch.int32 and err.dtype == torch.int32
+    N = rowptr.numel() - 1
+    D = X.size(1)
+    S = X.new_empty(N, D, D) if S is None else S
+    nu = X.new_empty(N) if nu is None else nu
+    nat.check(
+        nat.lib().lakde_mstep_tc(
+            nat.dtype_code(X), N, D, X.size(0), nat.ptr(rowptr), nat.ptr(col), nat.ptr(order), nat.ptr(r),
+            nat.ptr(X), float(nu_0), nat.ptr(S), nat.ptr(nu), nat.ptr(err), nat.stream_of(X),
+        ),
+        "mstep_tc",
+    )
+    return S, nu

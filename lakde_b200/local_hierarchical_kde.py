@@ -27,10 +27,12 @@ class LocalHierarchicalKDE(LocallyAdaptiveKDE):
     def __init__(self, nu_0: Union[torch.Tensor, float] = None, k_or_knn_graph: Union[torch.Tensor, int] = None,
                  block_size: int = 512, nu_shared_0: Union[torch.Tensor, float] = None,
                  a_0: Union[torch.Tensor, float] = 1e-6, b_0: Union[torch.Tensor, float] = 1e-6, verbose=False,
-                 logs=False, fused=False, candidates="knn", cuda_graph=True, candidate_counts=None):
+                 logs=False, fused=False, candidates="knn", cuda_graph=True, candidate_counts=None,
+                 precision="auto"):
         super().__init__(nu_0, a_0, b_0, block_size, verbose, logs, fused, candidates, cuda_graph)
         self.k_or_knn_graph = k_or_knn_graph
         self.candidate_counts = candidate_counts
+        self.precision = precision
         self.knn_graph = None
         self.k = None
         self.nu_shared_0 = nu_shared_0
@@ -74,7 +76,7 @@ class LocalHierarchicalKDE(LocallyAdaptiveKDE):
         if self.fused:
             pattern = build_pattern(self.candidates, self.knn_graph, N, X.device, self.candidate_counts)
             self.engine = FusedHier(X, self.knn_graph, pattern, self.nu_0, self.a_0, self.b_0, sparsity_threshold,
-                                    init_k, self.nu_shared_0)
+                                    init_k, self.nu_shared_0, self.precision)
             self._eager_steps = 0
             self._sync_from_engine()
             self._sync_shared()

@@ -143,3 +143,27 @@ def test_cuda_graph_replay_equals_eager():
     torch.testing.assert_close(res[0][0], res[1][0], rtol=0, atol=0)
     torch.testing.assert_close(res[0][1], res[1][1], rtol=0, atol=0)
     assert res[0][2] == res[1][2]
+
+
+def test_mixed_precision_within_1e3_nats_of_fp64():
+    """Tensor-core mixed precision and plain FP32 against the FP64 path on the
+    same data, kNN graph and candidate pattern (d = 21)."""
+    from lakde_b200 import LocalKNearestKDE
+    from lakde_b200.synthetic import wide_spectrum_mixture
+
+    Xn, Yn = wide_spectrum_mixture(seed=2, n_train=6000, n_test=800)
+    X = torch.tensor(Xn, device=DEV)
+    Y = torch.tensor(Yn, device=DEV)
+    from lakde_b200.utils import compute_knn_graph
+
+    graph = compute_knn_graph(X, 32)
+    out = {}
+    for name, dt, prec in (("fp64", torch.float64, "fp32"), ("fp32", torch.float32, "fp32"),
+                           ("mixed", torch.float32, "mixed")):
+        m = LocalKNearestKDE(k_or_knn_graph=graph, fused=True, cuda_graph=False, precision=prec)
+        m.fit(X.to(dt), iterations=5, sparsity_threshold=5e-4)
+        assert m.engine.precision == prec
+        out[name] = (float(m.compute_elbo(X.to(dt))), m.log_pred_density(X.to(dt), Y.to(dt)).double().mean().item())
+    for name in ("fp32", "mixed"):
+        assert abs(out[name][1] - out["fp64"][1]) <= 1e-3, (name, out)
+        assert abs(out[name][0] - out["fp64"][0]) <= 1e-4 * abs(out["fp64"][0]), (name, out)
