@@ -115,7 +115,9 @@ LAKDE_API int lakde_W_inv(int dtype, const void *rowptr, int rowptr_dtype, const
  * lakde/linalg_util.py:109-170 (stabilize_/stabilized_cholesky), :49-52
  * (tril_inverse), :30-37 (chol_logdet, chol_mm_trace).
  * P (optional) and T (optional) are [D,D] blocks with a batch stride in
- * elements (0 = one matrix shared by all n).  S [N,D,D] contiguous.
+ * elements (0 = one matrix shared by all n).  T_lower != 0 declares every
+ * T_n lower triangular (its entries above the diagonal are then not read).
+ * S [N,D,D] contiguous.
  * jitter [N] is read and updated in place.  Outputs: W_triu [N,D,D],
  * L [N,D,D] (optional), logdet_W [N], info [N] (int32: 0 ok, -1 ladder failed),
  * trace [N] (optional).  All value arrays have `dtype` (F32/F64); a, b, nu_0
@@ -126,7 +128,8 @@ LAKDE_API int lakde_posterior_factor(int dtype, int64_t N, int64_t D, const void
                            const void *nu_0, const void *a, const void *b,
                            void *jitter, double eps, void *W_triu, void *L,
                            void *logdet_W, int32_t *info, const void *T,
-                           int64_t T_batch_stride, void *trace, void *stream);
+                           int64_t T_batch_stride, int T_lower, void *trace,
+                           void *stream);
 
 /*
  * Fused-path M-step: the scatter covariance of lakde_W_inv for kernels

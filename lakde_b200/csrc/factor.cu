@@ -30,6 +30,7 @@ struct FactorArgs {
   int32_t *info;
   const T *Tm;
   int64_t Tbs;
+  int T_lower;
   T *trace;
   int64_t N;
   int D;
@@ -157,7 +158,10 @@ __global__ void __launch_bounds__(128) factor_thread_kernel(FactorArgs<T> g) {
         if (bcol >= D) continue;
         double s = 0.0;
 #pragma unroll
-        for (int k = 0; k <= bcol; ++k) s += (double)Tm[k * D + a] * Li[tri_idx<DP>(bcol, k)];
+        for (int k = 0; k <= bcol; ++k) {
+          const double tka = (g.T_lower && a > k) ? 0.0 : (double)Tm[k * D + a];
+          s += tka * Li[tri_idx<DP>(bcol, k)];
+        }
         acc += s * s;
       }
     }
@@ -170,23 +174,133 @@ template <int DP>
 struct DmmaCfg {
   static constexpr int NT = DP / 8;
   static constexpr int NTILE = NT * (NT + 1) / 2;
-  static constexpr int WPB = DP >= 48 ? 2 : 4;
-  static constexpr int per_warp = NTILE * 64 + 64 + DP + NT * 64;  // tiles, scratch, diag(L), T column block
+  static constexpr int WPB = 2;
+  // per warp: FP64 tiles, a scratch tile, 1 / L_ii, then the lower triangle
+  // of a per-matrix FP32 T_n (packed rows, in doubles rounded up to 16 bytes)
+  static constexpr int off_scratch = NTILE * 64;
+  static constexpr int off_rdiag = off_scratch + 64;
+  static constexpr int off_tstage = off_rdiag + DP;
+  static constexpr int tstage = ((DP * (DP + 1) / 2 + 3) / 4) * 2;
+  static constexpr int per_warp = off_tstage + tstage;
   static constexpr size_t smem = (size_t)WPB * per_warp * sizeof(double);
 };
 
+// Pulls one matrix (bytes from p) into L2 ahead of its use, one 128-byte line
+// per lane and step; every address issued lies inside the matrix.
+__device__ __forceinline__ void prefetch_l2(const void *p, int64_t bytes, int lane) {
+  const char *c = static_cast<const char *>(p);
+  for (int64_t off = (int64_t)lane * 128; off < bytes; off += 32 * 128)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(c + off));
+}
+
+// A_ij + jt [i == j] in the model dtype (the rounding of the reference's
+// separate tensor ops), as FP64; rows i >= D are the identity padding.
+template <typename T>
+__device__ __forceinline__ double assemble_one(T sv, T pv, bool has_p, T scale, T jt, int i, int c, int D) {
+  if (i >= D) return (c == i) ? 1.0 : 0.0;
+  if (c > i) return 0.0;
+  T x = sv;
+  if (has_p) x = add_rn(mul_rn(pv, scale), x);
+  if (c == i) x = add_rn(x, jt);
+  return (double)x;
+}
+
+// Lower tiles of A_n + jt I in FP64, padded with the identity, row block by
+// row block with all loads of a block issued before any is used (coalesced:
+// lanes read consecutive columns).  For FP32 with a per-matrix T_n, the lower
+// triangle of T_n is copied to the packed FP32 stage in the same batches.
 template <typename T, int DP>
-__global__ void __launch_bounds__(128) factor_dmma_kernel(FactorArgs<T> g) {
+__device__ __forceinline__ void assemble_tiles(const FactorArgs<T> &g, int64_t n, T scale, T jt, double *M,
+                                               float *tstage, int lane) {
+  constexpr int NT = DP / 8;
+  constexpr int H = DP > 32 ? 2 : 1;
+  const int D = g.D;
+  const T *Sn = g.S + n * (int64_t)D * D;
+  const T *Pn = g.P ? g.P + n * g.Pbs : nullptr;
+  if constexpr (sizeof(T) == 4) {
+    const float *Tn = tstage ? g.Tm + n * g.Tbs : nullptr;
+#pragma unroll 1
+    for (int I = 0; I < NT; ++I) {
+      float sv[8][H], pv[8][H], tv[8][H];
+#pragma unroll
+      for (int rr = 0; rr < 8; ++rr) {
+        const int i = 8 * I + rr;
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+          const int c = lane + 32 * h;
+          const bool in = i < D && c <= i;
+          sv[rr][h] = in ? Sn[i * D + c] : 0.f;
+          pv[rr][h] = (in && Pn) ? Pn[i * D + c] : 0.f;
+          tv[rr][h] = (in && Tn) ? Tn[i * D + c] : 0.f;
+        }
+      }
+#pragma unroll
+      for (int rr = 0; rr < 8; ++rr) {
+        const int i = 8 * I + rr;
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+          const int c = lane + 32 * h;
+          if (c >= 8 * I + 8) continue;  // right of the diagonal tile
+          M[dmma::tix(I, c >> 3) + rr * 8 + (c & 7)] =
+              assemble_one<T>(sv[rr][h], pv[rr][h], Pn != nullptr, scale, jt, i, c, D);
+          if (Tn && i < D && c <= i) tstage[i * (i + 1) / 2 + c] = tv[rr][h];
+        }
+      }
+    }
+    __syncwarp();
+  } else {
+#pragma unroll 1
+    for (int I = 0; I < NT; ++I) {
+      T sv[8][H], pv[8][H];
+#pragma unroll
+      for (int rr = 0; rr < 8; ++rr) {
+        const int i = 8 * I + rr;
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+          const int c = lane + 32 * h;
+          const bool in = i < D && c <= i;
+          sv[rr][h] = in ? Sn[i * D + c] : T(0);
+          pv[rr][h] = (in && Pn) ? Pn[i * D + c] : T(0);
+        }
+      }
+#pragma unroll
+      for (int rr = 0; rr < 8; ++rr) {
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+          const int c = lane + 32 * h;
+          if (c >= 8 * I + 8) continue;  // right of the diagonal tile
+          M[dmma::tix(I, c >> 3) + rr * 8 + (c & 7)] =
+              assemble_one<T>(sv[rr][h], pv[rr][h], Pn != nullptr, scale, jt, 8 * I + rr, c, D);
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// B fragments of the 8-column block Ac of T_n, tile K of rows 8K..8K+7:
+// tb[K][s] = T[8K + 4s + t % 4][8 Ac + t / 4].
+template <typename T, int NT>
+__device__ __forceinline__ void load_tcol(const T *Tn, int D, int lower, int Ac, int lane, T (&tb)[NT][2]) {
+  const int col = 8 * Ac + (lane >> 2);
+#pragma unroll
+  for (int K = 0; K < NT; ++K)
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const int row = 8 * K + 4 * s + (lane & 3);
+      tb[K][s] = (row < D && col < D && (!lower || col <= row)) ? Tn[row * D + col] : T(0);
+    }
+}
+
+template <typename T, int DP>
+__device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, double *M, int lane) {
   using C = DmmaCfg<DP>;
   constexpr int NT = C::NT;
-  extern __shared__ double smem_d[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t n = (int64_t)blockIdx.x * C::WPB + warp;
-  if (n >= g.N) return;
-  double *M = smem_d + warp * C::per_warp;
-  double *scratch = M + C::NTILE * 64;
-  double *ldiag = scratch + 64;
-  double *tcol = ldiag + DP;  // one 8-column block of T_n, NT tiles
+  double *scratch = M + C::off_scratch;
+  double *rdiag = M + C::off_rdiag;
+  // per-matrix FP32 T_n goes through shared memory with the other inputs
+  const bool staged = sizeof(T) == 4 && g.Tm && g.Tbs != 0;
+  float *tstage = staged ? reinterpret_cast<float *>(M + C::off_tstage) : nullptr;
   const int D = g.D;
   const T scale = posterior_scale(g, n);
   T jit = g.jitter[n];
@@ -198,14 +312,9 @@ __global__ void __launch_bounds__(128) factor_dmma_kernel(FactorArgs<T> g) {
       jt = T(0);
       for (int k = 0; k < attempt; ++k) jt = add_rn(jt, (T)(g.eps * ldexp(1.0, k)));
     }
-    for (int e = lane; e < DP * DP; e += 32) {
-      const int i = e / DP, j = e % DP;
-      if (j > i) continue;
-      const double v = (i < D) ? assembled(g, n, scale, i, j, jt) : (i == j ? 1.0 : 0.0);
-      M[dmma::tix(i >> 3, j >> 3) + (i & 7) * 8 + (j & 7)] = v;
-    }
+    assemble_tiles<T, DP>(g, n, scale, jt, M, tstage, lane);
     __syncwarp();
-    ok = dmma::chol_blocked<T>(M, scratch, ldiag, NT, lane, lout, D);
+    ok = dmma::chol_blocked<NT, T>(M, scratch, rdiag, lane, lout, D);
     if (ok) jit = jt;
     __syncwarp();
   }
@@ -233,49 +342,130 @@ __global__ void __launch_bounds__(128) factor_dmma_kernel(FactorArgs<T> g) {
       if ((c >> 3) > (r >> 3)) lout[e] = T(0);
     }
   }
-  dmma::trtri_blocked(M, scratch, NT, lane);
-  // W_triu = X^T (upper): W[r][c] = X[c][r], r <= c
-  for (int e = lane; e < D * D; e += 32) {
-    const int r = e / D, c = e % D;
-    const double v = (r <= c) ? M[dmma::tix(c >> 3, r >> 3) + (c & 7) * 8 + (r & 7)] : 0.0;
-    W[e] = (T)v;
+  // first column block of a shared or FP64 T in flight during the inverse
+  const T *Tn = g.Tm ? g.Tm + n * g.Tbs : nullptr;
+  T tb[NT][2];
+  if (Tn && !staged) load_tcol<T, NT>(Tn, D, g.T_lower, 0, lane, tb);
+  dmma::trtri_blocked<NT>(M, lane);
+  // W_triu = X^T: W tile (J, I) = X_IJ^T for I >= J, zero below; lanes write
+  // 8 consecutive columns of 4 rows per store
+  {
+    const int r = lane & 7;
+#pragma unroll 1
+    for (int J = 0; J < NT; ++J) {
+#pragma unroll
+      for (int I = 0; I < NT; ++I) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int c = (lane >> 3) + 4 * h;
+          const int row = 8 * J + c, col = 8 * I + r;
+          if (row < D && col < D) {
+            double v = 0.0;
+            if (I > J || (I == J && r >= c)) v = M[dmma::tix(I, J) + r * 8 + c];
+            W[row * D + col] = (T)v;
+          }
+        }
+      }
+    }
   }
   double ld = 0.0;
-  for (int i = lane; i < D; i += 32) ld += log((double)(T)(1.0 / ldiag[i]));
+  for (int i = lane; i < D; i += 32) ld += log((double)(T)rdiag[i]);
   ld = warp_sum(ld);
   if (lane == 0) g.logdet[n] = (T)(2.0 * ld);
-  if (g.Tm) {
-    // ||X T_n||_F^2 with X lower: (X T)_IA = sum_{K <= I} X_IK T_KA.  Each
-    // 8-column block A of T_n is staged in shared memory (coalesced rows) and
-    // its all-zero 8 x 8 tiles (the upper part of a triangular T) are skipped.
-    const T *Tn = g.Tm + n * g.Tbs;
+  if (staged) {
+    // ||X T_n||_F^2 with X lower: (X T)_IA = sum_{K <= I} X_IK T_KA, column
+    // block by column block; lower tiles of T_n (K >= A) from shared memory,
+    // upper ones from global memory unless T_n is declared lower triangular
+    const float *st = tstage;
     double acc = 0.0;
+#pragma unroll 1
     for (int Ac = 0; Ac < NT; ++Ac) {
-      __syncwarp();
-      for (int e = lane; e < NT * 64; e += 32) {
-        const int row = e >> 3, col = 8 * Ac + (e & 7);
-        tcol[e] = (row < D && col < D) ? (double)Tn[row * D + col] : 0.0;
+      const int col = 8 * Ac + (lane >> 2);
+      double cacc[NT][2];
+#pragma unroll
+      for (int I = 0; I < NT; ++I) {
+        cacc[I][0] = 0.0;
+        cacc[I][1] = 0.0;
       }
-      __syncwarp();
-      unsigned nonzero = 0;  // bit K: tile K of this column block has a non-zero
+#pragma unroll
       for (int K = 0; K < NT; ++K) {
-        const bool nz = tcol[K * 64 + lane] != 0.0 || tcol[K * 64 + 32 + lane] != 0.0;
-        if (__any_sync(0xffffffffu, nz)) nonzero |= 1u << K;
+        double b0 = 0.0, b1 = 0.0;
+        const int r0 = 8 * K + (lane & 3), r1 = r0 + 4;
+        if (K >= Ac) {
+          b0 = (r0 < D && col <= r0) ? (double)st[r0 * (r0 + 1) / 2 + col] : 0.0;
+          b1 = (r1 < D && col <= r1) ? (double)st[r1 * (r1 + 1) / 2 + col] : 0.0;
+        } else {
+          if (g.T_lower) continue;
+          b0 = (r0 < D && col < D) ? (double)Tn[r0 * D + col] : 0.0;
+          b1 = (r1 < D && col < D) ? (double)Tn[r1 * D + col] : 0.0;
+          if (!__any_sync(0xffffffffu, b0 != 0.0 || b1 != 0.0)) continue;
+        }
+#pragma unroll
+        for (int I = K; I < NT; ++I) {
+          const double *x = M + dmma::tix(I, K);
+          dmma::mma(cacc[I][0], cacc[I][1], dmma::afrag(x, 0, lane), b0);
+          dmma::mma(cacc[I][0], cacc[I][1], dmma::afrag(x, 1, lane), b1);
+        }
       }
+#pragma unroll
+      for (int I = 0; I < NT; ++I) acc = fma(cacc[I][0], cacc[I][0], fma(cacc[I][1], cacc[I][1], acc));
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) g.trace[n] = (T)acc;
+  } else if (Tn) {
+    // ||X T_n||_F^2 with X lower: (X T)_IA = sum_{K <= I} X_IK T_KA, column
+    // block by column block, the next block's loads issued before this one's
+    // products; all-zero tiles of T_n (its upper part when triangular) skipped
+    double acc = 0.0;
+#pragma unroll 1
+    for (int Ac = 0; Ac < NT; ++Ac) {
+      double b[NT][2];
+      unsigned nonzero = 0;
+#pragma unroll
+      for (int K = 0; K < NT; ++K) {
+        b[K][0] = (double)tb[K][0];
+        b[K][1] = (double)tb[K][1];
+        if (__any_sync(0xffffffffu, b[K][0] != 0.0 || b[K][1] != 0.0)) nonzero |= 1u << K;
+      }
+      if (Ac + 1 < NT) load_tcol<T, NT>(Tn, D, g.T_lower, Ac + 1, lane, tb);
+#pragma unroll
       for (int I = 0; I < NT; ++I) {
         double c0 = 0.0, c1 = 0.0;
+        asm volatile("" ::: "memory");
+#pragma unroll
         for (int K = 0; K <= I; ++K) {
           if (!((nonzero >> K) & 1u)) continue;
           const double *x = M + dmma::tix(I, K);
-          const double *tk = tcol + K * 64;
-#pragma unroll
-          for (int s = 0; s < 2; ++s) dmma::mma(c0, c1, dmma::afrag(x, s, lane), dmma::bfrag(tk, s, lane));
+          dmma::mma(c0, c1, dmma::afrag(x, 0, lane), b[K][0]);
+          dmma::mma(c0, c1, dmma::afrag(x, 1, lane), b[K][1]);
         }
-        acc += c0 * c0 + c1 * c1;
+        acc = fma(c0, c0, fma(c1, c1, acc));
       }
     }
     acc = warp_sum(acc);
     if (lane == 0) g.trace[n] = (T)acc;
+  }
+}
+
+// Persistent: each warp walks matrices n, n + stride, ... and pulls the next
+// one's inputs into L2 before factorising the current one.
+template <typename T, int DP>
+__global__ void __launch_bounds__(32 * DmmaCfg<DP>::WPB) factor_dmma_kernel(FactorArgs<T> g) {
+  using C = DmmaCfg<DP>;
+  extern __shared__ double smem_d[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double *M = smem_d + warp * C::per_warp;
+  const int64_t stride = (int64_t)gridDim.x * C::WPB;
+  const int64_t DD = (int64_t)g.D * g.D;
+  for (int64_t n = (int64_t)blockIdx.x * C::WPB + warp; n < g.N; n += stride) {
+    const int64_t nx = n + stride;
+    if (nx < g.N) {
+      prefetch_l2(g.S + nx * DD, DD * (int64_t)sizeof(T), lane);
+      if (g.P && g.Pbs) prefetch_l2(g.P + nx * g.Pbs, DD * (int64_t)sizeof(T), lane);
+      if (g.Tm && g.Tbs) prefetch_l2(g.Tm + nx * g.Tbs, DD * (int64_t)sizeof(T), lane);
+    }
+    factor_one<T, DP>(g, n, M, lane);
+    __syncwarp();
   }
 }
 
@@ -286,8 +476,8 @@ using namespace lakde;
 extern "C" int lakde_posterior_factor(int dtype, int64_t N, int64_t D, const void *S, const void *P,
                                       int64_t P_batch_stride, const void *nu_0, const void *a, const void *b,
                                       void *jitter, double eps, void *W_triu, void *L, void *logdet_W,
-                                      int32_t *info, const void *T, int64_t T_batch_stride, void *trace,
-                                      void *stream) {
+                                      int32_t *info, const void *T, int64_t T_batch_stride, int T_lower,
+                                      void *trace, void *stream) {
   clear_error();
   if (N < 0 || D < 1) {
     set_error("posterior_factor: invalid sizes (N=%lld, D=%lld)", (long long)N, (long long)D);
@@ -321,6 +511,7 @@ extern "C" int lakde_posterior_factor(int dtype, int64_t N, int64_t D, const voi
     g.info = info;
     g.Tm = static_cast<const TT *>(T);
     g.Tbs = T_batch_stride;
+    g.T_lower = T_lower != 0;
     g.trace = static_cast<TT *>(trace);
     g.N = N;
     g.D = (int)D;
@@ -338,7 +529,20 @@ extern "C" int lakde_posterior_factor(int dtype, int64_t N, int64_t D, const voi
             return (int)LAKDE_ECUDA;
           }
         }
-        kern<<<(unsigned)((N + C::WPB - 1) / C::WPB), 32 * C::WPB, C::smem, as_stream(stream)>>>(g);
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
+        // persistent grid: exactly the blocks that are resident at once
+        // (registers and shared memory), so every block starts immediately
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * C::WPB, C::smem) != cudaSuccess ||
+            per_sm < 1) {
+          cudaGetLastError();
+          per_sm = 1;
+        }
+        int64_t blocks = (N + C::WPB - 1) / C::WPB;
+        if (blocks > (int64_t)sms * per_sm) blocks = (int64_t)sms * per_sm;
+        kern<<<(unsigned)blocks, 32 * C::WPB, C::smem, as_stream(stream)>>>(g);
       }
       return check_launch("posterior_factor");
     });

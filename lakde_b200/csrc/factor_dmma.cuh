@@ -9,6 +9,8 @@
 //   B (4 x 8, col-major)  b = M[4 s + t % 4][t / 4]      (B = M)
 //                         b = M[t / 4][4 s + t % 4]      (B = M^T)
 //   C (8 x 8)             c0, c1 = M[t / 4][2 (t % 4) + {0, 1}]
+// NT is a template parameter so every tile offset is a compile-time constant
+// and the independent tile products of one step can be issued back to back.
 #pragma once
 
 #include "common.cuh"
@@ -18,10 +20,11 @@ namespace dmma {
 
 constexpr int TILE = 64;  // doubles per 8 x 8 tile
 
-__device__ __forceinline__ int tix(int I, int J) { return (I * (I + 1) / 2 + J) * TILE; }
+__host__ __device__ constexpr int tix(int I, int J) { return (I * (I + 1) / 2 + J) * TILE; }
 
 __device__ __forceinline__ void mma(double &c0, double &c1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+  // not volatile: the compiler may interleave independent tile products
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
                : "+d"(c0), "+d"(c1)
                : "d"(a), "d"(b));
 }
@@ -33,107 +36,150 @@ __device__ __forceinline__ double bfrag(const double *t, int s, int lane) { retu
 __device__ __forceinline__ double bfrag_t(const double *t, int s, int lane) { return afrag(t, s, lane); }
 
 __device__ __forceinline__ void load_c(const double *t, int lane, double &c0, double &c1) {
-  const int o = (lane >> 2) * 8 + 2 * (lane & 3);
-  c0 = t[o];
-  c1 = t[o + 1];
+  const double2 v = *reinterpret_cast<const double2 *>(t + (lane >> 2) * 8 + 2 * (lane & 3));
+  c0 = v.x;
+  c1 = v.y;
 }
 __device__ __forceinline__ void store_c(double *t, int lane, double c0, double c1) {
-  const int o = (lane >> 2) * 8 + 2 * (lane & 3);
-  t[o] = c0;
-  t[o + 1] = c1;
+  *reinterpret_cast<double2 *>(t + (lane >> 2) * 8 + 2 * (lane & 3)) = make_double2(c0, c1);
 }
 
-// Cholesky of the lower part of one 8 x 8 tile in place (lanes 0..7 own rows);
-// returns false (warp-uniform) if a pivot is not positive.  The upper part is
-// zeroed.
-__device__ __forceinline__ bool chol_tile(double *t, int lane) {
-  double r[8];
+// B fragment (s) of the 8 x 8 tile whose C fragment the warp holds in (c0, c1):
+// element (4 s + t % 4, t / 4) lives in lane 4 (4 s + t % 4) + (t / 4) / 2,
+// component (t / 4) % 2.
+__device__ __forceinline__ double c_to_b(double c0, double c1, int s, int lane) {
+  const int src = 16 * s + 4 * (lane & 3) + (lane >> 3);
+  const double v0 = __shfl_sync(0xffffffffu, c0, src);
+  const double v1 = __shfl_sync(0xffffffffu, c1, src);
+  return ((lane >> 2) & 1) ? v1 : v0;
+}
+
+// Cholesky and inverse of the 8 x 8 diagonal tile t (lower part), computed
+// redundantly by every lane from broadcast shared-memory reads (no shuffles
+// on the critical path).  On return t holds inv(L_KK) (lower, zero upper)
+// and rdiag[k] = 1 / L_kk.  Returns false (warp-uniform) if a
+// pivot is not positive.  If lt is given, L_KK (lower, zero upper) is written
+// there too.
+__device__ __forceinline__ bool diag_tile(double *t, double *rdiag, double *lt, int lane) {
+  double a[36];  // packed lower, row i at i (i + 1) / 2
 #pragma unroll
-  for (int j = 0; j < 8; ++j) r[j] = (lane < 8 && j <= lane) ? t[lane * 8 + j] : 0.0;
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j <= i; ++j) a[i * (i + 1) / 2 + j] = t[i * 8 + j];
   bool ok = true;
+  double rd[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    const double piv = __shfl_sync(0xffffffffu, r[k], k);
+    const double piv = a[k * (k + 1) / 2 + k];
     ok = ok && (piv > 0.0);
-    const double lkk = sqrt(piv > 0.0 ? piv : 1.0);
-    if (lane == k) r[k] = lkk;
-    if (lane > k && lane < 8) r[k] = r[k] / lkk;
+    const double rs = rsqrt(piv > 0.0 ? piv : 1.0);
+    rd[k] = rs;
+    a[k * (k + 1) / 2 + k] = piv * rs;
 #pragma unroll
-    for (int j = k + 1; j < 8; ++j) {
-      const double ljk = __shfl_sync(0xffffffffu, r[k], j);
-      if (lane >= j && lane < 8) r[j] -= r[k] * ljk;
+    for (int i = k + 1; i < 8; ++i) a[i * (i + 1) / 2 + k] *= rs;
+#pragma unroll
+    for (int i = k + 1; i < 8; ++i)
+#pragma unroll
+      for (int j = k + 1; j <= i; ++j)
+        a[i * (i + 1) / 2 + j] = fma(-a[i * (i + 1) / 2 + k], a[j * (j + 1) / 2 + k], a[i * (i + 1) / 2 + j]);
+  }
+  if (lane == 0 && lt) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) lt[i * 8 + j] = (j <= i) ? a[i * (i + 1) / 2 + j] : 0.0;
+  }
+  // X = L^-1 in place, column by column from the right: with the block below
+  // and right of (j, j) already inverted, X_jj = 1 / L_jj and
+  // X_ij = -X_jj sum_{k=j+1}^{i} X_ik L_kj (i > j)
+#pragma unroll
+  for (int j = 7; j >= 0; --j) {
+    double col[8];
+#pragma unroll
+    for (int i = j + 1; i < 8; ++i) {
+      double sacc = 0.0;
+#pragma unroll
+      for (int k = j + 1; k <= i; ++k) sacc = fma(a[i * (i + 1) / 2 + k], a[k * (k + 1) / 2 + j], sacc);
+      col[i] = -sacc * rd[j];
     }
+#pragma unroll
+    for (int i = j + 1; i < 8; ++i) a[i * (i + 1) / 2 + j] = col[i];
+    a[j * (j + 1) / 2 + j] = rd[j];
   }
   __syncwarp();
-  if (lane < 8) {
+  // lane 0 writes: every lane holds the same values
+  if (lane == 0) {
 #pragma unroll
-    for (int j = 0; j < 8; ++j) t[lane * 8 + j] = (j <= lane) ? r[j] : 0.0;
+    for (int i = 0; i < 8; ++i) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) t[i * 8 + j] = (j <= i) ? a[i * (i + 1) / 2 + j] : 0.0;
+      rdiag[i] = rd[i];
+    }
   }
   __syncwarp();
   return ok;
 }
 
-// inv(L) of a lower 8 x 8 tile (lanes 0..7 own columns), written to `out`
-// (lower, zero upper).  `t` is read only.
-__device__ __forceinline__ void inv_tile(const double *t, double *out, int lane) {
-  double x[8];
-  const int c = lane;
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    double s = (i == c) ? 1.0 : 0.0;
-#pragma unroll
-    for (int k = 0; k < i; ++k) s -= t[i * 8 + k] * ((k >= c) ? x[k] : 0.0);
-    x[i] = (i >= c) ? s / t[i * 8 + i] : 0.0;
-  }
-  __syncwarp();
-  if (lane < 8) {
-#pragma unroll
-    for (int i = 0; i < 8; ++i) out[i * 8 + c] = x[i];
-  }
-  __syncwarp();
-}
-
-// Blocked right-looking Cholesky of the tiled matrix M (NT tiles per side).
-// On return the diagonal tiles hold inv(L_KK) and the off-diagonal tiles
-// L_IK; the diagonal of L is saved in ldiag[0..8 NT).  If lout is given
-// (row-major D x D, ld), the factor L is written there as well.
-template <typename T>
-__device__ __forceinline__ bool chol_blocked(double *M, double *scratch, double *ldiag, int NT, int lane, T *lout,
+// Blocked right-looking Cholesky of the tiled matrix M.  On return the
+// diagonal tiles hold inv(L_KK) and the off-diagonal tiles L_IK; rdiag[i]
+// holds 1 / L_ii.  If lout is given (row-major D x D), the
+// factor L is written there as well (through the scratch tile).  The step loop runs at run time (small
+// code); the tile loops inside a step are unrolled and predicated.
+template <int NT, typename T>
+__device__ __forceinline__ bool chol_blocked(double *M, double *scratch, double *rdiag, int lane, T *lout,
                                              int D) {
+#pragma unroll 1
   for (int K = 0; K < NT; ++K) {
     double *dk = M + tix(K, K);
-    if (!chol_tile(dk, lane)) return false;
-    if (lane < 8) ldiag[8 * K + lane] = dk[lane * 8 + lane];
+    if (!diag_tile(dk, rdiag + 8 * K, lout ? scratch : nullptr, lane)) return false;
     if (lout) {
       for (int e = lane; e < 64; e += 32) {
         const int i = 8 * K + e / 8, j = 8 * K + e % 8;
-        if (i < D && j < D) lout[i * D + j] = (T)(j <= i ? dk[e] : 0.0);
+        if (i < D && j < D) lout[i * D + j] = (T)scratch[e];
       }
     }
-    inv_tile(dk, scratch, lane);
-    for (int e = lane; e < 64; e += 32) dk[e] = scratch[e];
-    __syncwarp();
     // panel: L_IK = A_IK inv(L_KK)^T
-    for (int I = K + 1; I < NT; ++I) {
-      double *t = M + tix(I, K);
-      double c0 = 0.0, c1 = 0.0;
+    const double b0 = bfrag_t(dk, 0, lane), b1 = bfrag_t(dk, 1, lane);
+    double pc[NT][2];
 #pragma unroll
-      for (int s = 0; s < 2; ++s) mma(c0, c1, afrag(t, s, lane), bfrag_t(dk, s, lane));
-      __syncwarp();
-      store_c(t, lane, c0, c1);
-      __syncwarp();
+    for (int I = 1; I < NT; ++I) {
+      if (I > K) {
+        const double *t = M + tix(I, 0) + K * TILE;
+        pc[I][0] = 0.0;
+        pc[I][1] = 0.0;
+        mma(pc[I][0], pc[I][1], afrag(t, 0, lane), b0);
+        mma(pc[I][0], pc[I][1], afrag(t, 1, lane), b1);
+      }
     }
-    // trailing update: A_IJ -= L_IK L_JK^T, K < J <= I
-    for (int J = K + 1; J < NT; ++J) {
-      const double *lj = M + tix(J, K);
-      for (int I = J; I < NT; ++I) {
-        const double *li = M + tix(I, K);
-        double *t = M + tix(I, J);
-        double c0, c1;
-        load_c(t, lane, c0, c1);
+    __syncwarp();
 #pragma unroll
-        for (int s = 0; s < 2; ++s) mma(c0, c1, -afrag(li, s, lane), bfrag_t(lj, s, lane));
-        store_c(t, lane, c0, c1);
+    for (int I = 1; I < NT; ++I)
+      if (I > K) store_c(M + tix(I, 0) + K * TILE, lane, pc[I][0], pc[I][1]);
+    __syncwarp();
+    // A fragments of the new panel (= B fragments of its transpose)
+    double pa[NT][2];
+#pragma unroll
+    for (int I = 1; I < NT; ++I) {
+      if (I > K) {
+        pa[I][0] = afrag(M + tix(I, 0) + K * TILE, 0, lane);
+        pa[I][1] = afrag(M + tix(I, 0) + K * TILE, 1, lane);
+      }
+    }
+    // trailing update: A_IJ -= L_IK L_JK^T, K < J <= I (each lane touches its own C elements)
+#pragma unroll
+    for (int J = 1; J < NT; ++J) {
+      if (J > K) {
+        // keeps the loads of one column of tiles together (register pressure)
+        asm volatile("" ::: "memory");
+#pragma unroll
+        for (int I = J; I < NT; ++I) {
+          double *t = M + tix(I, J);
+          double c0, c1;
+          load_c(t, lane, c0, c1);
+          mma(c0, c1, -pa[I][0], pa[J][0]);
+          mma(c0, c1, -pa[I][1], pa[J][1]);
+          store_c(t, lane, c0, c1);
+        }
       }
     }
     __syncwarp();
@@ -149,29 +195,51 @@ __device__ __forceinline__ bool chol_blocked(double *M, double *scratch, double 
 }
 
 // In-place blocked inverse: on entry the diagonal tiles hold inv(L_II) and the
-// off-diagonal tiles L_IJ; on return the tiles hold X = L^-1.
-__device__ __forceinline__ void trtri_blocked(double *M, double *scratch, int NT, int lane) {
-  for (int J = 0; J < NT; ++J) {
-    for (int I = J + 1; I < NT; ++I) {
-      // acc = sum_{K=J}^{I-1} L_IK X_KJ
-      double c0 = 0.0, c1 = 0.0;
-      for (int K = J; K < I; ++K) {
-        const double *l = M + tix(I, K);
-        const double *x = M + tix(K, J);
+// off-diagonal tiles L_IJ; on return the tiles hold X = L^-1.  Row block by
+// row block: X_IJ = -inv(L_II) sum_{K=J}^{I-1} L_IK X_KJ needs the finished
+// rows above and the L tiles of row I only, so the I tiles of row I are
+// independent; their products are interleaved (K outer, J inner) and they are
+// stored together once all of them are computed.
+template <int NT>
+__device__ __forceinline__ void trtri_blocked(double *M, int lane) {
+#pragma unroll 1
+  for (int I = 1; I < NT; ++I) {
+    const double *rowI = M + tix(I, 0);
+    double c[NT][2];
 #pragma unroll
-        for (int s = 0; s < 2; ++s) mma(c0, c1, afrag(l, s, lane), bfrag(x, s, lane));
-      }
-      store_c(scratch, lane, c0, c1);
-      __syncwarp();
-      // X_IJ = -inv(L_II) acc
-      const double *di = M + tix(I, I);
-      double d0 = 0.0, d1 = 0.0;
-#pragma unroll
-      for (int s = 0; s < 2; ++s) mma(d0, d1, -afrag(di, s, lane), bfrag(scratch, s, lane));
-      __syncwarp();
-      store_c(M + tix(I, J), lane, d0, d1);
-      __syncwarp();
+    for (int J = 0; J < NT; ++J) {
+      c[J][0] = 0.0;
+      c[J][1] = 0.0;
     }
+#pragma unroll 1
+    for (int K = 0; K < I; ++K) {
+      const double a0 = afrag(rowI + K * TILE, 0, lane), a1 = afrag(rowI + K * TILE, 1, lane);
+      const double *rowK = M + (K * (K + 1) / 2) * TILE;
+#pragma unroll
+      for (int J = 0; J < NT - 1; ++J) {
+        if (J <= K) {
+          mma(c[J][0], c[J][1], a0, bfrag(rowK + J * TILE, 0, lane));
+          mma(c[J][0], c[J][1], a1, bfrag(rowK + J * TILE, 1, lane));
+        }
+      }
+    }
+    const double *di = rowI + I * TILE;
+    const double n0 = -afrag(di, 0, lane), n1 = -afrag(di, 1, lane);
+    double xo[NT][2];
+#pragma unroll
+    for (int J = 0; J < NT - 1; ++J) {
+      if (J < I) {
+        xo[J][0] = 0.0;
+        xo[J][1] = 0.0;
+        mma(xo[J][0], xo[J][1], n0, c_to_b(c[J][0], c[J][1], 0, lane));
+        mma(xo[J][0], xo[J][1], n1, c_to_b(c[J][0], c[J][1], 1, lane));
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int J = 0; J < NT - 1; ++J)
+      if (J < I) store_c(M + tix(I, 0) + J * TILE, lane, xo[J][0], xo[J][1]);
+    __syncwarp();
   }
 }
 

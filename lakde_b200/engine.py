@@ -93,6 +93,9 @@ class FusedVI:
     def _tri(self):
         return self.pattern.rowptr, self.pattern.col
 
+    # whether the trace factor T of _prior() is lower triangular
+    _T_lower = False
+
     def _prior(self):
         """(P, P batch, T) for the posterior factorisation; set by the model."""
         raise NotImplementedError
@@ -110,7 +113,7 @@ class FusedVI:
         K.posterior_factor(
             self.S, self.W_inv_jitter, self.eps, P=P, nu_0=self.nu_0_t, a=self.a, b=self.b,
             T=T if with_trace else None, info=self.info, out=self.U, logdet=self.logdet_W,
-            trace=self.trace if with_trace else None,
+            trace=self.trace if with_trace else None, T_lower=self._T_lower,
         )
         torch.minimum(self.failed, self.info.min(), out=self.failed)
 
@@ -214,6 +217,8 @@ class FusedKNN(FusedVI):
         sigma_0.diagonal(dim1=-2, dim2=-1).add_(self.sigma_0_jitter[:, None])
         self.sigma_0 = sigma_0
         self.sigma_0_tril = L0
+
+    _T_lower = True  # the Cholesky factor of Sigma0
 
     def _prior(self):
         return self.sigma_0, self.sigma_0_tril

@@ -177,12 +177,13 @@ def mstep(rowptr, col, r, X, nu_0, kernel_offset=0, S=None, nu=None):
 
 
 def posterior_factor(S, jitter, eps, P=None, nu_0=None, a=None, b=None, T=None, want_L=False, info=None, out=None,
-                     logdet=None, trace=None, L=None):
+                     logdet=None, trace=None, L=None, T_lower=False):
     """FP64 jittered Cholesky of A_n = nu_0 a_n / b_n P_n + S_n (see include/lakde_b200.h).
 
     Returns (W_triu, logdet_W, info, L or None, trace or None); ``jitter`` is
     updated in place.  ``P`` and ``T`` may be [D, D] (shared) or [N, D, D].
     Output buffers may be passed in (out, logdet, info, trace, L).
+    ``T_lower=True`` declares T lower triangular (its upper part is not read).
     """
     nat.require_cuda(S, jitter, P, nu_0, a, b, T, op="posterior_factor")
     N, D, _ = S.shape
@@ -214,7 +215,7 @@ def posterior_factor(S, jitter, eps, P=None, nu_0=None, a=None, b=None, T=None, 
         nat.lib().lakde_posterior_factor(
             nat.dtype_code(S), N, D, nat.ptr(S), nat.ptr(P), pbs, nat.ptr(nu_0), nat.ptr(a), nat.ptr(b),
             nat.ptr(jitter), float(eps), nat.ptr(W), nat.ptr(L), nat.ptr(logdet), nat.ptr(info), nat.ptr(T), tbs,
-            nat.ptr(trace), nat.stream_of(S),
+            int(bool(T_lower)), nat.ptr(trace), nat.stream_of(S),
         ),
         "posterior_factor",
     )

@@ -36,7 +36,7 @@ def test_header_and_library_agree(nat):
 
 def test_metadata(nat):
     lib = nat.lib()
-    assert lib.lakde_abi_version() == 1
+    assert lib.lakde_abi_version() == 2
     assert lib.lakde_max_dim() == 64
 
 
@@ -54,7 +54,7 @@ def test_invalid_arguments_are_rejected_on_the_host(nat):
     # an unsupported dtype code is reported as such
     assert lib.lakde_posterior_factor(7, 1, 2, ctypes.c_void_p(8), None, 0, None, None, None,
                                       ctypes.c_void_p(8), 0.0, ctypes.c_void_p(8), None, ctypes.c_void_p(8),
-                                      ctypes.c_void_p(8), None, 0, None, None) in (1, 2)
+                                      ctypes.c_void_p(8), None, 0, 0, None, None) in (1, 2)
 
 
 def test_cpu_tensors_are_rejected():

@@ -196,6 +196,15 @@ def test_factor_random(K, D, dtype):
     np.testing.assert_allclose(L.cpu().numpy(), Lr, rtol=rtol, atol=rtol * np.abs(Lr).max())
     np.testing.assert_allclose(logdet.cpu().numpy(), O.chol_logdet(Ur), rtol=rtol, atol=rtol * 10)
     np.testing.assert_allclose(trace.cpu().numpy(), O.chol_mm_trace(Tm.astype(np.float64), Ur), rtol=10 * rtol)
+    # declaring T lower triangular skips its upper part: same results, and
+    # garbage above the diagonal is not read
+    Tg = Tm + np.triu(rng.standard_normal((N, D, D)), 1).astype(dtype)
+    jit2 = t(np.zeros(N, dtype))
+    W2, logdet2, info2, _, trace2 = K.posterior_factor(t(S), jit2, np.finfo(dtype).eps, P=t(P), nu_0=t(nu0),
+                                                       a=t(a), b=t(b), T=t(Tg), T_lower=True)
+    torch.testing.assert_close(W2, W, rtol=0, atol=0)
+    torch.testing.assert_close(logdet2, logdet, rtol=0, atol=0)
+    np.testing.assert_allclose(trace2.cpu().numpy(), trace.cpu().numpy(), rtol=1e-12 if dtype == np.float64 else 1e-5)
 
 
 def test_factor_shared_prior_and_failure(K):
