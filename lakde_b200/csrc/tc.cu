@@ -147,13 +147,12 @@ struct EsmCfg {
   static constexpr uint32_t bytes = off_c + MT * 4 + 128;
 };
 
-__global__ void __launch_bounds__(128) estep_tc_kernel(TcArgs g) {
+__global__ void __launch_bounds__(128, 4) estep_tc_kernel(TcArgs g) {
   using C = EsmCfg;
   extern __shared__ __align__(128) unsigned char sm[];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t s_tmem;
   __shared__ float s_cst, s_expo;
-  __shared__ float s_xn[DP];
   unsigned char *Ahi = sm + C::off_Ahi, *Alo = sm + C::off_Alo, *Bhi = sm + C::off_Bhi, *Blo = sm + C::off_Blo;
   int32_t *cidx = reinterpret_cast<int32_t *>(sm + C::off_c);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -173,66 +172,121 @@ __global__ void __launch_bounds__(128) estep_tc_kernel(TcArgs g) {
   constexpr uint32_t A_SBO = KG * 128, A_LBO = 128;
   constexpr uint32_t B_SBO = 128, B_LBO = KG * 128;
   const uint32_t idesc = idesc_bf16(MT, DP, 0, 1);
+  // this thread's dimensions: 8 k + 2 (lane % 4) and + 1, k = 0 .. KG - 1
+  const int dq = 2 * (lane & 3);
 
-  for (int64_t it = blockIdx.x; it < g.N && alive; it += gridDim.x) {
-    const int64_t n = g.order ? (int64_t)g.order[it] : it;
-    const int64_t start = g.rowptr[n], end = g.rowptr[n + 1];
-    // stage W_triu[n] (rows j, columns i) as B = [K = j][N = i], hi and lo
+  // the next row's index and CSR bounds are loaded one row ahead
+  int64_t it = blockIdx.x;
+  int64_t n_nx = 0, start_nx = 0, end_nx = 0;
+  if (it < g.N) {
+    n_nx = g.order ? (int64_t)g.order[it] : it;
+    start_nx = g.rowptr[n_nx];
+    end_nx = g.rowptr[n_nx + 1];
+  }
+  for (; it < g.N && alive; it += gridDim.x) {
+    const int64_t n = n_nx, start = start_nx, end = end_nx;
+    const int64_t it2 = it + gridDim.x;
+    if (it2 < g.N) {
+      n_nx = g.order ? (int64_t)g.order[it2] : it2;
+      start_nx = g.rowptr[n_nx];
+      end_nx = g.rowptr[n_nx + 1];
+    }
+    // loads of the row, all issued before use: W_triu[n] (staged below as
+    // B = [K = j][N = i], hi and lo), this thread's coordinates of x_n, and
+    // nu_n / logdet_n for warp 0
     const float *Wn = g.W + n * (int64_t)D * D;
-    // lane -> row j = 8 jg + lane / 4, columns i = 8 ig + 2 (lane % 4), + 1 (bank-conflict-free stores)
-    for (int e = tid; e < DP * DP / 2; e += 128) {
+    float wv[DP * DP / 256][2];
+#pragma unroll
+    for (int m = 0; m < DP * DP / 256; ++m) {
+      const int e = tid + 128 * m;
       const int q = e >> 5, ln = e & 31;  // q: (jg, ig) block of 8 x 8
       const int j = 8 * (q / KG) + (ln >> 2), i = 8 * (q % KG) + 2 * (ln & 3);
-      const float w0 = (j < D && i < D) ? Wn[j * D + i] : 0.f;
-      const float w1 = (j < D && i + 1 < D) ? Wn[j * D + i + 1] : 0.f;
-      uint32_t hi, lo;
-      split2(w0, w1, hi, lo);
-      // B is MN-major: core (k group j/8, n group i/8), 16-byte line = row j of 8 n's
-      const uint32_t o = (uint32_t)(j >> 3) * B_LBO + (uint32_t)(i >> 3) * B_SBO + (uint32_t)(j & 7) * 16u +
-                         (uint32_t)(i & 7) * 2u;
-      *reinterpret_cast<uint32_t *>(Bhi + o) = hi;
-      *reinterpret_cast<uint32_t *>(Blo + o) = lo;
+      wv[m][0] = (j < D && i < D) ? Wn[j * D + i] : 0.f;
+      wv[m][1] = (j < D && i + 1 < D) ? Wn[j * D + i + 1] : 0.f;
     }
-    for (int d = tid; d < DP; d += 128) s_xn[d] = d < D ? g.X[n * D + d] : 0.f;
+    const float *xnp = g.X + n * (int64_t)D;
+    float xn[KG][2];
+#pragma unroll
+    for (int k = 0; k < KG; ++k) {
+      const int d0 = 8 * k + dq;
+      xn[k][0] = d0 < D ? xnp[d0] : 0.f;
+      xn[k][1] = d0 + 1 < D ? xnp[d0 + 1] : 0.f;
+    }
+    float nv = 0.f, ldn = 0.f;
     if (warp == 0) {
-      // multivariate digamma, one term per lane
-      const float nv = g.nu[n];
-      double md = 0.0;
-      for (int i = 1 + (tid & 31); i <= D; i += 32) md += digamma_d(0.5 * (double)nv + 0.5 * (1 - i));
-      md = warp_sum(md);
-      if (tid == 0) {
-        s_cst = (float)(0.5 * (md + D * 0.69314718055994530942 + (double)g.logdet[n]));
-        s_expo = -0.5f * nv;
+      nv = g.nu[n];
+      ldn = g.logdet[n];
+    }
+    // B is written once per row: the previous row's last MMAs have completed
+    // (their mbarrier wait) and every thread has passed the row-end barrier
+    if (end > start) {
+#pragma unroll
+      for (int m = 0; m < DP * DP / 256; ++m) {
+        const int e = tid + 128 * m;
+        const int q = e >> 5, ln = e & 31;
+        const int j = 8 * (q / KG) + (ln >> 2), i = 8 * (q % KG) + 2 * (ln & 3);
+        uint32_t hi, lo;
+        split2(wv[m][0], wv[m][1], hi, lo);
+        // B is MN-major: core (k group j/8, n group i/8), 16-byte line = row j of 8 n's
+        const uint32_t o = (uint32_t)(j >> 3) * B_LBO + (uint32_t)(i >> 3) * B_SBO + (uint32_t)(j & 7) * 16u +
+                           (uint32_t)(i & 7) * 2u;
+        *reinterpret_cast<uint32_t *>(Bhi + o) = hi;
+        *reinterpret_cast<uint32_t *>(Blo + o) = lo;
       }
     }
-    __syncthreads();
+    bool first = true;
     for (int64_t base = start; base < end; base += MT) {
       const int cnt = (int)((end - base) < MT ? (end - base) : MT);
-      // gather: warp w takes the 8-row batches w, w + 4, ...; lane l the row
-      // 8 b + l / 4 and, for each 8-dimension group k, dimensions 8 k + 2 (l % 4)
-      // and + 1.  Every store instruction then covers 8 rows of one core-matrix
-      // column (32 distinct banks) and every load 8 whole 32-byte sectors.
-      for (int bt = warp; bt < MT / 8; bt += 4) {
-        const int p = 8 * bt + (lane >> 2);
+      // gather: warp w takes the 8-row batches w, w + 4, w + 8, w + 12; lane
+      // l the row 8 b + l / 4 and, for each 8-dimension group k, dimensions
+      // 8 k + 2 (l % 4) and + 1.  Every store instruction then covers 8 rows
+      // of one core-matrix column (32 distinct banks).  All column indices,
+      // then all coordinates, are loaded before any is used.
+      constexpr int NB = MT / 32;
+      int32_t cb[NB];
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        const int p = 8 * (warp + 4 * b) + (lane >> 2);
         int32_t c = -1;
         if (p < cnt) {
           c = g.col[base + p];
           if (c < 0 || c >= g.npts) c = -1;
         }
-        if ((lane & 3) == 0) cidx[p] = c;
-        const float *xm = g.X + (int64_t)(c < 0 ? 0 : c) * D;
-        float v[KG][2];
+        cb[b] = c;
+      }
+      float v[NB][KG][2];
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        const float *xm = g.X + (int64_t)(cb[b] < 0 ? 0 : cb[b]) * D;
 #pragma unroll
         for (int k = 0; k < KG; ++k) {
-          const int d0 = 8 * k + 2 * (lane & 3);
-          v[k][0] = (c >= 0 && d0 < D) ? xm[d0] : 0.f;
-          v[k][1] = (c >= 0 && d0 + 1 < D) ? xm[d0 + 1] : 0.f;
+          const int d0 = 8 * k + dq;
+          v[b][k][0] = (cb[b] >= 0 && d0 < D) ? xm[d0] : 0.f;
+          v[b][k][1] = (cb[b] >= 0 && d0 + 1 < D) ? xm[d0 + 1] : 0.f;
         }
+      }
+      if (first) {
+        if (warp == 0) {
+          // multivariate digamma, one term per lane
+          double md = 0.0;
+          for (int i = 1 + lane; i <= D; i += 32) md += digamma_d(0.5 * (double)nv + 0.5 * (1 - i));
+          md = warp_sum(md);
+          if (lane == 0) {
+            s_cst = (float)(0.5 * (md + D * 0.69314718055994530942 + (double)ldn));
+            s_expo = -0.5f * nv;
+          }
+        }
+        first = false;
+      }
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        const int p = 8 * (warp + 4 * b) + (lane >> 2);
+        if ((lane & 3) == 0) cidx[p] = cb[b];
 #pragma unroll
         for (int k = 0; k < KG; ++k) {
-          const int d0 = 8 * k + 2 * (lane & 3);
-          const float x0 = (c >= 0 && d0 < D) ? v[k][0] - s_xn[d0] : 0.f;
-          const float x1 = (c >= 0 && d0 + 1 < D) ? v[k][1] - s_xn[d0 + 1] : 0.f;
+          const int d0 = 8 * k + dq;
+          const float x0 = cb[b] >= 0 ? v[b][k][0] - xn[k][0] : 0.f;
+          const float x1 = cb[b] >= 0 ? v[b][k][1] - xn[k][1] : 0.f;
           uint32_t hi, lo;
           split2(x0, x1, hi, lo);
           const uint32_t o = core_off(p, d0, A_SBO);
@@ -270,10 +324,10 @@ __global__ void __launch_bounds__(128) estep_tc_kernel(TcArgs g) {
         const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll
         for (int c0 = 0; c0 < DP; c0 += 16) {
-          float v[16];
-          tmem_ld16(taddr + c0, v);
+          float vv[16];
+          tmem_ld16(taddr + c0, vv);
 #pragma unroll
-          for (int k = 0; k < 16; ++k) q = fmaf(v[k], v[k], q);
+          for (int k = 0; k < 16; ++k) q = fmaf(vv[k], vv[k], q);
         }
       }
       if (tid < cnt) {
@@ -304,12 +358,11 @@ struct MsmCfg {
   static constexpr uint32_t bytes = G_BYTES + 128;
 };
 
-__global__ void __launch_bounds__(128) mstep_tc_kernel(TcArgs g) {
+__global__ void __launch_bounds__(128, 4) mstep_tc_kernel(TcArgs g) {
   using C = MsmCfg;
   extern __shared__ __align__(128) unsigned char sm[];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t s_tmem;
-  __shared__ float s_xn[DP];
   __shared__ float s_rs[4];
   unsigned char *G = sm;
   float *red = reinterpret_cast<float *>(sm);  // [DP][DP + 1] after the MMAs
@@ -333,20 +386,46 @@ __global__ void __launch_bounds__(128) mstep_tc_kernel(TcArgs g) {
   constexpr uint32_t SBO = 128, LBO = RS;
   const uint32_t idesc = idesc_bf16(128, DP, 1, 1);
 
-  for (int64_t it = blockIdx.x; it < g.N && alive; it += gridDim.x) {
-    const int64_t n = g.order ? (int64_t)g.order[it] : it;
-    const int64_t start = g.rowptr[n], end = g.rowptr[n + 1];
-    for (int d = tid; d < DP; d += 128) s_xn[d] = d < D ? g.X[n * D + d] : 0.f;
-    __syncthreads();
+  const int dq = 2 * (lane & 3);
+  // the next row's index and CSR bounds are loaded one row ahead
+  int64_t it = blockIdx.x;
+  int64_t n_nx = 0, start_nx = 0, end_nx = 0;
+  if (it < g.N) {
+    n_nx = g.order ? (int64_t)g.order[it] : it;
+    start_nx = g.rowptr[n_nx];
+    end_nx = g.rowptr[n_nx + 1];
+  }
+  for (; it < g.N && alive; it += gridDim.x) {
+    const int64_t n = n_nx, start = start_nx, end = end_nx;
+    const int64_t it2 = it + gridDim.x;
+    if (it2 < g.N) {
+      n_nx = g.order ? (int64_t)g.order[it2] : it2;
+      start_nx = g.rowptr[n_nx];
+      end_nx = g.rowptr[n_nx + 1];
+    }
+    const float *xnp = g.X + n * (int64_t)D;
+    float xn[KG][2];
+#pragma unroll
+    for (int k = 0; k < KG; ++k) {
+      const int d0 = 8 * k + dq;
+      xn[k][0] = d0 < D ? xnp[d0] : 0.f;
+      xn[k][1] = d0 + 1 < D ? xnp[d0 + 1] : 0.f;
+    }
     float rsum = 0.f;
     bool bad = end < start;
     int ntile = 0;
     for (int64_t base = start; base < end; base += MT, ++ntile) {
       const int cnt = (int)((end - base) < MT ? (end - base) : MT);
-      // gather: as in the E-step, warp w takes the 8-row batches w, w + 4, ...;
-      // lane l the row 8 b + l / 4 and the dimension pairs 8 k + 2 (l % 4)
-      for (int bt = warp; bt < MT / 8; bt += 4) {
-        const int p = 8 * bt + (lane >> 2);
+      // gather: as in the E-step, warp w takes the 8-row batches w, w + 4,
+      // w + 8, w + 12; lane l the row 8 b + l / 4 and the dimension pairs
+      // 8 k + 2 (l % 4); all indices and weights, then all coordinates, are
+      // loaded before any is used
+      constexpr int NB = MT / 32;
+      int32_t cb[NB];
+      float rb[NB];
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        const int p = 8 * (warp + 4 * b) + (lane >> 2);
         int32_t c = -1;
         float rv = 0.f;
         if (p < cnt) {
@@ -358,21 +437,30 @@ __global__ void __launch_bounds__(128) mstep_tc_kernel(TcArgs g) {
             rv = 0.f;
           }
         }
-        if ((lane & 3) == 0) rsum += rv;
-        const float w = sqrtf(rv > 0.f ? rv : 0.f);
-        const float *xm = g.X + (int64_t)(c < 0 ? 0 : c) * D;
-        float v[KG][2];
+        cb[b] = c;
+        rb[b] = rv;
+      }
+      float v[NB][KG][2];
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        const float *xm = g.X + (int64_t)(cb[b] < 0 ? 0 : cb[b]) * D;
 #pragma unroll
         for (int k = 0; k < KG; ++k) {
-          const int d0 = 8 * k + 2 * (lane & 3);
-          v[k][0] = (c >= 0 && d0 < D) ? xm[d0] : 0.f;
-          v[k][1] = (c >= 0 && d0 + 1 < D) ? xm[d0 + 1] : 0.f;
+          const int d0 = 8 * k + dq;
+          v[b][k][0] = (cb[b] >= 0 && d0 < D) ? xm[d0] : 0.f;
+          v[b][k][1] = (cb[b] >= 0 && d0 + 1 < D) ? xm[d0 + 1] : 0.f;
         }
+      }
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        const int p = 8 * (warp + 4 * b) + (lane >> 2);
+        if ((lane & 3) == 0) rsum += rb[b];
+        const float w = sqrtf(rb[b] > 0.f ? rb[b] : 0.f);
 #pragma unroll
         for (int k = 0; k < KG; ++k) {
-          const int d0 = 8 * k + 2 * (lane & 3);
-          const float x0 = (c >= 0 && d0 < D) ? w * (v[k][0] - s_xn[d0]) : 0.f;
-          const float x1 = (c >= 0 && d0 + 1 < D) ? w * (v[k][1] - s_xn[d0 + 1]) : 0.f;
+          const int d0 = 8 * k + dq;
+          const float x0 = cb[b] >= 0 ? w * (v[b][k][0] - xn[k][0]) : 0.f;
+          const float x1 = cb[b] >= 0 ? w * (v[b][k][1] - xn[k][1]) : 0.f;
           uint32_t hi, lo;
           split2(x0, x1, hi, lo);
           *reinterpret_cast<uint32_t *>(G + core_off(p, d0, RS)) = hi;
