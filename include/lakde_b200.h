@@ -215,13 +215,15 @@ LAKDE_API int lakde_estep_tc(int dtype, int64_t N, int64_t D, int64_t npts,
 /*
  * Mixed-precision tensor-core M-step (tcgen05): S_n and nu_n of lakde_mstep
  * for kernels 0..N-1 of X, D <= 64, float32 values (S is symmetric up to the
- * order of the fp32 accumulation).  *err as in lakde_estep_tc.
+ * order of the fp32 accumulation).  lower_only != 0 writes only the lower
+ * triangle (j <= i) of each S_n and leaves the rest untouched (all
+ * lakde_posterior_factor reads).  *err as in lakde_estep_tc.
  */
 LAKDE_API int lakde_mstep_tc(int dtype, int64_t N, int64_t D, int64_t npts,
                              const void *rowptr, const void *col,
                              const void *order, const void *r, const void *X,
-                             double nu_0, void *S, void *nu, int32_t *err,
-                             void *stream);
+                             double nu_0, void *S, void *nu, int lower_only,
+                             int32_t *err, void *stream);
 
 /*
  * Per-point normaliser, responsibilities and rebalance over a pair pattern

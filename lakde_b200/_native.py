@@ -64,7 +64,8 @@ _SIGNATURES = {
         _c_int,
     ),
     "lakde_mstep_tc": (
-        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_vp, _c_vp, _c_vp, _c_vp],
+        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_vp, _c_vp, _c_int, _c_vp,
+         _c_vp],
         _c_int,
     ),
     "lakde_estep_normalise": (

@@ -129,6 +129,7 @@ struct TcArgs {
   float *logrho;        // E-step output
   float *S;             // M-step output [N, D, D]
   float *nu_out;        // M-step output
+  int lower_only;       // M-step: write only j <= i of S_n
   float nu0;
   int64_t npts;
   int64_t N;
@@ -519,8 +520,9 @@ __global__ void __launch_bounds__(128, 4) mstep_tc_kernel(TcArgs g) {
       g.nu_out[n] = any_bad ? NAN : nv;
     }
     if (warp < 2) {
+      // row i of S into shared memory (row stride DP + 1: conflict-free both
+      // here, a thread per row, and below, a warp per row)
       const int i = tid;
-      float *Srow = g.S + n * (int64_t)D * D + (int64_t)i * D;
 #pragma unroll
       for (int c0 = 0; c0 < DP; c0 += 16) {
         if (end > start) {
@@ -530,17 +532,23 @@ __global__ void __launch_bounds__(128, 4) mstep_tc_kernel(TcArgs g) {
 #pragma unroll
           for (int k = 0; k < 16; ++k) v1[k] = v2[k] = 0.f;
         }
-        if (i < D) {
 #pragma unroll
-          for (int k = 0; k < 16; ++k) {
-            const int j = c0 + k;
-            const float s = (end > start) ? v1[k] + red[i * (DP + 1) + j] + v2[k] : 0.f;
-            if (j < D) Srow[j] = any_bad ? NAN : s;
-          }
+        for (int k = 0; k < 16; ++k) {
+          float *rv = red + i * (DP + 1) + c0 + k;
+          *rv = (end > start) ? v1[k] + *rv + v2[k] : 0.f;
         }
       }
     }
     fence_before();
+    __syncthreads();
+    // coalesced stores: warp w writes rows w, w + 4, ..., lanes along the row
+    {
+      float *Sn = g.S + n * (int64_t)D * D;
+      for (int i = warp; i < D; i += 4) {
+        const int jend = g.lower_only ? i + 1 : D;
+        for (int j = lane; j < jend; j += 32) Sn[(int64_t)i * D + j] = any_bad ? NAN : red[i * (DP + 1) + j];
+      }
+    }
     __syncthreads();
   }
   __syncthreads();
@@ -623,7 +631,7 @@ extern "C" int lakde_estep_tc(int dtype, int64_t N, int64_t D, int64_t npts, con
 
 extern "C" int lakde_mstep_tc(int dtype, int64_t N, int64_t D, int64_t npts, const void *rowptr, const void *col,
                               const void *order, const void *r, const void *X, double nu_0, void *S, void *nu,
-                              int32_t *err, void *stream) {
+                              int lower_only, int32_t *err, void *stream) {
   clear_error();
   if (int st = tc_common_checks("mstep_tc", dtype, N, D, npts)) return st;
   if (N == 0) return LAKDE_OK;
@@ -641,6 +649,7 @@ extern "C" int lakde_mstep_tc(int dtype, int64_t N, int64_t D, int64_t npts, con
   g.S = static_cast<float *>(S);
   g.nu_out = static_cast<float *>(nu);
   g.nu0 = (float)nu_0;
+  g.lower_only = lower_only != 0;
   g.npts = npts;
   g.N = N;
   g.D = (int)D;

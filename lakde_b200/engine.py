@@ -104,7 +104,8 @@ class FusedVI:
     def mstep(self):
         rowptr, col = self._tri()
         if self.precision == "mixed":
-            K.mstep_tc(rowptr, col, self.r, self.X, self.nu_0, self.err, order=self.pattern.order, S=self.S, nu=self.nu)
+            K.mstep_tc(rowptr, col, self.r, self.X, self.nu_0, self.err, order=self.pattern.order, S=self.S, nu=self.nu,
+                       lower_only=True)
         else:
             K.mstep(rowptr, col, self.r, self.X, self.nu_0, S=self.S, nu=self.nu)
 
@@ -152,7 +153,8 @@ class FusedVI:
         nu = torch.empty_like(self.nu)
         rowptr, col = self._tri()
         if self.precision == "mixed":
-            K.mstep_tc(rowptr, col, self.r, self.X, self.nu_0, self.err, order=self.pattern.order, S=S, nu=nu)
+            K.mstep_tc(rowptr, col, self.r, self.X, self.nu_0, self.err, order=self.pattern.order, S=S, nu=nu,
+                       lower_only=True)
         else:
             K.mstep(rowptr, col, self.r, self.X, self.nu_0, S=S, nu=nu)
         P, _ = self._prior()

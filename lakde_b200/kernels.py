@@ -358,8 +358,10 @@ def estep_tc(rowptr, col, X, W_triu, nu, logdet_W, err, order=None, out=None):
     return out
 
 
-def mstep_tc(rowptr, col, r, X, nu_0, err, order=None, S=None, nu=None):
-    """Tensor-core (bf16 hi + lo) M-step S and nu, D <= 64 (see include/lakde_b200.h)."""
+def mstep_tc(rowptr, col, r, X, nu_0, err, order=None, S=None, nu=None, lower_only=False):
+    """Tensor-core (bf16 hi + lo) M-step S and nu, D <= 64 (see include/lakde_b200.h).
+
+    ``lower_only=True`` writes only the lower triangle of each S_n."""
     nat.require_cuda(rowptr, col, r, X, err, order, op="mstep_tc")
     assert rowptr.dtype == torch.int64 and col.dtype == torch.int32 and err.dtype == torch.int32
     N = rowptr.numel() - 1
@@ -369,7 +371,8 @@ def mstep_tc(rowptr, col, r, X, nu_0, err, order=None, S=None, nu=None):
     nat.check(
         nat.lib().lakde_mstep_tc(
             nat.dtype_code(X), N, D, X.size(0), nat.ptr(rowptr), nat.ptr(col), nat.ptr(order), nat.ptr(r),
-            nat.ptr(X), float(nu_0), nat.ptr(S), nat.ptr(nu), nat.ptr(err), nat.stream_of(X),
+            nat.ptr(X), float(nu_0), nat.ptr(S), nat.ptr(nu), int(bool(lower_only)), nat.ptr(err),
+            nat.stream_of(X),
         ),
         "mstep_tc",
     )

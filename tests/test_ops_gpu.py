@@ -403,6 +403,13 @@ def test_mstep_tc_matches_fp64(K, D):
     assert (np.abs(S - Sr) <= 2e-4 * scale).all()
     nur = D + 1.0 + np.bincount(O._rows_of(rowptr), weights=r.astype(np.float64), minlength=N)
     np.testing.assert_allclose(nu.cpu().numpy(), nur, rtol=1e-5)
+    # lower_only: the same lower triangle, the upper part left as it was
+    S2 = torch.full((N, D, D), 7.0, device=DEV)
+    K.mstep_tc(t(rowptr), t(cols, torch.int32), t(r), t(X), D + 1.0, err, S=S2, lower_only=True)
+    S2 = S2.cpu().numpy()
+    low = np.tril(np.ones((D, D), dtype=bool))
+    np.testing.assert_array_equal(S2[:, low], S[:, low])
+    assert (S2[:, ~low] == 7.0).all()
 
 
 def test_mstep_tc_long_rows_accumulate_over_tiles(K):
