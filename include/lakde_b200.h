@@ -201,20 +201,21 @@ LAKDE_API int lakde_vi_cta(int dtype, int64_t N, int64_t D, int64_t npts,
 /*
  * Mixed-precision tensor-core E-step (tcgen05, bf16 hi + lo split, fp32
  * accumulation in tensor memory), D <= 64, float32 values: the logrho of
- * lakde_estep_logrho for kernels 0..N-1 of X (no kernel offset), rows visited in
- * `order` (may be NULL).  *err is set to 1 if a tensor-core completion wait
- * times out (the affected rows are left unwritten).
+ * lakde_estep_logrho for rows n = 0..N-1, row n being kernel n + kernel_offset
+ * of X, rows visited in `order` (may be NULL).  *err is set to 1 if a
+ * tensor-core completion wait times out (the affected rows are left unwritten).
  */
 LAKDE_API int lakde_estep_tc(int dtype, int64_t N, int64_t D, int64_t npts,
                              const void *rowptr, const void *col,
                              const void *order, const void *X,
-                             const void *W_triu, const void *nu,
-                             const void *logdet_W, void *logrho, int32_t *err,
-                             void *stream);
+                             int64_t kernel_offset, const void *W_triu,
+                             const void *nu, const void *logdet_W, void *logrho,
+                             int32_t *err, void *stream);
 
 /*
  * Mixed-precision tensor-core M-step (tcgen05): S_n and nu_n of lakde_mstep
- * for kernels 0..N-1 of X, D <= 64, float32 values (S is symmetric up to the
+ * for rows n = 0..N-1, row n being kernel n + kernel_offset of X, D <= 64,
+ * float32 values (S is symmetric up to the
  * order of the fp32 accumulation).  lower_only != 0 writes only the lower
  * triangle (j <= i) of each S_n and leaves the rest untouched (all
  * lakde_posterior_factor reads).  *err as in lakde_estep_tc.
@@ -222,8 +223,9 @@ LAKDE_API int lakde_estep_tc(int dtype, int64_t N, int64_t D, int64_t npts,
 LAKDE_API int lakde_mstep_tc(int dtype, int64_t N, int64_t D, int64_t npts,
                              const void *rowptr, const void *col,
                              const void *order, const void *r, const void *X,
-                             double nu_0, void *S, void *nu, int lower_only,
-                             int32_t *err, void *stream);
+                             int64_t kernel_offset, double nu_0, void *S,
+                             void *nu, int lower_only, int32_t *err,
+                             void *stream);
 
 /*
  * Per-point normaliser, responsibilities and rebalance over a pair pattern
@@ -241,6 +243,29 @@ LAKDE_API int lakde_estep_normalise(int dtype, int64_t npts, const void *cptr,
                           const void *pos, int pos_dtype, const void *logrho,
                           void *r, void *c, void *rsum, int mode,
                           double threshold, void *stream);
+
+/*
+ * lakde_estep_normalise split into four stages for kernels sharded over
+ * devices (each device holds the pairs of its kernels; cptr / pos index its
+ * own pairs, over all npts points).  The caller reduces over the devices
+ * between stages: red by max after stage 0, red2 by sum after stages 1 and 2,
+ * rsum by sum after stage 3.
+ *   stage 0: red[m]  = max_local logrho
+ *   stage 1: red2[m] = sum_local exp(logrho - red[m])
+ *   stage 2: c_new from (c, rsum, red + log red2) as in lakde_estep_normalise;
+ *            red[m] = c_new, red2[m] = sum_local of the thresholded r
+ *   stage 3: c[m] = c_new + log(max(red2, eps)), r = r / red2 (clamped) on the
+ *            local pairs, rsum[m] = sum_local of the new r
+ * With one device (no reduction) the result equals lakde_estep_normalise.
+ * No counterpart of its own in the reference, whose rebalance runs on one
+ * device (lakde/local_adaptive_kde.py:120-181).  red, red2: dtype [npts].
+ */
+LAKDE_API int lakde_estep_normalise_stage(int dtype, int stage, int64_t npts,
+                                          const void *cptr, const void *pos,
+                                          int pos_dtype, const void *logrho,
+                                          void *r, void *c, void *rsum, void *red,
+                                          void *red2, int mode, double threshold,
+                                          void *stream);
 
 /*
  * Student-t log coefficients of the predictive density:

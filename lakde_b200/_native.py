@@ -60,16 +60,22 @@ _SIGNATURES = {
         _c_int,
     ),
     "lakde_estep_tc": (
-        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
+        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
+         _c_vp],
         _c_int,
     ),
     "lakde_mstep_tc": (
-        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_vp, _c_vp, _c_int, _c_vp,
-         _c_vp],
+        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64, _c_dbl, _c_vp, _c_vp, _c_int,
+         _c_vp, _c_vp],
         _c_int,
     ),
     "lakde_estep_normalise": (
         [_c_int, _c_i64, _c_vp, _c_vp, _c_int, _c_vp, _c_vp, _c_vp, _c_vp, _c_int, _c_dbl, _c_vp],
+        _c_int,
+    ),
+    "lakde_estep_normalise_stage": (
+        [_c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_int, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_int, _c_dbl,
+         _c_vp],
         _c_int,
     ),
     "lakde_pred_coeff": ([_c_int, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),

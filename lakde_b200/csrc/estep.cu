@@ -170,9 +170,107 @@ __global__ void __launch_bounds__(256) estep_normalise_kernel(const int64_t *__r
   }
 }
 
+// The per-point pass split into stages around cross-shard reductions (kernels
+// sharded over devices, every device holding the pairs of its kernels, the
+// point-major view cptr / pos over its own pairs).  Between stages the caller
+// reduces `red` / `red2` over the shards (max after stage 0, sums after 1, 2
+// and 3: rsum).  Per point m, over the local pairs:
+//   stage 0: red[m] = max logrho
+//   stage 1: red2[m] = sum exp(logrho - red[m])          (red = global max)
+//   stage 2: lse = red + log(red2) (global); c_new = normaliser update of
+//            (c[m], rsum[m], lse); red[m] = c_new; red2[m] = sum r (thresholded)
+//   stage 3: (red = c_new, red2 = global sum) coeff, c[m] = c_fin,
+//            r = r * coeff on the local pairs, rsum[m] = local sum of the new r
+// The arithmetic is that of estep_normalise_kernel.
+template <typename T, typename PI>
+__global__ void __launch_bounds__(256) estep_normalise_stage_kernel(const int64_t *__restrict__ cptr,
+                                                                    const PI *__restrict__ pos,
+                                                                    const T *__restrict__ logrho, T *__restrict__ r,
+                                                                    T *__restrict__ c, T *__restrict__ rsum,
+                                                                    T *__restrict__ red, T *__restrict__ red2,
+                                                                    int64_t npts, int stage, NormParams<T> np) {
+  const int lane = threadIdx.x & 31;
+  const int64_t m = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (m >= npts) return;
+  const int64_t s = cptr[m], e = cptr[m + 1];
+  if (stage == 0) {
+    T mx = neg_inf<T>();
+    for (int64_t p = s + lane; p < e; p += 32) mx = fmax(mx, logrho[pos[p]]);
+    mx = warp_max(mx);
+    if (lane == 0) red[m] = mx;
+  } else if (stage == 1) {
+    const T mx = red[m];
+    T se = T(0);
+    if (mx != neg_inf<T>())
+      for (int64_t p = s + lane; p < e; p += 32) se += exp(logrho[pos[p]] - mx);
+    se = warp_sum(se);
+    if (lane == 0) red2[m] = se;
+  } else if (stage == 2) {
+    const T mx = red[m];
+    const T lse = (mx == neg_inf<T>()) ? mx : mx + log(red2[m]);
+    const T c_new = normaliser_update(c[m], rsum[m], lse, np.mode);
+    T sum = T(0);
+    for (int64_t p = s + lane; p < e; p += 32) sum += responsibility(logrho[pos[p]], c_new, np.thr);
+    sum = warp_sum(sum);
+    __syncwarp();
+    if (lane == 0) {
+      red[m] = c_new;
+      red2[m] = sum;
+    }
+  } else {
+    const T c_new = red[m];
+    T c_fin;
+    const T coeff = clamp_coeff(red2[m], np, &c_fin, c_new);
+    T rs = T(0);
+    for (int64_t p = s + lane; p < e; p += 32) {
+      const T rv = responsibility(logrho[pos[p]], c_new, np.thr) * coeff;
+      r[pos[p]] = rv;
+      rs += rv;
+    }
+    rs = warp_sum(rs);
+    if (lane == 0) {
+      c[m] = c_fin;
+      rsum[m] = rs;
+    }
+  }
+}
+
 }  // namespace lakde
 
 using namespace lakde;
+
+extern "C" int lakde_estep_normalise_stage(int dtype, int stage, int64_t npts, const void *cptr, const void *pos,
+                                           int pos_dtype, const void *logrho, void *r, void *c, void *rsum,
+                                           void *red, void *red2, int mode, double threshold, void *stream) {
+  clear_error();
+  if (npts < 0 || (mode != 0 && mode != 1) || stage < 0 || stage > 3) {
+    set_error("estep_normalise_stage: invalid arguments");
+    return LAKDE_EINVAL;
+  }
+  if (npts == 0) return LAKDE_OK;
+  if (!cptr || !c || !rsum || !red || !red2) {
+    set_error("estep_normalise_stage: null pointer");
+    return LAKDE_EINVAL;
+  }
+  if (int st = bind_device("estep_normalise_stage", {c, cptr, pos, logrho, r, rsum, red, red2})) return st;
+  return dispatch_float(dtype, [&](auto t0) {
+    using T = decltype(t0);
+    return dispatch_index(pos_dtype, [&](auto p0) {
+      using PI = decltype(p0);
+      const int64_t threads = npts * 32;
+      const unsigned blocks = (unsigned)((threads + 255) / 256);
+      const T eps = std::is_same<T, float>::value ? (T)1.1920928955078125e-07 : (T)2.220446049250313e-16;
+      const T tiny = std::is_same<T, float>::value ? (T)1.1754943508222875e-38 : (T)2.2250738585072014e-308;
+      const T big = std::is_same<T, float>::value ? (T)3.4028234663852886e+38 : (T)1.7976931348623157e+308;
+      NormParams<T> np{mode, (T)threshold, eps, tiny, big};
+      estep_normalise_stage_kernel<T, PI><<<blocks, 256, 0, as_stream(stream)>>>(
+          static_cast<const int64_t *>(cptr), static_cast<const PI *>(pos), static_cast<const T *>(logrho),
+          static_cast<T *>(r), static_cast<T *>(c), static_cast<T *>(rsum), static_cast<T *>(red),
+          static_cast<T *>(red2), npts, stage, np);
+      return check_launch("estep_normalise_stage");
+    });
+  });
+}
 
 extern "C" int lakde_estep_logrho(int dtype, int64_t N, int64_t D, int64_t npts, const void *rowptr,
                                   int rowptr_dtype, const void *col, int col_dtype, const void *X,

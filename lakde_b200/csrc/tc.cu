@@ -133,6 +133,7 @@ struct TcArgs {
   float nu0;
   int64_t npts;
   int64_t N;
+  int64_t koff;  // row n is kernel n + koff of X
   int D;
   int *err;
 };
@@ -205,7 +206,7 @@ __global__ void __launch_bounds__(128, 4) estep_tc_kernel(TcArgs g) {
       wv[m][0] = (j < D && i < D) ? Wn[j * D + i] : 0.f;
       wv[m][1] = (j < D && i + 1 < D) ? Wn[j * D + i + 1] : 0.f;
     }
-    const float *xnp = g.X + n * (int64_t)D;
+    const float *xnp = g.X + (n + g.koff) * (int64_t)D;
     float xn[KG][2];
 #pragma unroll
     for (int k = 0; k < KG; ++k) {
@@ -336,7 +337,7 @@ __global__ void __launch_bounds__(128, 4) estep_tc_kernel(TcArgs g) {
         float lr = NAN;
         if (ok && c >= 0) {
           lr = __fadd_rn(__fmul_rn(q, s_expo), s_cst);
-          if ((int64_t)c == n) lr = -INFINITY;
+          if ((int64_t)c == n + g.koff) lr = -INFINITY;
         }
         g.logrho[base + tid] = lr;
       }
@@ -404,7 +405,7 @@ __global__ void __launch_bounds__(128, 4) mstep_tc_kernel(TcArgs g) {
       start_nx = g.rowptr[n_nx];
       end_nx = g.rowptr[n_nx + 1];
     }
-    const float *xnp = g.X + n * (int64_t)D;
+    const float *xnp = g.X + (n + g.koff) * (int64_t)D;
     float xn[KG][2];
 #pragma unroll
     for (int k = 0; k < KG; ++k) {
@@ -561,12 +562,12 @@ __global__ void __launch_bounds__(128, 4) mstep_tc_kernel(TcArgs g) {
 
 using namespace lakde;
 
-static int tc_common_checks(const char *what, int dtype, int64_t N, int64_t D, int64_t npts) {
+static int tc_common_checks(const char *what, int dtype, int64_t N, int64_t D, int64_t npts, int64_t koff) {
   if (dtype != LAKDE_F32) {
     set_error("%s: float32 values only", what);
     return LAKDE_EDTYPE;
   }
-  if (N < 0 || D < 1 || npts < N) {
+  if (N < 0 || D < 1 || koff < 0 || npts < N + koff) {
     set_error("%s: invalid sizes", what);
     return LAKDE_EINVAL;
   }
@@ -594,10 +595,10 @@ static int tc_grid(size_t smem, int tmem_cols, int64_t N, unsigned *grid) {
 }
 
 extern "C" int lakde_estep_tc(int dtype, int64_t N, int64_t D, int64_t npts, const void *rowptr, const void *col,
-                              const void *order, const void *X, const void *W_triu, const void *nu,
-                              const void *logdet_W, void *logrho, int32_t *err, void *stream) {
+                              const void *order, const void *X, int64_t kernel_offset, const void *W_triu,
+                              const void *nu, const void *logdet_W, void *logrho, int32_t *err, void *stream) {
   clear_error();
-  if (int st = tc_common_checks("estep_tc", dtype, N, D, npts)) return st;
+  if (int st = tc_common_checks("estep_tc", dtype, N, D, npts, kernel_offset)) return st;
   if (N == 0) return LAKDE_OK;
   if (!rowptr || !col || !X || !W_triu || !nu || !logdet_W || !logrho || !err) {
     set_error("estep_tc: null pointer");
@@ -614,6 +615,7 @@ extern "C" int lakde_estep_tc(int dtype, int64_t N, int64_t D, int64_t npts, con
   g.logdet = static_cast<const float *>(logdet_W);
   g.logrho = static_cast<float *>(logrho);
   g.npts = npts;
+  g.koff = kernel_offset;
   g.N = N;
   g.D = (int)D;
   g.err = err;
@@ -630,10 +632,10 @@ extern "C" int lakde_estep_tc(int dtype, int64_t N, int64_t D, int64_t npts, con
 }
 
 extern "C" int lakde_mstep_tc(int dtype, int64_t N, int64_t D, int64_t npts, const void *rowptr, const void *col,
-                              const void *order, const void *r, const void *X, double nu_0, void *S, void *nu,
-                              int lower_only, int32_t *err, void *stream) {
+                              const void *order, const void *r, const void *X, int64_t kernel_offset, double nu_0,
+                              void *S, void *nu, int lower_only, int32_t *err, void *stream) {
   clear_error();
-  if (int st = tc_common_checks("mstep_tc", dtype, N, D, npts)) return st;
+  if (int st = tc_common_checks("mstep_tc", dtype, N, D, npts, kernel_offset)) return st;
   if (N == 0) return LAKDE_OK;
   if (!rowptr || !col || !r || !X || !S || !nu || !err) {
     set_error("mstep_tc: null pointer");
@@ -651,6 +653,7 @@ extern "C" int lakde_mstep_tc(int dtype, int64_t N, int64_t D, int64_t npts, con
   g.nu0 = (float)nu_0;
   g.lower_only = lower_only != 0;
   g.npts = npts;
+  g.koff = kernel_offset;
   g.N = N;
   g.D = (int)D;
   g.err = err;

@@ -276,6 +276,21 @@ def estep_normalise(cptr, pos, logrho, r, c, rsum, mode, threshold):
     )
 
 
+def estep_normalise_stage(stage, cptr, pos, logrho, r, c, rsum, red, red2, mode, threshold):
+    """One stage of the per-point pass for kernels sharded over devices (see
+    include/lakde_b200.h); the caller reduces red / red2 / rsum between stages."""
+    nat.require_cuda(cptr, pos, logrho, r, c, rsum, red, red2, op="estep_normalise_stage")
+    assert cptr.dtype == torch.int64
+    nat.check(
+        nat.lib().lakde_estep_normalise_stage(
+            nat.dtype_code(c), int(stage), c.numel(), nat.ptr(cptr), nat.ptr(pos), nat.dtype_code(pos),
+            nat.ptr(logrho), nat.ptr(r), nat.ptr(c), nat.ptr(rsum), nat.ptr(red), nat.ptr(red2), int(mode),
+            float(threshold or 0.0), nat.stream_of(c),
+        ),
+        "estep_normalise_stage",
+    )
+
+
 def pred_coeff(nu, logdet_W, D, out=None):
     nat.require_cuda(nu, logdet_W, op="pred_coeff")
     out = torch.empty_like(nu) if out is None else out
@@ -342,8 +357,9 @@ def log_pred_density_bwd(X, W_triu, nu, log_coeff, Y, out, grad_out):
     return gY, sw, S_c
 
 
-def estep_tc(rowptr, col, X, W_triu, nu, logdet_W, err, order=None, out=None):
-    """Tensor-core (bf16 hi + lo) E-step numerators, D <= 64 (see include/lakde_b200.h)."""
+def estep_tc(rowptr, col, X, W_triu, nu, logdet_W, err, order=None, out=None, kernel_offset=0):
+    """Tensor-core (bf16 hi + lo) E-step numerators, D <= 64 (see include/lakde_b200.h).
+    Row n of rowptr is kernel n + kernel_offset of X."""
     nat.require_cuda(rowptr, col, X, W_triu, nu, logdet_W, err, order, op="estep_tc")
     assert rowptr.dtype == torch.int64 and col.dtype == torch.int32 and err.dtype == torch.int32
     N = rowptr.numel() - 1
@@ -351,17 +367,19 @@ def estep_tc(rowptr, col, X, W_triu, nu, logdet_W, err, order=None, out=None):
     nat.check(
         nat.lib().lakde_estep_tc(
             nat.dtype_code(X), N, X.size(1), X.size(0), nat.ptr(rowptr), nat.ptr(col), nat.ptr(order), nat.ptr(X),
-            nat.ptr(W_triu), nat.ptr(nu), nat.ptr(logdet_W), nat.ptr(out), nat.ptr(err), nat.stream_of(X),
+            int(kernel_offset), nat.ptr(W_triu), nat.ptr(nu), nat.ptr(logdet_W), nat.ptr(out), nat.ptr(err),
+            nat.stream_of(X),
         ),
         "estep_tc",
     )
     return out
 
 
-def mstep_tc(rowptr, col, r, X, nu_0, err, order=None, S=None, nu=None, lower_only=False):
+def mstep_tc(rowptr, col, r, X, nu_0, err, order=None, S=None, nu=None, lower_only=False, kernel_offset=0):
     """Tensor-core (bf16 hi + lo) M-step S and nu, D <= 64 (see include/lakde_b200.h).
 
-    ``lower_only=True`` writes only the lower triangle of each S_n."""
+    ``lower_only=True`` writes only the lower triangle of each S_n; row n of
+    rowptr is kernel n + kernel_offset of X."""
     nat.require_cuda(rowptr, col, r, X, err, order, op="mstep_tc")
     assert rowptr.dtype == torch.int64 and col.dtype == torch.int32 and err.dtype == torch.int32
     N = rowptr.numel() - 1
@@ -371,7 +389,7 @@ def mstep_tc(rowptr, col, r, X, nu_0, err, order=None, S=None, nu=None, lower_on
     nat.check(
         nat.lib().lakde_mstep_tc(
             nat.dtype_code(X), N, D, X.size(0), nat.ptr(rowptr), nat.ptr(col), nat.ptr(order), nat.ptr(r),
-            nat.ptr(X), float(nu_0), nat.ptr(S), nat.ptr(nu), int(bool(lower_only)), nat.ptr(err),
+            nat.ptr(X), int(kernel_offset), float(nu_0), nat.ptr(S), nat.ptr(nu), int(bool(lower_only)), nat.ptr(err),
             nat.stream_of(X),
         ),
         "mstep_tc",
