@@ -39,6 +39,9 @@ WORKLOADS = {
              "LocalKNearestKDE d=8 N_train=200000 N_test=20000 K=50 (10-component heavy-tail mixture)"),
     "bsds63": (dict(n_train=1_000_000, n_test=16_384), 100, 5e-4,
                "LocalKNearestKDE d=63 N_train=1000000 N_test=16384 K=100 (20-component decaying-spectrum mixture)"),
+    "bsds63s": (dict(n_train=50_000, n_test=1_024), 100, 5e-4,
+                "LocalKNearestKDE d=63 N_train=50000 N_test=1024 K=100 (the bsds63 mixture, small case for "
+                "profiling)"),
     "spec21": (dict(n_train=300_000, n_test=4_096), 64, 5e-4,
                "LocalKNearestKDE d=21 N_train=300000 N_test=4096 K=64 (12-component mixture)"),
     "circle2d": (dict(n_train=2_000, n_test=1_000), 20, 0.0,
@@ -51,6 +54,7 @@ def make_data(name):
 
     kw, k, thr, desc = WORKLOADS[name]
     gen = {"gas8": syn.heavy_tail_mixture, "bsds63": syn.decaying_spectrum_mixture,
+           "bsds63s": syn.decaying_spectrum_mixture,
            "spec21": syn.wide_spectrum_mixture, "circle2d": syn.circle_gmm}[name]
     Xtr, Xte = gen(seed=0, **kw)
     return Xtr, Xte, k, thr, desc

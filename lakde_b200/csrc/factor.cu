@@ -185,14 +185,6 @@ struct DmmaCfg {
   static constexpr size_t smem = (size_t)WPB * per_warp * sizeof(double);
 };
 
-// Pulls one matrix (bytes from p) into L2 ahead of its use, one 128-byte line
-// per lane and step; every address issued lies inside the matrix.
-__device__ __forceinline__ void prefetch_l2(const void *p, int64_t bytes, int lane) {
-  const char *c = static_cast<const char *>(p);
-  for (int64_t off = (int64_t)lane * 128; off < bytes; off += 32 * 128)
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(c + off));
-}
-
 // A_ij + jt [i == j] in the model dtype (the rounding of the reference's
 // separate tensor ops), as FP64; rows i >= D are the identity padding.
 template <typename T>
@@ -447,8 +439,8 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
   }
 }
 
-// Persistent: each warp walks matrices n, n + stride, ... and pulls the next
-// one's inputs into L2 before factorising the current one.
+// Persistent: each warp walks matrices n, n + stride, ... (a grid of exactly
+// the resident blocks).
 template <typename T, int DP>
 __global__ void __launch_bounds__(32 * DmmaCfg<DP>::WPB) factor_dmma_kernel(FactorArgs<T> g) {
   using C = DmmaCfg<DP>;
@@ -456,14 +448,7 @@ __global__ void __launch_bounds__(32 * DmmaCfg<DP>::WPB) factor_dmma_kernel(Fact
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double *M = smem_d + warp * C::per_warp;
   const int64_t stride = (int64_t)gridDim.x * C::WPB;
-  const int64_t DD = (int64_t)g.D * g.D;
   for (int64_t n = (int64_t)blockIdx.x * C::WPB + warp; n < g.N; n += stride) {
-    const int64_t nx = n + stride;
-    if (nx < g.N) {
-      prefetch_l2(g.S + nx * DD, DD * (int64_t)sizeof(T), lane);
-      if (g.P && g.Pbs) prefetch_l2(g.P + nx * g.Pbs, DD * (int64_t)sizeof(T), lane);
-      if (g.Tm && g.Tbs) prefetch_l2(g.Tm + nx * g.Tbs, DD * (int64_t)sizeof(T), lane);
-    }
     factor_one<T, DP>(g, n, M, lane);
     __syncwarp();
   }
