@@ -292,6 +292,25 @@ LAKDE_API int lakde_log_pred_density(int dtype, int64_t N, int64_t Nq, int64_t D
                            void *workspace, size_t workspace_bytes,
                            void *stream);
 
+/* Workspace bytes lakde_log_pred_density_tc needs (float32, D <= 64). */
+LAKDE_API size_t lakde_log_pred_density_tc_workspace(int64_t N, int64_t Nq,
+                                                     int64_t D);
+
+/*
+ * lakde_log_pred_density with the quad forms on the tensor cores (tcgen05,
+ * bf16 hi + lo split of the centred differences and of W_triu, fp32
+ * accumulation in tensor memory), float32 values, D <= 64
+ * (lakde/local_adaptive_kde.py:200-223).  *err is set to 1 if a tensor-core
+ * completion wait times out.
+ */
+LAKDE_API int lakde_log_pred_density_tc(int dtype, int64_t N, int64_t Nq,
+                                        int64_t D, const void *X,
+                                        const void *W_triu, const void *nu,
+                                        const void *log_coeff, const void *Y,
+                                        void *out, void *workspace,
+                                        size_t workspace_bytes, int32_t *err,
+                                        void *stream);
+
 /* Workspace bytes lakde_log_pred_density_bwd needs. */
 LAKDE_API size_t lakde_log_pred_density_bwd_workspace(int dtype, int64_t N,
                                                       int64_t Nq, int64_t D);

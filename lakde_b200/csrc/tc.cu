@@ -557,6 +557,224 @@ __global__ void __launch_bounds__(128, 4) mstep_tc_kernel(TcArgs g) {
   if (warp == 0) tmem_dealloc(tmem, 128);
 }
 
+// ------------------------------------------------------- predictive density
+// log p(y) = -log N + logsumexp_n [lc_n - h_n log1p(|W_triu_n^T (y - x_n)|^2)]
+// (lakde/local_adaptive_kde.py:200-223) with the quad forms on the tensor
+// cores: for each kernel n, the 128-query tiles of the query block are
+// centred on x_n in fp32, split bf16 hi / lo (A) against W_triu_n hi / lo (B),
+// 12 MMAs into tensor memory.  A CTA walks a chunk of kernels two at a time:
+// each query tile is read once into registers and centred on both kernels;
+// per query it keeps the running (max, sum) of its chunk in shared memory and
+// writes it out as the chunk's partial at the end.  A second pass
+// (pred_combine_kernel) folds the chunks.
+constexpr int PQ = 4096;  // queries per block (one launch each)
+
+struct PsmCfg {
+  static constexpr uint32_t A_BYTES = MT * DP * 2;  // 16 KB
+  static constexpr uint32_t B_BYTES = DP * DP * 2;  // 8 KB
+  static constexpr uint32_t off_Ahi = 0, off_Alo = A_BYTES;
+  static constexpr uint32_t off_B = 2 * A_BYTES;  // [kernel 0, 1][hi, lo]
+  static constexpr uint32_t off_m = off_B + 4 * B_BYTES;
+  static constexpr uint32_t off_s = off_m + PQ * 4;
+  static constexpr uint32_t bytes = off_s + PQ * 4 + 128;
+};
+
+struct PredArgs {
+  const float *X;
+  const float *W;
+  const float *lc;  // log coefficients [N]
+  const float *nu;
+  const float *Y;
+  float *ws_m, *ws_s;  // [nchunks, Nq]
+  int64_t N, Nq, q0, qn, chunk;
+  int D;
+  int *err;
+};
+
+__global__ void __launch_bounds__(128, 2) pred_tc_kernel(PredArgs g) {
+  using C = PsmCfg;
+  extern __shared__ __align__(128) unsigned char sm[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t s_tmem;
+  unsigned char *Ahi = sm + C::off_Ahi, *Alo = sm + C::off_Alo;
+  float *pm = reinterpret_cast<float *>(sm + C::off_m);
+  float *ps = reinterpret_cast<float *>(sm + C::off_s);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int D = g.D;
+  const int dq = 2 * (lane & 3);
+
+  if (warp == 0) tmem_alloc(&s_tmem, 128);
+  if (tid == 0) mbar_init(&mbar);
+  for (int i = tid; i < PQ; i += 128) {
+    pm[i] = -INFINITY;
+    ps[i] = 0.f;
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = s_tmem;
+  uint32_t phase = 0;
+  bool alive = true;
+  constexpr uint32_t A_SBO = KG * 128, A_LBO = 128;
+  constexpr uint32_t B_SBO = 128, B_LBO = KG * 128;
+  const uint32_t idesc = idesc_bf16(MT, DP, 0, 1);
+  const int64_t n_begin = (int64_t)blockIdx.x * g.chunk;
+  const int64_t n_end = (n_begin + g.chunk < g.N) ? n_begin + g.chunk : g.N;
+  const int ntiles = (int)((g.qn + MT - 1) / MT);
+
+  for (int64_t n0 = n_begin; n0 < n_end && alive; n0 += 2) {
+    const int nk = (n0 + 1 < n_end) ? 2 : 1;
+    // W_triu of the kernels as B (hi, lo), their centres and coefficients
+    float xn[2][KG][2], lc[2], hh[2];
+#pragma unroll
+    for (int kk = 0; kk < 2; ++kk) {
+      const int64_t n = kk < nk ? n0 + kk : n0;
+      const float *Wn = g.W + n * (int64_t)D * D;
+      float wv[DP * DP / 256][2];
+#pragma unroll
+      for (int m = 0; m < DP * DP / 256; ++m) {
+        const int e = tid + 128 * m;
+        const int q = e >> 5, ln = e & 31;
+        const int j = 8 * (q / KG) + (ln >> 2), i = 8 * (q % KG) + 2 * (ln & 3);
+        wv[m][0] = (kk < nk && j < D && i < D) ? Wn[j * D + i] : 0.f;
+        wv[m][1] = (kk < nk && j < D && i + 1 < D) ? Wn[j * D + i + 1] : 0.f;
+      }
+      const float *xp = g.X + n * (int64_t)D;
+#pragma unroll
+      for (int k = 0; k < KG; ++k) {
+        const int d0 = 8 * k + dq;
+        xn[kk][k][0] = d0 < D ? xp[d0] : 0.f;
+        xn[kk][k][1] = d0 + 1 < D ? xp[d0 + 1] : 0.f;
+      }
+      lc[kk] = g.lc[n];
+      hh[kk] = 0.5f * (g.nu[n] + 1.f);
+      unsigned char *Bhi = sm + C::off_B + (2 * kk) * C::B_BYTES, *Blo = Bhi + C::B_BYTES;
+#pragma unroll
+      for (int m = 0; m < DP * DP / 256; ++m) {
+        const int e = tid + 128 * m;
+        const int q = e >> 5, ln = e & 31;
+        const int j = 8 * (q / KG) + (ln >> 2), i = 8 * (q % KG) + 2 * (ln & 3);
+        uint32_t hi, lo;
+        split2(wv[m][0], wv[m][1], hi, lo);
+        const uint32_t o = (uint32_t)(j >> 3) * B_LBO + (uint32_t)(i >> 3) * B_SBO + (uint32_t)(j & 7) * 16u +
+                           (uint32_t)(i & 7) * 2u;
+        *reinterpret_cast<uint32_t *>(Bhi + o) = hi;
+        *reinterpret_cast<uint32_t *>(Blo + o) = lo;
+      }
+    }
+    for (int t = 0; t < ntiles && alive; ++t) {
+      // this thread's coordinates of the tile's queries (rows 8 (w + 4 b) + l / 4)
+      constexpr int NB = MT / 32;
+      float v[NB][KG][2];
+      bool vq[NB];
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        const int p = 8 * (warp + 4 * b) + (lane >> 2);
+        const int64_t qi = (int64_t)t * MT + p;
+        vq[b] = qi < g.qn;
+        const float *yp = g.Y + (g.q0 + (vq[b] ? qi : 0)) * (int64_t)D;
+#pragma unroll
+        for (int k = 0; k < KG; ++k) {
+          const int d0 = 8 * k + dq;
+          v[b][k][0] = (vq[b] && d0 < D) ? yp[d0] : 0.f;
+          v[b][k][1] = (vq[b] && d0 + 1 < D) ? yp[d0 + 1] : 0.f;
+        }
+      }
+      for (int kk = 0; kk < nk; ++kk) {
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+          const int p = 8 * (warp + 4 * b) + (lane >> 2);
+#pragma unroll
+          for (int k = 0; k < KG; ++k) {
+            const int d0 = 8 * k + dq;
+            const float x0 = vq[b] ? v[b][k][0] - xn[kk][k][0] : 0.f;
+            const float x1 = vq[b] ? v[b][k][1] - xn[kk][k][1] : 0.f;
+            uint32_t hi, lo;
+            split2(x0, x1, hi, lo);
+            const uint32_t o = core_off(p, d0, A_SBO);
+            *reinterpret_cast<uint32_t *>(Ahi + o) = hi;
+            *reinterpret_cast<uint32_t *>(Alo + o) = lo;
+          }
+        }
+        fence_async_smem();
+        fence_before();
+        __syncthreads();
+        if (tid == 0) {
+          fence_after();
+          const uint32_t ahi = smem_u32(Ahi), alo = smem_u32(Alo);
+          const uint32_t bhi = smem_u32(sm + C::off_B + (2 * kk) * C::B_BYTES), blo = bhi + C::B_BYTES;
+          const uint32_t td = tmem + 64u * (uint32_t)kk;
+#pragma unroll
+          for (int s = 0; s < DP / 16; ++s) {
+            const uint32_t ao = 2 * s * A_LBO, bo = 2 * s * B_LBO;
+            mma(td, desc(ahi + ao, A_LBO, A_SBO), desc(bhi + bo, B_LBO, B_SBO), idesc, s > 0);
+            mma(td, desc(alo + ao, A_LBO, A_SBO), desc(bhi + bo, B_LBO, B_SBO), idesc, 1);
+            mma(td, desc(ahi + ao, A_LBO, A_SBO), desc(blo + bo, B_LBO, B_SBO), idesc, 1);
+          }
+          commit(&mbar);
+        }
+        // A is rewritten for the next kernel only after these MMAs completed
+        const bool ok = __syncthreads_and(mbar_wait(&mbar, phase) ? 1 : 0) != 0;
+        phase ^= 1;
+        fence_after();
+        if (!ok) {
+          if (tid == 0) atomicExch(g.err, 1);
+          alive = false;
+          break;
+        }
+      }
+      if (!alive) break;
+      // epilogue: thread = query row; fold the kernels into the running
+      // (max, sum) of the query
+      const int64_t qi = (int64_t)t * MT + tid;
+      const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+      for (int kk = 0; kk < nk; ++kk) {
+        float q = 0.f;
+#pragma unroll
+        for (int c0 = 0; c0 < DP; c0 += 16) {
+          float vv[16];
+          tmem_ld16(tmem + lane_base + 64u * (uint32_t)kk + c0, vv);
+#pragma unroll
+          for (int k = 0; k < 16; ++k) q = fmaf(vv[k], vv[k], q);
+        }
+        if (qi < g.qn) {
+          const float lp = lc[kk] - hh[kk] * log1pf(q);
+          const float m = pm[qi];
+          if (lp > m) {
+            ps[qi] = ps[qi] * expf(m - lp) + 1.f;
+            pm[qi] = lp;
+          } else {
+            ps[qi] += expf(lp - m);
+          }
+        }
+      }
+      fence_before();
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  // this chunk's partials for the query block
+  for (int64_t i = tid; i < g.qn; i += 128) {
+    g.ws_m[(int64_t)blockIdx.x * g.Nq + g.q0 + i] = pm[i];
+    g.ws_s[(int64_t)blockIdx.x * g.Nq + g.q0 + i] = ps[i];
+  }
+  fence_after();
+  if (warp == 0) tmem_dealloc(tmem, 128);
+}
+
+// out[q] = -log N + logsumexp over the chunks' (max, sum) partials
+__global__ void pred_fold_kernel(const float *__restrict__ ws_m, const float *__restrict__ ws_s,
+                                 float *__restrict__ out, int64_t Nq, int64_t nchunks, float log_n) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= Nq) return;
+  float M = -INFINITY;
+  for (int64_t c = 0; c < nchunks; ++c) M = fmaxf(M, ws_m[c * Nq + q]);
+  float S = 0.f;
+  if (M != -INFINITY)
+    for (int64_t c = 0; c < nchunks; ++c) S += ws_s[c * Nq + q] * expf(ws_m[c * Nq + q] - M);
+  out[q] = (M == -INFINITY) ? M : (M + logf(S)) - log_n;
+}
+
 }  // namespace tc
 }  // namespace lakde
 
@@ -667,4 +885,75 @@ extern "C" int lakde_mstep_tc(int dtype, int64_t N, int64_t D, int64_t npts, con
   tc_grid(smem, 128, N, &grid);
   tc::mstep_tc_kernel<<<grid, 128, smem, as_stream(stream)>>>(g);
   return check_launch("mstep_tc");
+}
+
+static int64_t pred_tc_chunks(int64_t N) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
+  int64_t nchunks = 2 * (int64_t)sms;  // two CTAs per SM (shared memory, TMEM)
+  if (nchunks > (N + 1) / 2) nchunks = (N + 1) / 2;
+  return nchunks < 1 ? 1 : nchunks;
+}
+
+extern "C" size_t lakde_log_pred_density_tc_workspace(int64_t N, int64_t Nq, int64_t D) {
+  if (N <= 0 || Nq <= 0 || D < 1 || D > 64) return 0;
+  return (size_t)(2 * pred_tc_chunks(N) * Nq) * sizeof(float);
+}
+
+extern "C" int lakde_log_pred_density_tc(int dtype, int64_t N, int64_t Nq, int64_t D, const void *X,
+                                         const void *W_triu, const void *nu, const void *log_coeff, const void *Y,
+                                         void *out, void *workspace, size_t workspace_bytes, int32_t *err,
+                                         void *stream) {
+  clear_error();
+  if (dtype != LAKDE_F32) {
+    set_error("log_pred_density_tc: float32 values only");
+    return LAKDE_EDTYPE;
+  }
+  if (N < 1 || Nq < 0 || D < 1 || D > 64) {
+    set_error("log_pred_density_tc: invalid sizes (N=%lld, Nq=%lld, D=%lld)", (long long)N, (long long)Nq,
+              (long long)D);
+    return D > 64 ? LAKDE_EUNSUPPORTED : LAKDE_EINVAL;
+  }
+  if (Nq == 0) return LAKDE_OK;
+  const size_t need = lakde_log_pred_density_tc_workspace(N, Nq, D);
+  if (!workspace || workspace_bytes < need) {
+    set_error("log_pred_density_tc: workspace of %zu bytes needed, %zu given", need, workspace_bytes);
+    return LAKDE_EINVAL;
+  }
+  if (!X || !W_triu || !nu || !log_coeff || !Y || !out || !err) {
+    set_error("log_pred_density_tc: null pointer");
+    return LAKDE_EINVAL;
+  }
+  if (int st = bind_device("log_pred_density_tc", {out, X, W_triu, nu, log_coeff, Y, workspace, err})) return st;
+  const int64_t nchunks = pred_tc_chunks(N);
+  tc::PredArgs g{};
+  g.X = static_cast<const float *>(X);
+  g.W = static_cast<const float *>(W_triu);
+  g.lc = static_cast<const float *>(log_coeff);
+  g.nu = static_cast<const float *>(nu);
+  g.Y = static_cast<const float *>(Y);
+  g.ws_m = static_cast<float *>(workspace);
+  g.ws_s = g.ws_m + nchunks * Nq;
+  g.N = N;
+  g.Nq = Nq;
+  g.chunk = (N + nchunks - 1) / nchunks;
+  g.D = (int)D;
+  g.err = err;
+  const size_t smem = tc::PsmCfg::bytes;
+  cudaError_t e = cudaFuncSetAttribute(tc::pred_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) {
+    set_error("log_pred_density_tc: %s", cudaGetErrorString(e));
+    return LAKDE_ECUDA;
+  }
+  const int64_t grid = (N + g.chunk - 1) / g.chunk;
+  for (int64_t q0 = 0; q0 < Nq; q0 += tc::PQ) {
+    g.q0 = q0;
+    g.qn = (Nq - q0) < tc::PQ ? (Nq - q0) : tc::PQ;
+    tc::pred_tc_kernel<<<(unsigned)grid, 128, smem, as_stream(stream)>>>(g);
+    if (int st = check_launch("log_pred_density_tc")) return st;
+  }
+  tc::pred_fold_kernel<<<(unsigned)((Nq + 255) / 256), 256, 0, as_stream(stream)>>>(
+      g.ws_m, g.ws_s, static_cast<float *>(out), Nq, grid, (float)log((double)N));
+  return check_launch("log_pred_density_tc_combine");
 }

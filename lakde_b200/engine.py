@@ -163,6 +163,8 @@ class FusedVI:
         del S
         torch.minimum(self.failed, info.min(), out=self.failed)
         lc = K.pred_coeff(nu, logdet, self.D)
+        if self.precision == "mixed":
+            return K.log_pred_density_tc(self.X, W, nu, lc, Y.to(self.dtype), self.err)
         return K.log_pred_density(self.X, W, nu, lc, Y.to(self.dtype))
 
     def posterior_factors(self):

@@ -329,6 +329,29 @@ def log_pred_density(X, W_triu, nu, log_coeff, Y, out=None, workspace=None):
     return out
 
 
+def log_pred_density_tc(X, W_triu, nu, log_coeff, Y, err, out=None, workspace=None):
+    """log_pred_density with the quad forms on the tensor cores (bf16 hi + lo),
+    float32, D <= 64 (see include/lakde_b200.h)."""
+    nat.require_cuda(X, W_triu, nu, log_coeff, Y, err, op="log_pred_density_tc")
+    N, D = X.shape
+    Y = Y.contiguous()
+    Nq = Y.size(0)
+    out = Y.new_empty(Nq) if out is None else out
+    if Nq == 0:
+        return out
+    need = nat.lib().lakde_log_pred_density_tc_workspace(N, Nq, D)
+    if workspace is None or workspace.numel() < need:
+        workspace = torch.empty(need, dtype=torch.uint8, device=X.device)
+    nat.check(
+        nat.lib().lakde_log_pred_density_tc(
+            nat.dtype_code(X), N, Nq, D, nat.ptr(X), nat.ptr(W_triu), nat.ptr(nu), nat.ptr(log_coeff),
+            nat.ptr(Y), nat.ptr(out), nat.ptr(workspace), workspace.numel(), nat.ptr(err), nat.stream_of(X),
+        ),
+        "log_pred_density_tc",
+    )
+    return out
+
+
 def log_pred_density_bwd(X, W_triu, nu, log_coeff, Y, out, grad_out):
     """Pair pass of the predictive-density backward (see include/lakde_b200.h).
 

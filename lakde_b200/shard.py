@@ -133,9 +133,11 @@ class CudaShardOps:
     def normalise_stage(self, stage, pat, logrho, r, c, rsum, red, red2, mode, threshold):
         self.K.estep_normalise_stage(stage, pat.cptr, pat.pos, logrho, r, c, rsum, red, red2, mode, threshold)
 
-    def pred(self, Xk, U, nu, logdet, Y):
+    def pred(self, Xk, U, nu, logdet, Y, precision, err):
         """-log n + logsumexp over these n kernels, per query."""
         lc = self.K.pred_coeff(nu, logdet, Xk.size(1))
+        if precision == "mixed":
+            return self.K.log_pred_density_tc(Xk, U, nu, lc, Y, err)
         return self.K.log_pred_density(Xk, U, nu, lc, Y)
 
 
@@ -300,7 +302,7 @@ class ShardedKNN:
             info = torch.empty_like(self.info)
             self.ops.factor(S, self.W_inv_jitter, self.eps, self.sigma_0, self.nu_0_t, self.a, self.b, None, U, logdet,
                             None, info)
-            v = self.ops.pred(self.X[self.lo : self.hi], U, nu, logdet, Y) + math.log(self.n)
+            v = self.ops.pred(self.X[self.lo : self.hi], U, nu, logdet, Y, self.precision, self.err) + math.log(self.n)
         else:
             v = torch.full((Y.size(0),), -math.inf, dtype=self.dtype, device=self.device)
         mx = v.clone()

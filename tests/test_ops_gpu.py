@@ -429,3 +429,26 @@ def test_mstep_tc_long_rows_accumulate_over_tiles(K):
         sc = np.abs(Sr[n]).max() + 1e-30
         assert np.abs(S[n] - Sr[n]).max() <= 2e-4 * sc
     assert int(err) == 0
+
+
+@pytest.mark.parametrize("D,Nq", [(21, 300), (43, 5000), (63, 130), (64, 4097)])
+def test_log_pred_density_tc_matches_fp64(K, D, Nq):
+    """Tensor-core predictive density: query blocks of 4096 and ragged tiles,
+    an odd kernel count (the last kernel of a chunk alone), against the
+    float64 restatement and the plain FP32 kernel."""
+    rng = np.random.default_rng(D + Nq)
+    N = 777
+    X = (rng.standard_normal((N, D)) * 2 + 5).astype(np.float32)
+    Y = (X[rng.integers(0, N, Nq)] + 0.3 * rng.standard_normal((Nq, D))).astype(np.float32)
+    W = (rand_upper(rng, N, D, np.float64) / np.sqrt(D)).astype(np.float32)
+    nu = rng.uniform(D + 1, D + 30, N).astype(np.float32)
+    logdet = O.chol_logdet(W).astype(np.float32)
+    err = torch.zeros(1, dtype=torch.int32, device=DEV)
+    lc = K.pred_coeff(t(nu), t(logdet), D)
+    out = K.log_pred_density_tc(t(X), t(W), t(nu), lc, t(Y), err)
+    assert int(err) == 0
+    ref = O.log_pred_density_from_factors(X.astype(np.float64), Y.astype(np.float64), W.astype(np.float64),
+                                          nu.astype(np.float64), logdet.astype(np.float64))
+    np.testing.assert_allclose(out.cpu().numpy(), ref, rtol=0, atol=2e-3)
+    plain = K.log_pred_density(t(X), t(W), t(nu), lc, t(Y))
+    assert float((out - plain).abs().max()) <= 2e-3

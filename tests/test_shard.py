@@ -122,7 +122,7 @@ class NumpyShardOps:
             c.copy_(torch.from_numpy((c_new + np.log(sums)).astype(dt)))
             rsum.copy_(torch.from_numpy(rs))
 
-    def pred(self, Xk, U, nu, logdet, Y):
+    def pred(self, Xk, U, nu, logdet, Y, precision=None, err=None):
         return torch.from_numpy(O.log_pred_density_from_factors(self._np(Xk), self._np(Y), self._np(U),
                                                                 self._np(nu), self._np(logdet)))
 
