@@ -56,11 +56,49 @@ __device__ __forceinline__ double f_div(double a, double b) { return __ddiv_rn(a
 template <int DP>
 __device__ __forceinline__ constexpr int tix(int i, int j) { return i * (i + 1) / 2 + j; }
 
+// Row m of X (D <= DP, zero padded).  With D == DP and an aligned base the
+// rows are DP * 4 or DP * 8 bytes apart and start 16-byte aligned (DP in
+// {4, 8}) or 8-byte aligned (DP = 2): vector loads, so a gather of one row per
+// thread is one or two load instructions instead of DP.
+template <typename T, int DP>
+__device__ __forceinline__ void load_row(const T *__restrict__ X, int64_t m, int D, T (&out)[DP]) {
+  const uintptr_t base = reinterpret_cast<uintptr_t>(X);
+  if constexpr (sizeof(T) == 4 && DP >= 4) {
+    if (D == DP && (base & 15u) == 0) {
+      const float4 *p = reinterpret_cast<const float4 *>(X + m * DP);
+#pragma unroll
+      for (int v = 0; v < DP / 4; ++v) {
+        const float4 f = p[v];
+        out[4 * v] = f.x;
+        out[4 * v + 1] = f.y;
+        out[4 * v + 2] = f.z;
+        out[4 * v + 3] = f.w;
+      }
+      return;
+    }
+  }
+  if constexpr (DP >= 2) {
+    if (D == DP && (base & (2 * sizeof(T) - 1)) == 0) {
+      using V2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+      const V2 *p = reinterpret_cast<const V2 *>(X + m * DP);
+#pragma unroll
+      for (int v = 0; v < DP / 2; ++v) {
+        const V2 f = p[v];
+        out[2 * v] = f.x;
+        out[2 * v + 1] = f.y;
+      }
+      return;
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < DP; ++d) out[d] = d < D ? X[m * D + d] : T(0);
+}
+
 // Cholesky of (scale P + S + jit I) in FP64 registers; false if a pivot is
 // not positive.  Padded dimensions are the identity.
 template <typename T, int DP>
-__device__ __forceinline__ bool chol_rows(const T (&S)[DP * (DP + 1) / 2], const T *__restrict__ P, T scale, T jit,
-                                          int D, double (&L)[DP * (DP + 1) / 2]) {
+__device__ __forceinline__ bool chol_rows(const T (&S)[DP * (DP + 1) / 2], const T (&Pv)[DP * (DP + 1) / 2],
+                                          bool has_p, T scale, T jit, int D, double (&L)[DP * (DP + 1) / 2]) {
 #pragma unroll
   for (int i = 0; i < DP; ++i)
 #pragma unroll
@@ -68,7 +106,7 @@ __device__ __forceinline__ bool chol_rows(const T (&S)[DP * (DP + 1) / 2], const
       double v;
       if (i < D) {
         T s = S[tix<DP>(i, j)];
-        if (P) s = f_add(f_mul(P[i * D + j], scale), s);
+        if (has_p) s = f_add(f_mul(Pv[tix<DP>(i, j)], scale), s);
         if (i == j) s = f_add(s, jit);
         v = (double)s;
       } else {
@@ -105,46 +143,78 @@ __global__ void __launch_bounds__(128) vi_rows_kernel(RowArgs<T> g) {
   bool bad = end < start;
 
   T xn[DP];
-#pragma unroll
-  for (int d = 0; d < DP; ++d) xn[d] = d < D ? g.X[n * D + d] : T(0);
+  load_row<T, DP>(g.X, n, D, xn);
 
   // ---------------------------------------------------------------- M-step
+  // pairs in batches of U: the indices, then the point rows of a batch are
+  // all loaded before any is used (the gathers of a row overlap); the
+  // accumulation order is the pair order
+  constexpr int U = 4;
   T S[TT];
 #pragma unroll
   for (int e = 0; e < TT; ++e) S[e] = T(0);
   T vsum = T(0);
-  for (int64_t p = start; p < end; ++p) {
-    const int64_t c = g.col[p];
-    const T v = g.r[p];
-    if (c < 0 || c >= g.npts) {
-      bad = true;
-      continue;
+  for (int64_t p0 = start; p0 < end; p0 += U) {
+    int64_t c[U];
+    T v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      c[u] = -1;
+      v[u] = T(0);
+      if (p0 + u < end) {
+        c[u] = g.col[p0 + u];
+        v[u] = g.r[p0 + u];
+        if (c[u] < 0 || c[u] >= g.npts) {
+          bad = true;
+          c[u] = -1;
+        }
+      }
     }
-    T dl[DP];
+    T dl[U][DP];
 #pragma unroll
-    for (int d = 0; d < DP; ++d) dl[d] = d < D ? g.X[c * D + d] - xn[d] : T(0);
+    for (int u = 0; u < U; ++u) {
+      load_row<T, DP>(g.X, c[u] < 0 ? 0 : c[u], D, dl[u]);
 #pragma unroll
-    for (int i = 0; i < DP; ++i) {
-      const T vi = v * dl[i];
-#pragma unroll
-      for (int j = 0; j <= i; ++j) S[tix<DP>(i, j)] = fma(vi, dl[j], S[tix<DP>(i, j)]);
+      for (int d = 0; d < DP; ++d) dl[u][d] = (c[u] >= 0 && d < D) ? dl[u][d] - xn[d] : T(0);
     }
-    vsum += v;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (c[u] < 0) continue;
+#pragma unroll
+      for (int i = 0; i < DP; ++i) {
+        const T vi = v[u] * dl[u][i];
+#pragma unroll
+        for (int j = 0; j <= i; ++j) S[tix<DP>(i, j)] = fma(vi, dl[u][j], S[tix<DP>(i, j)]);
+      }
+      vsum += v[u];
+    }
   }
   const T nu = g.nu0 + vsum;
 
   // ------------------------------------------------------------- posterior
   const T b_old = g.b[n];
   const T scale = f_mul(g.nu0, f_div(g.a[n], b_old));
-  const T *P = g.P ? g.P + n * g.Pbs : nullptr;
+  // the lower triangle of P_n, row by row (vector loads for D == DP)
+  T Pv[TT];
+  const bool has_p = g.P != nullptr;
+  if (has_p) {
+    const T *P = g.P + n * g.Pbs;
+#pragma unroll
+    for (int i = 0; i < DP; ++i) {
+      T row[DP];
+      load_row<T, DP>(P, i, D, row);
+#pragma unroll
+      for (int j = 0; j <= i; ++j) Pv[tix<DP>(i, j)] = i < D ? row[j] : T(0);
+    }
+  }
   T jit = g.jitter[n];
   double L[TT];
-  bool ok = chol_rows<T, DP>(S, P, scale, jit, D, L);
+  bool ok = chol_rows<T, DP>(S, Pv, has_p, scale, jit, D, L);
   if (!ok) {
     T jt = T(0);
     for (int k = 0; k < 32 && !ok; ++k) {
       jt = f_add(jt, (T)(g.eps * ldexp(1.0, k)));
-      ok = chol_rows<T, DP>(S, P, scale, jt, D, L);
+      ok = chol_rows<T, DP>(S, Pv, has_p, scale, jt, D, L);
       if (ok) jit = jt;
     }
   }
@@ -161,11 +231,16 @@ __global__ void __launch_bounds__(128) vi_rows_kernel(RowArgs<T> g) {
   double tr = 0.0;
   if (g.Tm) {
     const T *Tn = g.Tm + n * g.Tbs;
-    for (int a = 0; a < D; ++a) {
+    T Tv[DP][DP];
+#pragma unroll
+    for (int i = 0; i < DP; ++i) load_row<T, DP>(Tn, i, D, Tv[i]);
+#pragma unroll
+    for (int a = 0; a < DP; ++a) {
+      if (a >= D) continue;
       double z[DP];
 #pragma unroll
       for (int i = 0; i < DP; ++i) {
-        double s = i < D ? (double)Tn[i * D + a] : 0.0;
+        double s = i < D ? (double)Tv[i][a] : 0.0;
 #pragma unroll
         for (int j = 0; j < i; ++j) s -= L[tix<DP>(i, j)] * z[j];
         z[i] = s / L[tix<DP>(i, i)];
@@ -193,25 +268,44 @@ __global__ void __launch_bounds__(128) vi_rows_kernel(RowArgs<T> g) {
   const double e = mvdigamma_d(0.5 * (double)nu, D) + D * 0.69314718055994530942 + (double)logdet;
   const T cst = (T)(0.5 * e);
   const T expo = T(-0.5) * nu;
-  for (int64_t p = start; p < end; ++p) {
-    const int64_t c = g.col[p];
-    if (!ok || c < 0 || c >= g.npts) {
-      g.logrho[p] = nanv;
-      continue;
-    }
-    T y[DP];
-    T q = T(0);
+  for (int64_t p0 = start; p0 < end; p0 += U) {
+    int64_t c[U];
 #pragma unroll
-    for (int i = 0; i < DP; ++i) {
-      T s = i < D ? g.X[c * D + i] - xn[i] : T(0);
-#pragma unroll
-      for (int j = 0; j < i; ++j) s = fma(-Lf[tix<DP>(i, j)], y[j], s);
-      y[i] = s * rinv[i];
-      q = fma(y[i], y[i], q);
+    for (int u = 0; u < U; ++u) {
+      c[u] = -1;
+      if (p0 + u < end) {
+        c[u] = g.col[p0 + u];
+        if (!ok || c[u] < 0 || c[u] >= g.npts) c[u] = -2;
+      }
     }
-    T lr = f_add(f_mul(q, expo), cst);
-    if (c == n) lr = neg_inf<T>();
-    g.logrho[p] = lr;
+    T dl[U][DP];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      load_row<T, DP>(g.X, c[u] < 0 ? 0 : c[u], D, dl[u]);
+#pragma unroll
+      for (int d = 0; d < DP; ++d) dl[u][d] = (c[u] >= 0 && d < D) ? dl[u][d] - xn[d] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (c[u] == -1) continue;  // past the end of the row
+      if (c[u] == -2) {
+        g.logrho[p0 + u] = nanv;
+        continue;
+      }
+      T y[DP];
+      T q = T(0);
+#pragma unroll
+      for (int i = 0; i < DP; ++i) {
+        T s = dl[u][i];
+#pragma unroll
+        for (int j = 0; j < i; ++j) s = fma(-Lf[tix<DP>(i, j)], y[j], s);
+        y[i] = s * rinv[i];
+        q = fma(y[i], y[i], q);
+      }
+      T lr = f_add(f_mul(q, expo), cst);
+      if (c[u] == n) lr = neg_inf<T>();
+      g.logrho[p0 + u] = lr;
+    }
   }
 }
 
