@@ -292,6 +292,22 @@ LAKDE_API int lakde_log_pred_density(int dtype, int64_t N, int64_t Nq, int64_t D
                            void *workspace, size_t workspace_bytes,
                            void *stream);
 
+/* Workspace bytes lakde_knn_elbo needs. */
+LAKDE_API size_t lakde_knn_elbo_workspace(void);
+
+/*
+ * ELBO of LocalKNearestKDE in FP64 (lakde/local_knn_kde.py:256-341, terms
+ * :24-47) from the per-kernel a, b, nu, logdet_W, logdet_sigma_0,
+ * mm = nu * trace [N] and the per-point normaliser c [N], written to *out (one
+ * double on the device).  Deterministic reduction order.
+ */
+LAKDE_API int lakde_knn_elbo(int dtype, int64_t N, int64_t D, const void *a,
+                             const void *b, const void *nu, const void *logdet_W,
+                             const void *logdet_sigma_0, const void *mm,
+                             const void *c, double a_0, double b_0, double nu_0,
+                             void *workspace, size_t workspace_bytes,
+                             double *out, void *stream);
+
 /* Workspace bytes lakde_log_pred_density_tc needs (float32, D <= 64). */
 LAKDE_API size_t lakde_log_pred_density_tc_workspace(int64_t N, int64_t Nq,
                                                      int64_t D);

@@ -95,6 +95,12 @@ _SIGNATURES = {
         _c_int,
     ),
     "lakde_log_pred_density_tc_workspace": ([_c_i64, _c_i64, _c_i64], ctypes.c_size_t),
+    "lakde_knn_elbo_workspace": ([], ctypes.c_size_t),
+    "lakde_knn_elbo": (
+        [_c_int, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_dbl, _c_dbl, _c_vp,
+         ctypes.c_size_t, _c_vp, _c_vp],
+        _c_int,
+    ),
     "lakde_log_pred_density_tc": (
         [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, ctypes.c_size_t, _c_vp,
          _c_vp],

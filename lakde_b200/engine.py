@@ -44,7 +44,8 @@ class FusedVI:
         self.nu_0_t = torch.full((1,), self.nu_0, dtype=self.dtype, device=self.device)
         self.a_0 = a_0
         self.b_0 = b_0
-        self.b_0_f = float(b_0)  # host copy: no device read inside a captured step
+        self.b_0_f = float(b_0)  # host copies: no device read inside a captured step
+        self.a_0_f = float(a_0)
         self.threshold = float(threshold or 0.0)
         self.eps = torch.finfo(self.dtype).eps
         N, D = self.N, self.D
@@ -253,26 +254,16 @@ class FusedKNN(FusedVI):
         torch.add(self.sigma_0_lambda_mm_trace * (self.nu_0 / 2), self.b_0, out=self.b)
 
     def compute_elbo(self):
-        """lakde/local_knn_kde.py:256-341 (terms :24-47), reduced in float64."""
-        N, D = self.N, self.D
-        f = lambda t: t.double()  # noqa: E731
-        a, b, nu = f(self.a), f(self.b), f(self.nu)
-        a_0 = torch.tensor(float(self.a_0), dtype=torch.float64, device=self.device)
-        b_0 = torch.tensor(float(self.b_0), dtype=torch.float64, device=self.device)
-        nu_0 = torch.tensor(self.nu_0, dtype=torch.float64, device=self.device)
-        e_tau = a / b
-        e_log_tau = torch.digamma(a) - torch.log(b)
-        e_logdet = mvdigamma(nu / 2, D) + D * LOG2 + f(self.logdet_W)
-        p_tau = torch.sum(-lgamma(a_0) + a_0 * torch.log(b_0) + (a_0 - 1) * e_log_tau - b_0 * e_tau)
-        q_tau = torch.sum(-lgamma(a) + a * torch.log(b) + (a - 1) * e_log_tau - b * e_tau)
-        B_p = -nu_0 / 2 * (D * LOG2 - f(self.logdet_sigma_0) - D * e_log_tau - D * torch.log(nu_0)) - mvlgamma(
-            nu_0 / 2, D
-        )
-        p_lam = torch.sum(B_p + (nu_0 - D - 1) * e_logdet / 2 - e_tau * nu_0 * f(self.sigma_0_lambda_mm_trace) / 2)
-        B_q = -nu / 2 * (f(self.logdet_W) + D * LOG2) - mvlgamma(nu / 2, D)
-        q_lam = torch.sum(B_q + (nu - D - 1) * e_logdet / 2 - nu / 2 * D)
-        ll = torch.sum(-D / 2 * math.log(2 * math.pi) + f(self.c))
-        return ll + (p_lam - q_lam) - N * math.log(N - 1) + (p_tau - q_tau)
+        """lakde/local_knn_kde.py:256-341 (terms :24-47): one FP64 kernel over
+        kernels and points with a fixed reduction order; a 0-dim float64
+        device tensor."""
+        if getattr(self, "_elbo_out", None) is None:
+            self._elbo_out = torch.empty((), dtype=torch.float64, device=self.device)
+            self._elbo_ws = torch.empty(K.nat.lib().lakde_knn_elbo_workspace(), dtype=torch.uint8,
+                                        device=self.device)
+        return K.knn_elbo(self.a, self.b, self.nu, self.logdet_W, self.logdet_sigma_0, self.sigma_0_lambda_mm_trace,
+                          self.c, self.a_0_f, self.b_0_f, self.nu_0, self.D, out=self._elbo_out,
+                          workspace=self._elbo_ws).clone()
 
 
 class FusedHier(FusedVI):

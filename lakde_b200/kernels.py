@@ -329,6 +329,25 @@ def log_pred_density(X, W_triu, nu, log_coeff, Y, out=None, workspace=None):
     return out
 
 
+def knn_elbo(a, b, nu, logdet_W, logdet_sigma_0, mm, c, a_0, b_0, nu_0, D, out=None, workspace=None):
+    """ELBO of LocalKNearestKDE in float64 as a 0-dim device tensor (see include/lakde_b200.h)."""
+    nat.require_cuda(a, b, nu, logdet_W, logdet_sigma_0, mm, c, op="knn_elbo")
+    dev = a.device
+    out = torch.empty((), dtype=torch.float64, device=dev) if out is None else out
+    need = nat.lib().lakde_knn_elbo_workspace()
+    if workspace is None or workspace.numel() < need:
+        workspace = torch.empty(need, dtype=torch.uint8, device=dev)
+    nat.check(
+        nat.lib().lakde_knn_elbo(
+            nat.dtype_code(a), a.numel(), int(D), nat.ptr(a), nat.ptr(b), nat.ptr(nu), nat.ptr(logdet_W),
+            nat.ptr(logdet_sigma_0), nat.ptr(mm), nat.ptr(c), float(a_0), float(b_0), float(nu_0),
+            nat.ptr(workspace), workspace.numel(), nat.ptr(out), nat.stream_of(a),
+        ),
+        "knn_elbo",
+    )
+    return out
+
+
 def log_pred_density_tc(X, W_triu, nu, log_coeff, Y, err, out=None, workspace=None):
     """log_pred_density with the quad forms on the tensor cores (bf16 hi + lo),
     float32, D <= 64 (see include/lakde_b200.h)."""
