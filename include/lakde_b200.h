@@ -292,6 +292,58 @@ LAKDE_API int lakde_log_pred_density(int dtype, int64_t N, int64_t Nq, int64_t D
                            void *workspace, size_t workspace_bytes,
                            void *stream);
 
+/* ------------------------------------------------------------------------- */
+/* Tiled per-kernel matrices (8 < D <= 64, float32).                          */
+/* ------------------------------------------------------------------------- */
+/*
+ * With DP = D rounded up to 16, 24, 32, 48 or 64 and NT = DP / 8, a matrix is
+ * kept as its NT (NT + 1) / 2 lower 8 x 8 tiles, tile (I, J), J <= I, at
+ * index I (I + 1) / 2 + J, each 64 floats row-major, zero outside D x D and
+ * above the diagonal.  "SP" interleaves, per kernel and tile, the S tile
+ * then the P tile (128 floats per tile): the bytes of a tile pair are exactly
+ * those of the FP64 tile the factorisation builds from it, so one bulk copy
+ * per matrix brings both operands in.  No counterpart in the reference (its
+ * matrices are dense [N, D, D]).
+ */
+/* Number of tiles NT (NT + 1) / 2 for dimension D (0 if D is out of range). */
+LAKDE_API int64_t lakde_tile_count(int64_t D);
+
+/*
+ * dst[n * dst_batch_stride + t * dst_tile_stride + dst_offset + e] = element
+ * e of tile t of src[n] ([D, D] blocks src_batch_stride elements apart).
+ */
+LAKDE_API int lakde_pack_tiles(int dtype, int64_t N, int64_t D, const void *src,
+                               int64_t src_batch_stride, void *dst,
+                               int64_t dst_batch_stride, int64_t dst_tile_stride,
+                               int64_t dst_offset, void *stream);
+
+/*
+ * lakde_mstep_tc with S_n written as tiles into the S halves of SP (per
+ * kernel 128 * tiles floats); nu as in lakde_mstep_tc.
+ */
+LAKDE_API int lakde_mstep_tc_tiled(int dtype, int64_t N, int64_t D, int64_t npts,
+                                   const void *rowptr, const void *col,
+                                   const void *order, const void *r,
+                                   const void *X, int64_t kernel_offset,
+                                   double nu_0, void *SP, void *nu,
+                                   int32_t *err, void *stream);
+
+/*
+ * lakde_posterior_factor from tiled inputs: A_n = nu_0 a_n / b_n P_n + S_n
+ * with S_n and P_n from SP, and the trace term from the lower triangular T_n
+ * as tiles (T_tiles, 64 * tiles floats per kernel, may be NULL).  float32,
+ * 8 < D <= 64, SP and T_tiles 16-byte aligned; outputs as in
+ * lakde_posterior_factor (no L).  info_n = -2 marks a matrix whose input copy
+ * did not complete within the wait limit.
+ */
+LAKDE_API int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D,
+                                           const void *SP, const void *nu_0,
+                                           const void *a, const void *b,
+                                           void *jitter, double eps,
+                                           void *W_triu, void *logdet_W,
+                                           int32_t *info, const void *T_tiles,
+                                           void *trace, void *stream);
+
 /* Workspace bytes lakde_knn_elbo needs. */
 LAKDE_API size_t lakde_knn_elbo_workspace(void);
 

@@ -96,6 +96,18 @@ _SIGNATURES = {
     ),
     "lakde_log_pred_density_tc_workspace": ([_c_i64, _c_i64, _c_i64], ctypes.c_size_t),
     "lakde_knn_elbo_workspace": ([], ctypes.c_size_t),
+    "lakde_tile_count": ([_c_i64], _c_i64),
+    "lakde_pack_tiles": ([_c_int, _c_i64, _c_i64, _c_vp, _c_i64, _c_vp, _c_i64, _c_i64, _c_i64, _c_vp], _c_int),
+    "lakde_mstep_tc_tiled": (
+        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64, _c_dbl, _c_vp, _c_vp, _c_vp,
+         _c_vp],
+        _c_int,
+    ),
+    "lakde_posterior_factor_tiled": (
+        [_c_int, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
+         _c_vp],
+        _c_int,
+    ),
     "lakde_knn_elbo": (
         [_c_int, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_dbl, _c_dbl, _c_vp,
          ctypes.c_size_t, _c_vp, _c_vp],

@@ -32,6 +32,10 @@ struct FactorArgs {
   int64_t Tbs;
   int T_lower;
   T *trace;
+  // tiled inputs (float32, 8 < D <= 64): per matrix, tile t of the lower
+  // 8 x 8 tiles of S then of P (SP, 128 floats per tile) and of T (Tt, 64)
+  const float *SP;
+  const float *Tt;
   int64_t N;
   int D;
 };
@@ -175,13 +179,17 @@ struct DmmaCfg {
   static constexpr int NT = DP / 8;
   static constexpr int NTILE = NT * (NT + 1) / 2;
   static constexpr int WPB = 2;
-  // per warp: FP64 tiles, a scratch tile, 1 / L_ii, then the lower triangle
-  // of a per-matrix FP32 T_n (packed rows, in doubles rounded up to 16 bytes)
-  static constexpr int off_scratch = NTILE * 64;
-  static constexpr int off_rdiag = off_scratch + 64;
+  // per warp: FP64 tiles, 1 / L_ii, then the lower triangle of a per-matrix
+  // FP32 T_n (packed rows or tiles, in doubles rounded up to 16 bytes), which
+  // doubles as the scratch tile of the L output (T_n is then not staged)
+  static constexpr int off_rdiag = NTILE * 64;
   static constexpr int off_tstage = off_rdiag + DP;
-  static constexpr int tstage = ((DP * (DP + 1) / 2 + 3) / 4) * 2;
-  static constexpr int per_warp = off_tstage + tstage;
+  static constexpr int off_scratch = off_tstage;
+  // T_n as packed rows, or as NTILE tiles of 64 floats (tiled inputs)
+  static constexpr int tstage_rows = ((DP * (DP + 1) / 2 + 3) / 4) * 2;
+  static constexpr int tstage = tstage_rows > NTILE * 32 ? tstage_rows : NTILE * 32;
+  static constexpr int off_mbar = off_tstage + tstage;  // one mbarrier (two doubles keep 16-byte alignment)
+  static constexpr int per_warp = off_mbar + 2;
   static constexpr size_t smem = (size_t)WPB * per_warp * sizeof(double);
 };
 
@@ -270,6 +278,95 @@ __device__ __forceinline__ void assemble_tiles(const FactorArgs<T> &g, int64_t n
   }
 }
 
+// ---- tiled inputs: one bulk copy per matrix, converted in place ----------
+__device__ __forceinline__ uint32_t sm_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+constexpr uint32_t kBulkSpinLimit = 1u << 24;
+
+// Waits for the mbarrier phase; false after kBulkSpinLimit polls.
+__device__ __forceinline__ bool bulk_wait(uint64_t *mbar, uint32_t parity) {
+  const uint32_t a = sm_u32(mbar);
+  for (uint32_t it = 0; it < kBulkSpinLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// Lane 0 issues the copies of SP_n (into the tile area) and T_n (into the T
+// stage) on the warp's mbarrier; every lane first orders its earlier shared
+// memory accesses before the asynchronous writes.
+template <int DP>
+__device__ __forceinline__ void bulk_issue(const FactorArgs<float> &g, int64_t n, double *M, uint64_t *mbar, int lane) {
+  using C = DmmaCfg<DP>;
+  constexpr uint32_t sp_bytes = C::NTILE * 512u, t_bytes = C::NTILE * 256u;
+  const uint32_t total = sp_bytes + (g.Tt ? t_bytes : 0u);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncwarp();
+  if (lane == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sm_u32(mbar)), "r"(total)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     sm_u32(M)),
+                 "l"(g.SP + n * (int64_t)(C::NTILE * 128)), "r"(sp_bytes), "r"(sm_u32(mbar))
+                 : "memory");
+    if (g.Tt)
+      asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                       sm_u32(M + C::off_tstage)),
+                   "l"(g.Tt + n * (int64_t)(C::NTILE * 64)), "r"(t_bytes), "r"(sm_u32(mbar))
+                   : "memory");
+  }
+}
+
+// Tile t of the copied area holds S_t then P_t (128 floats = the 512 bytes
+// of FP64 tile t): each lane reads its 2 + 2 values of a batch of tiles,
+// the warp synchronises, and the FP64 entries of A_n + jt I replace them.
+template <int DP>
+__device__ __forceinline__ void convert_tiles(double *M, float scale, float jt, int D, int lane) {
+  constexpr int NT = DP / 8;
+  constexpr int NB = 6;  // tiles per batch
+  const float *F = reinterpret_cast<const float *>(M);
+  int t0 = 0;
+#pragma unroll 1
+  for (int I0 = 0; I0 < NT; ++I0) {
+    // the tiles of row block I0 (I0 + 1 of them) in batches of NB
+#pragma unroll 1
+    for (int J0 = 0; J0 <= I0; J0 += NB) {
+      float sv[NB][2], pv[NB][2];
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        if (J0 + b <= I0) {
+          const float *tt = F + (t0 + J0 + b) * 128;
+          sv[b][0] = tt[lane];
+          sv[b][1] = tt[lane + 32];
+          pv[b][0] = tt[64 + lane];
+          pv[b][1] = tt[64 + lane + 32];
+        }
+      }
+      __syncwarp();
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        if (J0 + b <= I0) {
+          double *out = M + (t0 + J0 + b) * 64;
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int e = lane + 32 * h;
+            const int i = 8 * I0 + (e >> 3), j = 8 * (J0 + b) + (e & 7);
+            out[e] = assemble_one<float>(sv[b][h], pv[b][h], true, scale, jt, i, j, D);
+          }
+        }
+      }
+      __syncwarp();
+    }
+    t0 += I0 + 1;
+  }
+}
+
 // B fragments of the 8-column block Ac of T_n, tile K of rows 8K..8K+7:
 // tb[K][s] = T[8K + 4s + t % 4][8 Ac + t / 4].
 template <typename T, int NT>
@@ -285,13 +382,15 @@ __device__ __forceinline__ void load_tcol(const T *Tn, int D, int lower, int Ac,
 }
 
 template <typename T, int DP>
-__device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, double *M, int lane) {
+__device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, double *M, int lane, uint32_t *phase,
+                                           bool *halt) {
   using C = DmmaCfg<DP>;
   constexpr int NT = C::NT;
   double *scratch = M + C::off_scratch;
   double *rdiag = M + C::off_rdiag;
   // per-matrix FP32 T_n goes through shared memory with the other inputs
-  const bool staged = sizeof(T) == 4 && g.Tm && g.Tbs != 0;
+  const bool tiled = sizeof(T) == 4 && g.SP != nullptr;
+  const bool staged = sizeof(T) == 4 && !g.L && ((g.Tm && g.Tbs != 0) || (tiled && g.Tt));
   float *tstage = staged ? reinterpret_cast<float *>(M + C::off_tstage) : nullptr;
   const int D = g.D;
   const T scale = posterior_scale(g, n);
@@ -304,7 +403,26 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
       jt = T(0);
       for (int k = 0; k < attempt; ++k) jt = add_rn(jt, (T)(g.eps * ldexp(1.0, k)));
     }
-    assemble_tiles<T, DP>(g, n, scale, jt, M, tstage, lane);
+    if constexpr (sizeof(T) == 4) {
+      if (tiled) {
+        uint64_t *mbar = reinterpret_cast<uint64_t *>(M + C::off_mbar);
+        bulk_issue<DP>(g, n, M, mbar, lane);
+        const bool arrived = bulk_wait(mbar, *phase);
+        *phase ^= 1u;
+        if (!arrived) {
+          // no copy lands after a second bounded wait: the warp stops here
+          bulk_wait(mbar, *phase ^ 1u);
+          if (lane == 0) g.info[n] = -2;
+          *halt = true;
+          return;
+        }
+        convert_tiles<DP>(M, scale, jt, D, lane);
+      } else {
+        assemble_tiles<T, DP>(g, n, scale, jt, M, tstage, lane);
+      }
+    } else {
+      assemble_tiles<T, DP>(g, n, scale, jt, M, tstage, lane);
+    }
     __syncwarp();
     ok = dmma::chol_blocked<NT, T>(M, scratch, rdiag, lane, lout, D);
     if (ok) jit = jt;
@@ -323,7 +441,7 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
     }
     if (lane == 0) {
       g.logdet[n] = nanv;
-      if (g.Tm) g.trace[n] = nanv;
+      if (g.Tm || g.Tt) g.trace[n] = nanv;
     }
     return;
   }
@@ -383,11 +501,16 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
       for (int K = 0; K < NT; ++K) {
         double b0 = 0.0, b1 = 0.0;
         const int r0 = 8 * K + (lane & 3), r1 = r0 + 4;
-        if (K >= Ac) {
+        if (K >= Ac && tiled) {
+          // tile (K, Ac): local row lane % 4 (+ 4), local column lane / 4
+          const float *tk = st + (K * (K + 1) / 2 + Ac) * 64 + (lane & 3) * 8 + (lane >> 2);
+          b0 = (double)tk[0];
+          b1 = (double)tk[32];
+        } else if (K >= Ac) {
           b0 = (r0 < D && col <= r0) ? (double)st[r0 * (r0 + 1) / 2 + col] : 0.0;
           b1 = (r1 < D && col <= r1) ? (double)st[r1 * (r1 + 1) / 2 + col] : 0.0;
         } else {
-          if (g.T_lower) continue;
+          if (g.T_lower || tiled) continue;
           b0 = (r0 < D && col < D) ? (double)Tn[r0 * D + col] : 0.0;
           b1 = (r1 < D && col < D) ? (double)Tn[r1 * D + col] : 0.0;
           if (!__any_sync(0xffffffffu, b0 != 0.0 || b1 != 0.0)) continue;
@@ -448,8 +571,16 @@ __global__ void __launch_bounds__(32 * DmmaCfg<DP>::WPB) factor_dmma_kernel(Fact
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double *M = smem_d + warp * C::per_warp;
   const int64_t stride = (int64_t)gridDim.x * C::WPB;
-  for (int64_t n = (int64_t)blockIdx.x * C::WPB + warp; n < g.N; n += stride) {
-    factor_one<T, DP>(g, n, M, lane);
+  uint32_t phase = 0;
+  bool halt = false;
+  if (lane == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(M + C::off_mbar))
+                 : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  for (int64_t n = (int64_t)blockIdx.x * C::WPB + warp; n < g.N && !halt; n += stride) {
+    factor_one<T, DP>(g, n, M, lane, &phase, &halt);
     __syncwarp();
   }
 }
@@ -457,6 +588,34 @@ __global__ void __launch_bounds__(32 * DmmaCfg<DP>::WPB) factor_dmma_kernel(Fact
 }  // namespace lakde
 
 using namespace lakde;
+
+// Persistent DMMA launch: exactly the blocks that are resident at once
+// (registers and shared memory), so every block starts immediately.
+template <typename TT, int DP>
+static int launch_factor_dmma(const FactorArgs<TT> &g, int64_t N, void *stream) {
+  using C = DmmaCfg<DP>;
+  auto kern = factor_dmma_kernel<TT, DP>;
+  if (C::smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
+    if (e != cudaSuccess) {
+      set_error("posterior_factor: %s", cudaGetErrorString(e));
+      return (int)LAKDE_ECUDA;
+    }
+  }
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * C::WPB, C::smem) != cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  int64_t blocks = (N + C::WPB - 1) / C::WPB;
+  if (blocks > (int64_t)sms * per_sm) blocks = (int64_t)sms * per_sm;
+  kern<<<(unsigned)blocks, 32 * C::WPB, C::smem, as_stream(stream)>>>(g);
+  return check_launch("posterior_factor");
+}
 
 extern "C" int lakde_posterior_factor(int dtype, int64_t N, int64_t D, const void *S, const void *P,
                                       int64_t P_batch_stride, const void *nu_0, const void *a, const void *b,
@@ -481,7 +640,7 @@ extern "C" int lakde_posterior_factor(int dtype, int64_t N, int64_t D, const voi
     return st;
   return dispatch_float(dtype, [&](auto t0) {
     using TT = decltype(t0);
-    FactorArgs<TT> g;
+    FactorArgs<TT> g{};
     g.S = static_cast<const TT *>(S);
     g.P = static_cast<const TT *>(P);
     g.Pbs = P_batch_stride;
@@ -505,31 +664,122 @@ extern "C" int lakde_posterior_factor(int dtype, int64_t N, int64_t D, const voi
       if constexpr (DP <= 8) {
         factor_thread_kernel<TT, DP><<<(unsigned)((N + 127) / 128), 128, 0, as_stream(stream)>>>(g);
       } else {
-        using C = DmmaCfg<DP>;
-        auto kern = factor_dmma_kernel<TT, DP>;
-        if (C::smem > 48 * 1024) {
-          cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
-          if (e != cudaSuccess) {
-            set_error("posterior_factor: %s", cudaGetErrorString(e));
-            return (int)LAKDE_ECUDA;
-          }
-        }
-        int dev = 0, sms = 148;
-        cudaGetDevice(&dev);
-        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
-        // persistent grid: exactly the blocks that are resident at once
-        // (registers and shared memory), so every block starts immediately
-        int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * C::WPB, C::smem) != cudaSuccess ||
-            per_sm < 1) {
-          cudaGetLastError();
-          per_sm = 1;
-        }
-        int64_t blocks = (N + C::WPB - 1) / C::WPB;
-        if (blocks > (int64_t)sms * per_sm) blocks = (int64_t)sms * per_sm;
-        kern<<<(unsigned)blocks, 32 * C::WPB, C::smem, as_stream(stream)>>>(g);
+        return launch_factor_dmma<TT, DP>(g, N, stream);
       }
       return check_launch("posterior_factor");
     });
+  });
+}
+
+// ------------------------------------------------------------- tiled layout
+extern "C" int64_t lakde_tile_count(int64_t D) {
+  int64_t nt = 0;
+  if (D >= 1 && D <= kMaxDim) {
+    dispatch_dp(D, [&](auto dp) {
+      nt = decltype(dp)::value / 8;
+      return 0;
+    });
+  }
+  return nt * (nt + 1) / 2;
+}
+
+template <typename T>
+__global__ void pack_tiles_kernel(const T *__restrict__ src, int64_t sbs, T *__restrict__ dst, int64_t dbs,
+                                  int64_t dts, int64_t doff, int64_t N, int D, int NT) {
+  const int ntile = NT * (NT + 1) / 2;
+  const int64_t total = N * ntile * 64;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
+    const int e = (int)(k & 63);
+    const int64_t rest = k >> 6;
+    const int t = (int)(rest % ntile);
+    const int64_t n = rest / ntile;
+    int I = 0;
+    while ((I + 1) * (I + 2) / 2 <= t) ++I;
+    const int J = t - I * (I + 1) / 2;
+    const int i = 8 * I + (e >> 3), j = 8 * J + (e & 7);
+    const T v = (i < D && j < D && j <= i) ? src[n * sbs + (int64_t)i * D + j] : T(0);
+    dst[n * dbs + (int64_t)t * dts + doff + e] = v;
+  }
+}
+
+extern "C" int lakde_pack_tiles(int dtype, int64_t N, int64_t D, const void *src, int64_t src_batch_stride,
+                                void *dst, int64_t dst_batch_stride, int64_t dst_tile_stride, int64_t dst_offset,
+                                void *stream) {
+  clear_error();
+  if (N < 0 || D < 1 || D > kMaxDim || dst_tile_stride < 64 || dst_offset < 0) {
+    set_error("pack_tiles: invalid sizes");
+    return LAKDE_EINVAL;
+  }
+  if (N == 0) return LAKDE_OK;
+  if (!src || !dst) {
+    set_error("pack_tiles: null pointer");
+    return LAKDE_EINVAL;
+  }
+  if (int st = bind_device("pack_tiles", {dst, src})) return st;
+  const int64_t ntile = lakde_tile_count(D);
+  int NT = 0;
+  while (NT * (NT + 1) / 2 < ntile) ++NT;
+  return dispatch_float(dtype, [&](auto t0) {
+    using T = decltype(t0);
+    const int64_t total = N * ntile * 64;
+    int64_t blocks = (total + 255) / 256;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    pack_tiles_kernel<T><<<(unsigned)blocks, 256, 0, as_stream(stream)>>>(
+        static_cast<const T *>(src), src_batch_stride, static_cast<T *>(dst), dst_batch_stride, dst_tile_stride,
+        dst_offset, N, (int)D, NT);
+    return check_launch("pack_tiles");
+  });
+}
+
+extern "C" int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D, const void *SP, const void *nu_0,
+                                            const void *a, const void *b, void *jitter, double eps, void *W_triu,
+                                            void *logdet_W, int32_t *info, const void *T_tiles, void *trace,
+                                            void *stream) {
+  clear_error();
+  if (dtype != LAKDE_F32) {
+    set_error("posterior_factor_tiled: float32 values only");
+    return LAKDE_EDTYPE;
+  }
+  if (N < 0 || D <= 8 || D > kMaxDim) {
+    set_error("posterior_factor_tiled: needs 8 < D <= %d (N=%lld, D=%lld)", kMaxDim, (long long)N, (long long)D);
+    return LAKDE_EUNSUPPORTED;
+  }
+  if (N == 0) return LAKDE_OK;
+  if (!SP || !nu_0 || !a || !b || !jitter || !W_triu || !logdet_W || !info || (T_tiles && !trace)) {
+    set_error("posterior_factor_tiled: missing buffer");
+    return LAKDE_EINVAL;
+  }
+  if (N > 0x7fffffffLL) {
+    set_error("posterior_factor_tiled: N too large");
+    return LAKDE_EUNSUPPORTED;
+  }
+  if ((reinterpret_cast<uintptr_t>(SP) | reinterpret_cast<uintptr_t>(T_tiles)) & 15u) {
+    set_error("posterior_factor_tiled: SP and T_tiles must be 16-byte aligned");
+    return LAKDE_EINVAL;
+  }
+  if (int st = bind_device("posterior_factor_tiled", {W_triu, SP, nu_0, a, b, jitter, logdet_W, info, T_tiles, trace}))
+    return st;
+  FactorArgs<float> g{};
+  g.SP = static_cast<const float *>(SP);
+  g.Tt = static_cast<const float *>(T_tiles);
+  g.nu0 = static_cast<const float *>(nu_0);
+  g.a = static_cast<const float *>(a);
+  g.b = static_cast<const float *>(b);
+  g.jitter = static_cast<float *>(jitter);
+  g.eps = eps;
+  g.W = static_cast<float *>(W_triu);
+  g.logdet = static_cast<float *>(logdet_W);
+  g.info = info;
+  g.T_lower = 1;
+  g.trace = static_cast<float *>(trace);
+  g.N = N;
+  g.D = (int)D;
+  return dispatch_dp(D, [&](auto dp) {
+    constexpr int DP = decltype(dp)::value;
+    if constexpr (DP <= 8) {
+      return (int)LAKDE_EUNSUPPORTED;
+    } else {
+      return launch_factor_dmma<float, DP>(g, N, stream);
+    }
   });
 }

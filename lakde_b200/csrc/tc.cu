@@ -131,6 +131,8 @@ struct TcArgs {
   float *S;             // M-step output [N, D, D]
   float *nu_out;        // M-step output
   int lower_only;       // M-step: write only j <= i of S_n
+  float *SPo;           // M-step: S_n as lower 8 x 8 tiles into the S halves of SP
+  int ntile;
   float nu0;
   int64_t npts;
   int64_t N;
@@ -543,8 +545,24 @@ __global__ void __launch_bounds__(128, 4) mstep_tc_kernel(TcArgs g) {
     }
     fence_before();
     __syncthreads();
-    // coalesced stores: warp w writes rows w, w + 4, ..., lanes along the row
-    {
+    if (g.SPo) {
+      // tiled: warp w writes tiles w, w + 4, ... (256 contiguous bytes each),
+      // zero outside D and above the diagonal
+      float *dst = g.SPo + n * (int64_t)(g.ntile * 128);
+      for (int t = warp; t < g.ntile; t += 4) {
+        int I = 0;
+        while ((I + 1) * (I + 2) / 2 <= t) ++I;
+        const int J = t - I * (I + 1) / 2;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int e = lane + 32 * h;
+          const int i = 8 * I + (e >> 3), j = 8 * J + (e & 7);
+          const float v = (i < D && j <= i) ? red[i * (DP + 1) + j] : 0.f;
+          dst[t * 128 + e] = any_bad ? NAN : v;
+        }
+      }
+    } else {
+      // coalesced stores: warp w writes rows w, w + 4, ..., lanes along the row
       float *Sn = g.S + n * (int64_t)D * D;
       for (int i = warp; i < D; i += 4) {
         const int jend = g.lower_only ? i + 1 : D;
@@ -957,4 +975,49 @@ extern "C" int lakde_log_pred_density_tc(int dtype, int64_t N, int64_t Nq, int64
   tc::pred_fold_kernel<<<(unsigned)((Nq + 255) / 256), 256, 0, as_stream(stream)>>>(
       g.ws_m, g.ws_s, static_cast<float *>(out), Nq, grid, (float)log((double)N));
   return check_launch("log_pred_density_tc_combine");
+}
+
+extern "C" int64_t lakde_tile_count(int64_t D);
+
+extern "C" int lakde_mstep_tc_tiled(int dtype, int64_t N, int64_t D, int64_t npts, const void *rowptr,
+                                    const void *col, const void *order, const void *r, const void *X,
+                                    int64_t kernel_offset, double nu_0, void *SP, void *nu, int32_t *err,
+                                    void *stream) {
+  clear_error();
+  if (int st = tc_common_checks("mstep_tc_tiled", dtype, N, D, npts, kernel_offset)) return st;
+  if (D <= 8) {
+    set_error("mstep_tc_tiled: needs 8 < D <= 64");
+    return LAKDE_EUNSUPPORTED;
+  }
+  if (N == 0) return LAKDE_OK;
+  if (!rowptr || !col || !r || !X || !SP || !nu || !err) {
+    set_error("mstep_tc_tiled: null pointer");
+    return LAKDE_EINVAL;
+  }
+  if (int st = bind_device("mstep_tc_tiled", {SP, rowptr, col, order, r, X, nu, err})) return st;
+  tc::TcArgs g{};
+  g.rowptr = static_cast<const int64_t *>(rowptr);
+  g.col = static_cast<const int32_t *>(col);
+  g.order = static_cast<const int32_t *>(order);
+  g.r = static_cast<const float *>(r);
+  g.X = static_cast<const float *>(X);
+  g.SPo = static_cast<float *>(SP);
+  g.ntile = (int)lakde_tile_count(D);
+  g.nu_out = static_cast<float *>(nu);
+  g.nu0 = (float)nu_0;
+  g.npts = npts;
+  g.N = N;
+  g.koff = kernel_offset;
+  g.D = (int)D;
+  g.err = err;
+  const size_t smem = tc::MsmCfg::bytes;
+  cudaError_t e = cudaFuncSetAttribute(tc::mstep_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) {
+    set_error("mstep_tc_tiled: %s", cudaGetErrorString(e));
+    return LAKDE_ECUDA;
+  }
+  unsigned grid;
+  tc_grid(smem, 128, N, &grid);
+  tc::mstep_tc_kernel<<<grid, 128, smem, as_stream(stream)>>>(g);
+  return check_launch("mstep_tc_tiled");
 }

@@ -102,15 +102,29 @@ class FusedVI:
         raise NotImplementedError
 
     # --------------------------------------------------------------- kernels
+    # S and P of the mixed path as interleaved 8 x 8 tiles (SP), the trace
+    # factor as tiles (Tt): set by models whose prior is per kernel
+    SP = None
+    Tt = None
+
     def mstep(self):
         rowptr, col = self._tri()
-        if self.precision == "mixed":
+        if self.precision == "mixed" and self.SP is not None:
+            K.mstep_tc_tiled(rowptr, col, self.r, self.X, self.nu_0, self.err, self.SP, self.nu,
+                             order=self.pattern.order)
+        elif self.precision == "mixed":
             K.mstep_tc(rowptr, col, self.r, self.X, self.nu_0, self.err, order=self.pattern.order, S=self.S, nu=self.nu,
                        lower_only=True)
         else:
             K.mstep(rowptr, col, self.r, self.X, self.nu_0, S=self.S, nu=self.nu)
 
     def factor(self, with_trace=True):
+        if self.precision == "mixed" and self.SP is not None:
+            K.posterior_factor_tiled(self.SP, self.D, self.W_inv_jitter, self.eps, self.nu_0_t, self.a, self.b,
+                                     self.U, self.logdet_W, self.info, T_tiles=self.Tt if with_trace else None,
+                                     trace=self.trace if with_trace else None)
+            torch.minimum(self.failed, self.info.min(), out=self.failed)
+            return
         P, T = self._prior()
         K.posterior_factor(
             self.S, self.W_inv_jitter, self.eps, P=P, nu_0=self.nu_0_t, a=self.a, b=self.b,
@@ -222,6 +236,14 @@ class FusedKNN(FusedVI):
         sigma_0.diagonal(dim1=-2, dim2=-1).add_(self.sigma_0_jitter[:, None])
         self.sigma_0 = sigma_0
         self.sigma_0_tril = L0
+        if self.precision == "mixed" and 8 < self.D <= 64:
+            # the tensor-core path reads S and P as interleaved tiles (P halves
+            # fixed here) and the trace factor as tiles
+            nt = K.tile_count(self.D)
+            self.SP = torch.zeros(self.N, nt * 128, dtype=self.dtype, device=self.device)
+            self.Tt = torch.zeros(self.N, nt * 64, dtype=self.dtype, device=self.device)
+            K.pack_tiles(sigma_0, self.SP, 128, 64)
+            K.pack_tiles(L0, self.Tt, 64, 0)
 
     _T_lower = True  # the Cholesky factor of Sigma0
 

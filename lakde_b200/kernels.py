@@ -329,6 +329,53 @@ def log_pred_density(X, W_triu, nu, log_coeff, Y, out=None, workspace=None):
     return out
 
 
+def tile_count(D):
+    """Number of lower 8 x 8 tiles of the tiled layout for dimension D (see include/lakde_b200.h)."""
+    return int(nat.lib().lakde_tile_count(int(D)))
+
+
+def pack_tiles(src, dst, dst_tile_stride, dst_offset):
+    """Lower tiles of src [N, D, D] into dst [N, tiles * dst_tile_stride] at dst_offset within each tile slot."""
+    nat.require_cuda(src, dst, op="pack_tiles")
+    N, D, _ = src.shape
+    src = src.contiguous()
+    assert dst.dtype == src.dtype and dst.is_contiguous() and dst.size(0) == N
+    nat.check(
+        nat.lib().lakde_pack_tiles(nat.dtype_code(src), N, D, nat.ptr(src), D * D, nat.ptr(dst), dst.stride(0),
+                                   int(dst_tile_stride), int(dst_offset), nat.stream_of(src)),
+        "pack_tiles",
+    )
+    return dst
+
+
+def mstep_tc_tiled(rowptr, col, r, X, nu_0, err, SP, nu, order=None, kernel_offset=0):
+    """Tensor-core M-step writing S_n as tiles into the S halves of SP (see include/lakde_b200.h)."""
+    nat.require_cuda(rowptr, col, r, X, err, SP, nu, order, op="mstep_tc_tiled")
+    assert rowptr.dtype == torch.int64 and col.dtype == torch.int32 and err.dtype == torch.int32
+    N = rowptr.numel() - 1
+    nat.check(
+        nat.lib().lakde_mstep_tc_tiled(
+            nat.dtype_code(X), N, X.size(1), X.size(0), nat.ptr(rowptr), nat.ptr(col), nat.ptr(order), nat.ptr(r),
+            nat.ptr(X), int(kernel_offset), float(nu_0), nat.ptr(SP), nat.ptr(nu), nat.ptr(err), nat.stream_of(X),
+        ),
+        "mstep_tc_tiled",
+    )
+
+
+def posterior_factor_tiled(SP, D, jitter, eps, nu_0, a, b, out, logdet, info, T_tiles=None, trace=None):
+    """posterior_factor from the tiled SP (and T) layout (see include/lakde_b200.h)."""
+    nat.require_cuda(SP, jitter, nu_0, a, b, out, logdet, info, T_tiles, trace, op="posterior_factor_tiled")
+    N = jitter.numel()
+    nat.check(
+        nat.lib().lakde_posterior_factor_tiled(
+            nat.dtype_code(SP), N, int(D), nat.ptr(SP), nat.ptr(nu_0), nat.ptr(a), nat.ptr(b), nat.ptr(jitter),
+            float(eps), nat.ptr(out), nat.ptr(logdet), nat.ptr(info), nat.ptr(T_tiles), nat.ptr(trace),
+            nat.stream_of(SP),
+        ),
+        "posterior_factor_tiled",
+    )
+
+
 def knn_elbo(a, b, nu, logdet_W, logdet_sigma_0, mm, c, a_0, b_0, nu_0, D, out=None, workspace=None):
     """ELBO of LocalKNearestKDE in float64 as a 0-dim device tensor (see include/lakde_b200.h)."""
     nat.require_cuda(a, b, nu, logdet_W, logdet_sigma_0, mm, c, op="knn_elbo")

@@ -452,3 +452,65 @@ def test_log_pred_density_tc_matches_fp64(K, D, Nq):
     np.testing.assert_allclose(out.cpu().numpy(), ref, rtol=0, atol=2e-3)
     plain = K.log_pred_density(t(X), t(W), t(nu), lc, t(Y))
     assert float((out - plain).abs().max()) <= 2e-3
+
+
+# ------------------------------------------------------------ tiled layout
+def spd_lowrank(rng, N, D, rank):
+    A = rng.standard_normal((N, D, rank))
+    return A @ np.swapaxes(A, 1, 2) / rank
+
+
+@pytest.mark.parametrize("D", [13, 21, 43, 63, 64])
+def test_factor_tiled_equals_dense_layout(K, D):
+    """Bulk-copied tiles (S and P interleaved, T as tiles) give the dense
+    layout's factorisation bit for bit, jitter ladder included."""
+    rng = np.random.default_rng(D)
+    N = 150
+    S = spd_lowrank(rng, N, D, D).astype(np.float32)
+    S[:20] = spd_lowrank(rng, 20, D, 3).astype(np.float32)  # rank-deficient: the prior carries them
+    S[20:25] = spd_lowrank(rng, 5, D, 2).astype(np.float32)
+    P = spd_lowrank(rng, N, D, D + 2).astype(np.float32)
+    P[20:25] = spd_lowrank(rng, 5, D, 2).astype(np.float32)  # A singular without jitter: the ladder runs
+    Tm = np.linalg.cholesky(P.astype(np.float64) + 1e-3 * np.eye(D)).astype(np.float32)
+    a = rng.uniform(1, 3, N).astype(np.float32)
+    b = rng.uniform(1, 3, N).astype(np.float32)
+    nu0 = torch.tensor([D + 1.5], device=DEV)
+    jit1 = t(np.zeros(N, np.float32))
+    W1, ld1, info1, _, tr1 = K.posterior_factor(t(S), jit1, 1.2e-7, P=t(P), nu_0=nu0, a=t(a), b=t(b), T=t(Tm),
+                                                T_lower=True)
+    nt = K.tile_count(D)
+    SP = torch.zeros(N, nt * 128, device=DEV)
+    Tt = torch.zeros(N, nt * 64, device=DEV)
+    K.pack_tiles(t(S), SP, 128, 0)
+    K.pack_tiles(t(P), SP, 128, 64)
+    K.pack_tiles(t(Tm), Tt, 64, 0)
+    jit2 = t(np.zeros(N, np.float32))
+    W2, ld2, tr2 = torch.empty_like(W1), torch.empty_like(ld1), torch.empty_like(tr1)
+    info2 = torch.empty_like(info1)
+    K.posterior_factor_tiled(SP, D, jit2, 1.2e-7, nu0, t(a), t(b), W2, ld2, info2, T_tiles=Tt, trace=tr2)
+    assert (jit1[20:25] > 0).all()
+    torch.testing.assert_close(info2, info1, rtol=0, atol=0)
+    torch.testing.assert_close(jit2, jit1, rtol=0, atol=0)
+    torch.testing.assert_close(W2, W1, rtol=0, atol=0, equal_nan=True)
+    torch.testing.assert_close(ld2, ld1, rtol=0, atol=0, equal_nan=True)
+    torch.testing.assert_close(tr2, tr1, rtol=0, atol=0, equal_nan=True)
+
+
+@pytest.mark.parametrize("D", [21, 63])
+def test_mstep_tc_tiled_equals_rows(K, D):
+    rng, X, rowptr, cols = tc_problem(D, seed=5)
+    N = len(X)
+    r = rng.uniform(0, 1, size=len(cols)).astype(np.float32)
+    err = torch.zeros(1, dtype=torch.int32, device=DEV)
+    S, nu = K.mstep_tc(t(rowptr), t(cols, torch.int32), t(r), t(X), D + 1.0, err)
+    nt = K.tile_count(D)
+    SP = torch.full((N, nt * 128), 3.0, device=DEV)
+    nu2 = torch.empty_like(nu)
+    K.mstep_tc_tiled(t(rowptr), t(cols, torch.int32), t(r), t(X), D + 1.0, err, SP, nu2)
+    assert int(err) == 0
+    ref = torch.zeros(N, nt * 128, device=DEV)
+    K.pack_tiles(S, ref, 128, 0)
+    view = SP.view(N, nt, 2, 64)
+    torch.testing.assert_close(view[:, :, 0], ref.view(N, nt, 2, 64)[:, :, 0], rtol=0, atol=0)
+    assert (view[:, :, 1] == 3.0).all()  # the P halves are left alone
+    torch.testing.assert_close(nu2, nu, rtol=0, atol=0)
