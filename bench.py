@@ -192,10 +192,7 @@ def kernel_split(eng, reps, flush, torch):
     else:
         tcs = "_tc" if eng.precision == "mixed" else ""
         launches = {"mstep" + tcs: eng.mstep, "posterior_factor": eng.factor,
-                    "estep" + (tcs or "_logrho"): lambda: (
-                        K.estep_tc(p.rowptr, p.col, eng.X, eng.U, eng.nu, eng.logdet_W, eng.err, order=p.order,
-                                   out=eng.logrho) if eng.precision == "mixed" else
-                        K.estep_logrho(p.rowptr, p.col, eng.X, eng.U, eng.nu, eng.logdet_W, out=eng.logrho))}
+                    "estep" + (tcs or "_logrho"): eng.estep_numerators}
     launches["estep_normalise"] = lambda: K.estep_normalise(p.cptr, p.pos, eng.logrho, eng.r, eng.c, eng.rsum, 1,
                                                             eng.threshold)
     out = {k: 0.0 for k in launches}

@@ -329,20 +329,35 @@ LAKDE_API int lakde_mstep_tc_tiled(int dtype, int64_t N, int64_t D, int64_t npts
                                    int32_t *err, void *stream);
 
 /*
+ * lakde_estep_tc with W_triu_n given as X_n = W_triu_n^T in lower tiles
+ * (X_tiles, 64 * tiles floats per kernel, as lakde_posterior_factor_tiled
+ * writes it).
+ */
+LAKDE_API int lakde_estep_tc_tiled(int dtype, int64_t N, int64_t D, int64_t npts,
+                                   const void *rowptr, const void *col,
+                                   const void *order, const void *X,
+                                   int64_t kernel_offset, const void *X_tiles,
+                                   const void *nu, const void *logdet_W,
+                                   void *logrho, int32_t *err, void *stream);
+
+/*
  * lakde_posterior_factor from tiled inputs: A_n = nu_0 a_n / b_n P_n + S_n
  * with S_n and P_n from SP, and the trace term from the lower triangular T_n
  * as tiles (T_tiles, 64 * tiles floats per kernel, may be NULL).  float32,
- * 8 < D <= 64, SP and T_tiles 16-byte aligned; outputs as in
- * lakde_posterior_factor (no L).  info_n = -2 marks a matrix whose input copy
- * did not complete within the wait limit.
+ * 8 < D <= 64, SP and T_tiles 16-byte aligned.  Outputs as in
+ * lakde_posterior_factor (no L), W_triu dense [N, D, D] and / or X_tiles:
+ * X_n = L_n^-1 = W_triu_n^T as lower tiles (64 * tiles floats per kernel);
+ * either may be NULL.  info_n = -2 marks a matrix whose input copy did not
+ * complete within the wait limit.
  */
 LAKDE_API int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D,
                                            const void *SP, const void *nu_0,
                                            const void *a, const void *b,
                                            void *jitter, double eps,
-                                           void *W_triu, void *logdet_W,
-                                           int32_t *info, const void *T_tiles,
-                                           void *trace, void *stream);
+                                           void *W_triu, void *X_tiles,
+                                           void *logdet_W, int32_t *info,
+                                           const void *T_tiles, void *trace,
+                                           void *stream);
 
 /* Workspace bytes lakde_knn_elbo needs. */
 LAKDE_API size_t lakde_knn_elbo_workspace(void);

@@ -36,6 +36,7 @@ struct FactorArgs {
   // 8 x 8 tiles of S then of P (SP, 128 floats per tile) and of T (Tt, 64)
   const float *SP;
   const float *Tt;
+  float *Xt;  // optional output: X = L^-1 (= W_triu^T) as lower tiles, 64 floats per tile
   int64_t N;
   int D;
 };
@@ -433,12 +434,15 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
     g.info[n] = ok ? 0 : -1;
   }
   const T nanv = T(NAN);
-  T *W = g.W + n * (int64_t)D * D;
+  T *W = g.W ? g.W + n * (int64_t)D * D : nullptr;
+  float *Xt = g.Xt ? g.Xt + n * (int64_t)(C::NTILE * 64) : nullptr;
   if (!ok) {
     for (int e = lane; e < D * D; e += 32) {
-      W[e] = nanv;
+      if (W) W[e] = nanv;
       if (lout) lout[e] = nanv;
     }
+    if (Xt)
+      for (int e = lane; e < C::NTILE * 64; e += 32) Xt[e] = NAN;
     if (lane == 0) {
       g.logdet[n] = nanv;
       if (g.Tm || g.Tt) g.trace[n] = nanv;
@@ -457,9 +461,24 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
   T tb[NT][2];
   if (Tn && !staged) load_tcol<T, NT>(Tn, D, g.T_lower, 0, lane, tb);
   dmma::trtri_blocked<NT>(M, lane);
+  if (Xt) {
+    // X as lower tiles, zero outside D (256 contiguous bytes per tile)
+#pragma unroll 1
+    for (int I = 0; I < NT; ++I)
+#pragma unroll 1
+      for (int J = 0; J <= I; ++J) {
+        const int t = I * (I + 1) / 2 + J;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int e = lane + 32 * h;
+          const int i = 8 * I + (e >> 3), j = 8 * J + (e & 7);
+          Xt[t * 64 + e] = (i < D && j <= i) ? (float)M[t * 64 + e] : 0.f;
+        }
+      }
+  }
   // W_triu = X^T: W tile (J, I) = X_IJ^T for I >= J, zero below; lanes write
   // 8 consecutive columns of 4 rows per store
-  {
+  if (W) {
     const int r = lane & 7;
 #pragma unroll 1
     for (int J = 0; J < NT; ++J) {
@@ -733,8 +752,8 @@ extern "C" int lakde_pack_tiles(int dtype, int64_t N, int64_t D, const void *src
 
 extern "C" int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D, const void *SP, const void *nu_0,
                                             const void *a, const void *b, void *jitter, double eps, void *W_triu,
-                                            void *logdet_W, int32_t *info, const void *T_tiles, void *trace,
-                                            void *stream) {
+                                            void *X_tiles, void *logdet_W, int32_t *info, const void *T_tiles,
+                                            void *trace, void *stream) {
   clear_error();
   if (dtype != LAKDE_F32) {
     set_error("posterior_factor_tiled: float32 values only");
@@ -745,7 +764,7 @@ extern "C" int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D, con
     return LAKDE_EUNSUPPORTED;
   }
   if (N == 0) return LAKDE_OK;
-  if (!SP || !nu_0 || !a || !b || !jitter || !W_triu || !logdet_W || !info || (T_tiles && !trace)) {
+  if (!SP || !nu_0 || !a || !b || !jitter || (!W_triu && !X_tiles) || !logdet_W || !info || (T_tiles && !trace)) {
     set_error("posterior_factor_tiled: missing buffer");
     return LAKDE_EINVAL;
   }
@@ -757,7 +776,8 @@ extern "C" int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D, con
     set_error("posterior_factor_tiled: SP and T_tiles must be 16-byte aligned");
     return LAKDE_EINVAL;
   }
-  if (int st = bind_device("posterior_factor_tiled", {W_triu, SP, nu_0, a, b, jitter, logdet_W, info, T_tiles, trace}))
+  if (int st = bind_device("posterior_factor_tiled",
+                           {SP, W_triu, X_tiles, nu_0, a, b, jitter, logdet_W, info, T_tiles, trace}))
     return st;
   FactorArgs<float> g{};
   g.SP = static_cast<const float *>(SP);
@@ -768,6 +788,7 @@ extern "C" int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D, con
   g.jitter = static_cast<float *>(jitter);
   g.eps = eps;
   g.W = static_cast<float *>(W_triu);
+  g.Xt = static_cast<float *>(X_tiles);
   g.logdet = static_cast<float *>(logdet_W);
   g.info = info;
   g.T_lower = 1;

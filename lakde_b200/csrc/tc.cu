@@ -132,6 +132,7 @@ struct TcArgs {
   float *nu_out;        // M-step output
   int lower_only;       // M-step: write only j <= i of S_n
   float *SPo;           // M-step: S_n as lower 8 x 8 tiles into the S halves of SP
+  const float *Xt;      // E-step: W_triu_n^T as lower 8 x 8 tiles (instead of W)
   int ntile;
   float nu0;
   int64_t npts;
@@ -199,15 +200,32 @@ __global__ void __launch_bounds__(128, 4) estep_tc_kernel(TcArgs g) {
     // loads of the row, all issued before use: W_triu[n] (staged below as
     // B = [K = j][N = i], hi and lo), this thread's coordinates of x_n, and
     // nu_n / logdet_n for warp 0
-    const float *Wn = g.W + n * (int64_t)D * D;
     float wv[DP * DP / 256][2];
+    if (g.Xt) {
+      // W[j][i] = X[i][j]: element (i % 8, j % 8) of tile (i / 8, j / 8) of X,
+      // zero above the block diagonal (the tiles are zero outside D)
+      const float *Xn_t = g.Xt + n * (int64_t)(g.ntile * 64);
 #pragma unroll
-    for (int m = 0; m < DP * DP / 256; ++m) {
-      const int e = tid + 128 * m;
-      const int q = e >> 5, ln = e & 31;  // q: (jg, ig) block of 8 x 8
-      const int j = 8 * (q / KG) + (ln >> 2), i = 8 * (q % KG) + 2 * (ln & 3);
-      wv[m][0] = (j < D && i < D) ? Wn[j * D + i] : 0.f;
-      wv[m][1] = (j < D && i + 1 < D) ? Wn[j * D + i + 1] : 0.f;
+      for (int m = 0; m < DP * DP / 256; ++m) {
+        const int e = tid + 128 * m;
+        const int q = e >> 5, ln = e & 31;
+        const int j = 8 * (q / KG) + (ln >> 2), i = 8 * (q % KG) + 2 * (ln & 3);
+        const int I = i >> 3, J = j >> 3;
+        const bool in = I >= J && i < D && j < D;
+        const float *tp = Xn_t + (in ? (I * (I + 1) / 2 + J) * 64 + (i & 7) * 8 + (j & 7) : 0);
+        wv[m][0] = in ? tp[0] : 0.f;
+        wv[m][1] = (in && i + 1 < D) ? tp[8] : 0.f;
+      }
+    } else {
+      const float *Wn = g.W + n * (int64_t)D * D;
+#pragma unroll
+      for (int m = 0; m < DP * DP / 256; ++m) {
+        const int e = tid + 128 * m;
+        const int q = e >> 5, ln = e & 31;  // q: (jg, ig) block of 8 x 8
+        const int j = 8 * (q / KG) + (ln >> 2), i = 8 * (q % KG) + 2 * (ln & 3);
+        wv[m][0] = (j < D && i < D) ? Wn[j * D + i] : 0.f;
+        wv[m][1] = (j < D && i + 1 < D) ? Wn[j * D + i + 1] : 0.f;
+      }
     }
     const float *xnp = g.X + (n + g.koff) * (int64_t)D;
     float xn[KG][2];
@@ -1020,4 +1038,47 @@ extern "C" int lakde_mstep_tc_tiled(int dtype, int64_t N, int64_t D, int64_t npt
   tc_grid(smem, 128, N, &grid);
   tc::mstep_tc_kernel<<<grid, 128, smem, as_stream(stream)>>>(g);
   return check_launch("mstep_tc_tiled");
+}
+
+extern "C" int lakde_estep_tc_tiled(int dtype, int64_t N, int64_t D, int64_t npts, const void *rowptr,
+                                    const void *col, const void *order, const void *X, int64_t kernel_offset,
+                                    const void *X_tiles, const void *nu, const void *logdet_W, void *logrho,
+                                    int32_t *err, void *stream) {
+  clear_error();
+  if (int st = tc_common_checks("estep_tc_tiled", dtype, N, D, npts, kernel_offset)) return st;
+  if (D <= 8) {
+    set_error("estep_tc_tiled: needs 8 < D <= 64");
+    return LAKDE_EUNSUPPORTED;
+  }
+  if (N == 0) return LAKDE_OK;
+  if (!rowptr || !col || !X || !X_tiles || !nu || !logdet_W || !logrho || !err) {
+    set_error("estep_tc_tiled: null pointer");
+    return LAKDE_EINVAL;
+  }
+  if (int st = bind_device("estep_tc_tiled", {logrho, rowptr, col, order, X, X_tiles, nu, logdet_W, err})) return st;
+  tc::TcArgs g{};
+  g.rowptr = static_cast<const int64_t *>(rowptr);
+  g.col = static_cast<const int32_t *>(col);
+  g.order = static_cast<const int32_t *>(order);
+  g.X = static_cast<const float *>(X);
+  g.Xt = static_cast<const float *>(X_tiles);
+  g.ntile = (int)lakde_tile_count(D);
+  g.nu = static_cast<const float *>(nu);
+  g.logdet = static_cast<const float *>(logdet_W);
+  g.logrho = static_cast<float *>(logrho);
+  g.npts = npts;
+  g.N = N;
+  g.koff = kernel_offset;
+  g.D = (int)D;
+  g.err = err;
+  const size_t smem = tc::EsmCfg::bytes;
+  cudaError_t e = cudaFuncSetAttribute(tc::estep_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) {
+    set_error("estep_tc_tiled: %s", cudaGetErrorString(e));
+    return LAKDE_ECUDA;
+  }
+  unsigned grid;
+  tc_grid(smem, 64, N, &grid);
+  tc::estep_tc_kernel<<<grid, 128, smem, as_stream(stream)>>>(g);
+  return check_launch("estep_tc_tiled");
 }

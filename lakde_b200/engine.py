@@ -106,6 +106,7 @@ class FusedVI:
     # factor as tiles (Tt): set by models whose prior is per kernel
     SP = None
     Tt = None
+    Ut = None  # W_triu^T as tiles (the tiled factor's output, the tiled E-step's input)
 
     def mstep(self):
         rowptr, col = self._tri()
@@ -121,8 +122,8 @@ class FusedVI:
     def factor(self, with_trace=True):
         if self.precision == "mixed" and self.SP is not None:
             K.posterior_factor_tiled(self.SP, self.D, self.W_inv_jitter, self.eps, self.nu_0_t, self.a, self.b,
-                                     self.U, self.logdet_W, self.info, T_tiles=self.Tt if with_trace else None,
-                                     trace=self.trace if with_trace else None)
+                                     None, self.logdet_W, self.info, T_tiles=self.Tt if with_trace else None,
+                                     trace=self.trace if with_trace else None, X_tiles=self.Ut)
             torch.minimum(self.failed, self.info.min(), out=self.failed)
             return
         P, T = self._prior()
@@ -133,9 +134,24 @@ class FusedVI:
         )
         torch.minimum(self.failed, self.info.min(), out=self.failed)
 
+    def estep_numerators(self):
+        """log rho of every pair of the pattern (the E-step before the normaliser)."""
+        rowptr, col = self._tri()
+        if self.precision == "mixed" and self.Ut is not None:
+            K.estep_tc_tiled(rowptr, col, self.X, self.Ut, self.nu, self.logdet_W, self.err, order=self.pattern.order,
+                             out=self.logrho)
+        elif self.precision == "mixed":
+            K.estep_tc(rowptr, col, self.X, self.U, self.nu, self.logdet_W, self.err, order=self.pattern.order,
+                       out=self.logrho)
+        else:
+            K.estep_logrho(rowptr, col, self.X, self.U, self.nu, self.logdet_W, out=self.logrho)
+
     def estep(self, mode):
         rowptr, col = self._tri()
-        if self.precision == "mixed":
+        if self.precision == "mixed" and self.Ut is not None:
+            K.estep_tc_tiled(rowptr, col, self.X, self.Ut, self.nu, self.logdet_W, self.err, order=self.pattern.order,
+                             out=self.logrho)
+        elif self.precision == "mixed":
             K.estep_tc(rowptr, col, self.X, self.U, self.nu, self.logdet_W, self.err, order=self.pattern.order,
                        out=self.logrho)
         else:
@@ -242,6 +258,7 @@ class FusedKNN(FusedVI):
             nt = K.tile_count(self.D)
             self.SP = torch.zeros(self.N, nt * 128, dtype=self.dtype, device=self.device)
             self.Tt = torch.zeros(self.N, nt * 64, dtype=self.dtype, device=self.device)
+            self.Ut = torch.zeros(self.N, nt * 64, dtype=self.dtype, device=self.device)
             K.pack_tiles(sigma_0, self.SP, 128, 64)
             K.pack_tiles(L0, self.Tt, 64, 0)
 

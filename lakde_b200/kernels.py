@@ -362,18 +362,38 @@ def mstep_tc_tiled(rowptr, col, r, X, nu_0, err, SP, nu, order=None, kernel_offs
     )
 
 
-def posterior_factor_tiled(SP, D, jitter, eps, nu_0, a, b, out, logdet, info, T_tiles=None, trace=None):
-    """posterior_factor from the tiled SP (and T) layout (see include/lakde_b200.h)."""
-    nat.require_cuda(SP, jitter, nu_0, a, b, out, logdet, info, T_tiles, trace, op="posterior_factor_tiled")
+def posterior_factor_tiled(SP, D, jitter, eps, nu_0, a, b, out, logdet, info, T_tiles=None, trace=None,
+                           X_tiles=None):
+    """posterior_factor from the tiled SP (and T) layout (see include/lakde_b200.h); writes W_triu to
+    ``out`` and / or X = W_triu^T as tiles to ``X_tiles`` (either may be None)."""
+    nat.require_cuda(SP, jitter, nu_0, a, b, out, X_tiles, logdet, info, T_tiles, trace,
+                     op="posterior_factor_tiled")
     N = jitter.numel()
     nat.check(
         nat.lib().lakde_posterior_factor_tiled(
             nat.dtype_code(SP), N, int(D), nat.ptr(SP), nat.ptr(nu_0), nat.ptr(a), nat.ptr(b), nat.ptr(jitter),
-            float(eps), nat.ptr(out), nat.ptr(logdet), nat.ptr(info), nat.ptr(T_tiles), nat.ptr(trace),
-            nat.stream_of(SP),
+            float(eps), nat.ptr(out), nat.ptr(X_tiles), nat.ptr(logdet), nat.ptr(info), nat.ptr(T_tiles),
+            nat.ptr(trace), nat.stream_of(SP),
         ),
         "posterior_factor_tiled",
     )
+
+
+def estep_tc_tiled(rowptr, col, X, X_tiles, nu, logdet_W, err, order=None, out=None, kernel_offset=0):
+    """Tensor-core E-step numerators with W_triu^T given as tiles (see include/lakde_b200.h)."""
+    nat.require_cuda(rowptr, col, X, X_tiles, nu, logdet_W, err, order, op="estep_tc_tiled")
+    assert rowptr.dtype == torch.int64 and col.dtype == torch.int32 and err.dtype == torch.int32
+    N = rowptr.numel() - 1
+    out = X.new_empty(col.numel()) if out is None else out
+    nat.check(
+        nat.lib().lakde_estep_tc_tiled(
+            nat.dtype_code(X), N, X.size(1), X.size(0), nat.ptr(rowptr), nat.ptr(col), nat.ptr(order), nat.ptr(X),
+            int(kernel_offset), nat.ptr(X_tiles), nat.ptr(nu), nat.ptr(logdet_W), nat.ptr(out), nat.ptr(err),
+            nat.stream_of(X),
+        ),
+        "estep_tc_tiled",
+    )
+    return out
 
 
 def knn_elbo(a, b, nu, logdet_W, logdet_sigma_0, mm, c, a_0, b_0, nu_0, D, out=None, workspace=None):

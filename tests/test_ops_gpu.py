@@ -487,7 +487,13 @@ def test_factor_tiled_equals_dense_layout(K, D):
     jit2 = t(np.zeros(N, np.float32))
     W2, ld2, tr2 = torch.empty_like(W1), torch.empty_like(ld1), torch.empty_like(tr1)
     info2 = torch.empty_like(info1)
-    K.posterior_factor_tiled(SP, D, jit2, 1.2e-7, nu0, t(a), t(b), W2, ld2, info2, T_tiles=Tt, trace=tr2)
+    Xt = torch.full((N, nt * 64), 5.0, device=DEV)
+    K.posterior_factor_tiled(SP, D, jit2, 1.2e-7, nu0, t(a), t(b), W2, ld2, info2, T_tiles=Tt, trace=tr2,
+                             X_tiles=Xt)
+    # X = W_triu^T as lower tiles
+    ref = torch.zeros(N, nt * 64, device=DEV)
+    K.pack_tiles(W1.mT.contiguous(), ref, 64, 0)
+    torch.testing.assert_close(Xt, ref, rtol=0, atol=0)
     assert (jit1[20:25] > 0).all()
     torch.testing.assert_close(info2, info1, rtol=0, atol=0)
     torch.testing.assert_close(jit2, jit1, rtol=0, atol=0)
@@ -514,3 +520,20 @@ def test_mstep_tc_tiled_equals_rows(K, D):
     torch.testing.assert_close(view[:, :, 0], ref.view(N, nt, 2, 64)[:, :, 0], rtol=0, atol=0)
     assert (view[:, :, 1] == 3.0).all()  # the P halves are left alone
     torch.testing.assert_close(nu2, nu, rtol=0, atol=0)
+
+
+@pytest.mark.parametrize("D", [21, 43, 63])
+def test_estep_tc_tiled_equals_dense(K, D):
+    rng, X, rowptr, cols = tc_problem(D, seed=9)
+    N = len(X)
+    W = (rand_upper(rng, N, D, np.float64) / np.sqrt(D)).astype(np.float32)
+    nu = rng.uniform(D + 1, D + 10, N).astype(np.float32)
+    logdet = O.chol_logdet(W).astype(np.float32)
+    err = torch.zeros(1, dtype=torch.int32, device=DEV)
+    lr = K.estep_tc(t(rowptr), t(cols, torch.int32), t(X), t(W), t(nu), t(logdet), err)
+    nt = K.tile_count(D)
+    Xt = torch.zeros(N, nt * 64, device=DEV)
+    K.pack_tiles(t(W).mT.contiguous(), Xt, 64, 0)
+    lr2 = K.estep_tc_tiled(t(rowptr), t(cols, torch.int32), t(X), Xt, t(nu), t(logdet), err)
+    assert int(err) == 0
+    torch.testing.assert_close(lr2, lr, rtol=0, atol=0)
