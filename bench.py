@@ -146,13 +146,17 @@ def alg_flops(N, D, nnz):
 
 
 def alg_bytes(N, D, nnz, es=4):
-    """Compulsory bytes per launch of the kernels of one iteration (each array once)."""
-    T = D * D
+    """Compulsory bytes per launch of the kernels of one iteration (each array
+    once; triangular matrices count their triangle, T = D (D + 1) / 2)."""
+    T = D * (D + 1) // 2
     b = {
-        # rowptr, order, col, r, X, prior P and factor T, per-kernel vectors, logrho
+        # rowptr, order, col, r, X, prior P and factor L0, per-kernel vectors, logrho
         "vi_rows": 8 * (N + 1) + 4 * N + 4 * nnz + es * nnz + es * N * D + 2 * es * N * T + 8 * es * N + es * nnz,
+        # rowptr, col, r, X; S (symmetric: its triangle) and nu out
         "mstep": 8 * (N + 1) + 4 * nnz + es * nnz + es * N * D + es * N * T + es * N,
-        "posterior_factor": 3 * es * N * T + es * N * T + 3 * es * N + 4 * es * N + 4 * N,
+        # S, P, L0 in, W_triu out (triangles); nu, a, b, jitter in; logdet, trace, jitter, info out
+        "posterior_factor": 4 * es * N * T + 4 * es * N + 3 * es * N + 4 * N,
+        # rowptr, col, X, W_triu (triangle), nu, logdet in; logrho out
         "estep_logrho": 8 * (N + 1) + 4 * nnz + es * N * D + es * N * T + 2 * es * N + es * nnz,
         "estep_normalise": 8 * (N + 1) + 4 * nnz + es * nnz + es * nnz + 4 * es * N,
     }
