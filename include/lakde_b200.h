@@ -329,14 +329,23 @@ LAKDE_API int lakde_mstep_tc_tiled(int dtype, int64_t N, int64_t D, int64_t npts
                                    int32_t *err, void *stream);
 
 /*
- * lakde_estep_tc with W_triu_n given as X_n = W_triu_n^T in lower tiles
- * (X_tiles, 64 * tiles floats per kernel, as lakde_posterior_factor_tiled
- * writes it).
+ * "W cores": W_triu_n split into bf16 hi = bf16(w) and lo = bf16(w - hi)
+ * (round to nearest), laid out as the 8 x 8 core matrices (J, I), I >= J, of
+ * the E-step's B operand B[j][i] = W_triu_n[j][i]: core (J, I) is 64 bf16,
+ * element (j % 8, i % 8) at 8 (j % 8) + i % 8.  Per kernel, for J = 0 .. NT-1,
+ * the hi cores I = J .. NT-1 then the lo cores I = J .. NT-1: 128 * tiles
+ * bf16 (the bytes of the float32 tiles), zero outside D.
+ */
+
+/*
+ * lakde_estep_tc with W_triu_n given as W cores (W_cores, 16-byte aligned, as
+ * lakde_posterior_factor_tiled writes them): one bulk copy per core segment
+ * instead of the split of W_triu_n in the kernel.
  */
 LAKDE_API int lakde_estep_tc_tiled(int dtype, int64_t N, int64_t D, int64_t npts,
                                    const void *rowptr, const void *col,
                                    const void *order, const void *X,
-                                   int64_t kernel_offset, const void *X_tiles,
+                                   int64_t kernel_offset, const void *W_cores,
                                    const void *nu, const void *logdet_W,
                                    void *logrho, int32_t *err, void *stream);
 
@@ -345,19 +354,20 @@ LAKDE_API int lakde_estep_tc_tiled(int dtype, int64_t N, int64_t D, int64_t npts
  * with S_n and P_n from SP, and the trace term from the lower triangular T_n
  * as tiles (T_tiles, 64 * tiles floats per kernel, may be NULL).  float32,
  * 8 < D <= 64, SP and T_tiles 16-byte aligned.  Outputs as in
- * lakde_posterior_factor (no L), W_triu dense [N, D, D] and / or X_tiles:
- * X_n = L_n^-1 = W_triu_n^T as lower tiles (64 * tiles floats per kernel);
- * either may be NULL.  info_n = -2 marks a matrix whose input copy did not
- * complete within the wait limit.
+ * lakde_posterior_factor (no L), W_triu dense [N, D, D], X_tiles:
+ * X_n = L_n^-1 = W_triu_n^T as lower tiles (64 * tiles floats per kernel)
+ * and / or W_cores (16-byte aligned, 128 * tiles bf16 per kernel; NaN for a
+ * failed matrix); any two may be NULL.  info_n = -2 marks a matrix whose
+ * input copy did not complete within the wait limit.
  */
 LAKDE_API int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D,
                                            const void *SP, const void *nu_0,
                                            const void *a, const void *b,
                                            void *jitter, double eps,
                                            void *W_triu, void *X_tiles,
-                                           void *logdet_W, int32_t *info,
-                                           const void *T_tiles, void *trace,
-                                           void *stream);
+                                           void *W_cores, void *logdet_W,
+                                           int32_t *info, const void *T_tiles,
+                                           void *trace, void *stream);
 
 /* Workspace bytes lakde_knn_elbo needs. */
 LAKDE_API size_t lakde_knn_elbo_workspace(void);

@@ -105,7 +105,7 @@ _SIGNATURES = {
     ),
     "lakde_posterior_factor_tiled": (
         [_c_int, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
-         _c_vp, _c_vp],
+         _c_vp, _c_vp, _c_vp],
         _c_int,
     ),
     "lakde_estep_tc_tiled": (

@@ -9,6 +9,8 @@
 // m8n8k4 f64): blocked right-looking Cholesky over 8 x 8 lower tiles in shared
 // memory, in-place blocked triangular inverse, trace by tile products
 // (factor_dmma.cuh).
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 #include "factor_dmma.cuh"
 
@@ -37,6 +39,9 @@ struct FactorArgs {
   const float *SP;
   const float *Tt;
   float *Xt;  // optional output: X = L^-1 (= W_triu^T) as lower tiles, 64 floats per tile
+  // optional output: W_triu as the bf16 hi / lo core matrices of the tensor-core
+  // E-step's B operand, 64 32-bit words per tile (layout at lakde_posterior_factor_tiled)
+  uint32_t *Wc;
   int64_t N;
   int D;
 };
@@ -281,6 +286,16 @@ __device__ __forceinline__ void assemble_tiles(const FactorArgs<T> &g, int64_t n
 
 // ---- tiled inputs: one bulk copy per matrix, converted in place ----------
 __device__ __forceinline__ uint32_t sm_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// hi = bf16(x), lo = bf16(x - hi), round to nearest, packed pairwise (x0 in the
+// low half): the operand split of the tensor-core kernels
+__device__ __forceinline__ void split_bf16x2(float x0, float x1, uint32_t &hi, uint32_t &lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+  const float2 hf = __bfloat1622float2(h);
+  const __nv_bfloat162 lw = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
+  hi = *reinterpret_cast<const uint32_t *>(&h);
+  lo = *reinterpret_cast<const uint32_t *>(&lw);
+}
 constexpr uint32_t kBulkSpinLimit = 1u << 24;
 
 // Waits for the mbarrier phase; false after kBulkSpinLimit polls.
@@ -324,47 +339,59 @@ __device__ __forceinline__ void bulk_issue(const FactorArgs<float> &g, int64_t n
   }
 }
 
+// Row block of tile t = I (I + 1) / 2 + J of the lower tiles.
+__host__ __device__ constexpr int tile_row(int t) {
+  int I = 0;
+  while ((I + 1) * (I + 2) / 2 <= t) ++I;
+  return I;
+}
+
 // Tile t of the copied area holds S_t then P_t (128 floats = the 512 bytes
-// of FP64 tile t): each lane reads its 2 + 2 values of a batch of tiles,
-// the warp synchronises, and the FP64 entries of A_n + jt I replace them.
+// of FP64 tile t).  Lane l takes the element pair 2 l, 2 l + 1 of every tile
+// (row l / 4, columns 2 (l % 4) and + 1): a batch of NB tiles is read as
+// float2 pairs, the warp synchronises, and the FP64 entries of A_n + jt I
+// replace them as double2 pairs.  SP is zero outside D and above the
+// diagonal, so only the diagonal tiles (jitter, identity padding) and the
+// rows beyond D of the last row block need masks.
 template <int DP>
 __device__ __forceinline__ void convert_tiles(double *M, float scale, float jt, int D, int lane) {
-  constexpr int NT = DP / 8;
-  constexpr int NB = 6;  // tiles per batch
+  constexpr int NT = DP / 8, NTILE = NT * (NT + 1) / 2;
+  constexpr int NB = 9;  // tiles per batch
   const float *F = reinterpret_cast<const float *>(M);
-  int t0 = 0;
-#pragma unroll 1
-  for (int I0 = 0; I0 < NT; ++I0) {
-    // the tiles of row block I0 (I0 + 1 of them) in batches of NB
-#pragma unroll 1
-    for (int J0 = 0; J0 <= I0; J0 += NB) {
-      float sv[NB][2], pv[NB][2];
+  const int r = lane >> 2, c = 2 * (lane & 3);
 #pragma unroll
-      for (int b = 0; b < NB; ++b) {
-        if (J0 + b <= I0) {
-          const float *tt = F + (t0 + J0 + b) * 128;
-          sv[b][0] = tt[lane];
-          sv[b][1] = tt[lane + 32];
-          pv[b][0] = tt[64 + lane];
-          pv[b][1] = tt[64 + lane + 32];
-        }
+  for (int t0 = 0; t0 < NTILE; t0 += NB) {
+    float2 sv[NB], pv[NB];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      if (t0 + b < NTILE) {
+        sv[b] = *reinterpret_cast<const float2 *>(F + (t0 + b) * 128 + 2 * lane);
+        pv[b] = *reinterpret_cast<const float2 *>(F + (t0 + b) * 128 + 64 + 2 * lane);
       }
-      __syncwarp();
-#pragma unroll
-      for (int b = 0; b < NB; ++b) {
-        if (J0 + b <= I0) {
-          double *out = M + (t0 + J0 + b) * 64;
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int e = lane + 32 * h;
-            const int i = 8 * I0 + (e >> 3), j = 8 * (J0 + b) + (e & 7);
-            out[e] = assemble_one<float>(sv[b][h], pv[b][h], true, scale, jt, i, j, D);
-          }
-        }
-      }
-      __syncwarp();
     }
-    t0 += I0 + 1;
+    __syncwarp();
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      const int t = t0 + b;
+      if (t < NTILE) {
+        const int I = tile_row(t), J = t - I * (I + 1) / 2;
+        const int i = 8 * I + r;
+        const float x0 = add_rn(mul_rn(pv[b].x, scale), sv[b].x);
+        const float x1 = add_rn(mul_rn(pv[b].y, scale), sv[b].y);
+        double d0 = (double)x0, d1 = (double)x1;
+        if (I == J) {
+          const int j0 = 8 * J + c;
+          d0 = (i >= D) ? (i == j0 ? 1.0 : 0.0) : (j0 > i ? 0.0 : (j0 == i ? (double)add_rn(x0, jt) : d0));
+          d1 = (i >= D) ? (i == j0 + 1 ? 1.0 : 0.0)
+                        : (j0 + 1 > i ? 0.0 : (j0 + 1 == i ? (double)add_rn(x1, jt) : d1));
+        } else if (i >= D) {
+          d0 = 0.0;
+          d1 = 0.0;
+        }
+        *reinterpret_cast<double2 *>(M + t * 64 + 2 * lane) = make_double2(d0, d1);
+      }
+    }
+    __syncwarp();
   }
 }
 
@@ -436,6 +463,7 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
   const T nanv = T(NAN);
   T *W = g.W ? g.W + n * (int64_t)D * D : nullptr;
   float *Xt = g.Xt ? g.Xt + n * (int64_t)(C::NTILE * 64) : nullptr;
+  uint32_t *Wc = g.Wc ? g.Wc + n * (int64_t)(C::NTILE * 64) : nullptr;
   if (!ok) {
     for (int e = lane; e < D * D; e += 32) {
       if (W) W[e] = nanv;
@@ -443,6 +471,8 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
     }
     if (Xt)
       for (int e = lane; e < C::NTILE * 64; e += 32) Xt[e] = NAN;
+    if (Wc)
+      for (int e = lane; e < C::NTILE * 64; e += 32) Wc[e] = 0x7fc07fc0u;  // bf16 NaN pairs
     if (lane == 0) {
       g.logdet[n] = nanv;
       if (g.Tm || g.Tt) g.trace[n] = nanv;
@@ -475,6 +505,31 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
           Xt[t * 64 + e] = (i < D && j <= i) ? (float)M[t * 64 + e] : 0.f;
         }
       }
+  }
+  if (Wc) {
+    // B[j][i] = W_triu[j][i] = X[i][j] as core matrices (j / 8, i / 8), i / 8 >= j / 8:
+    // line j % 8, element i % 8.  Lane t packs elements i % 8 = 2 (t % 4) and
+    // + 1 of line t / 4, which is word t of the core, so a warp store is one
+    // contiguous core.  Segment J holds the hi cores I = J .. NT - 1, then the
+    // lo cores.
+    const int l = lane >> 2, p = 2 * (lane & 3);
+    uint32_t *seg = Wc;
+#pragma unroll 1
+    for (int J = 0; J < NT; ++J) {
+#pragma unroll 2
+      for (int I = J; I < NT; ++I) {
+        // X is zero above the diagonal; its identity padding (i >= D) is masked
+        const double *tile = M + dmma::tix(I, J);
+        const int i0 = 8 * I + p;
+        const float v0 = i0 < D ? (float)tile[p * 8 + l] : 0.f;
+        const float v1 = i0 + 1 < D ? (float)tile[(p + 1) * 8 + l] : 0.f;
+        uint32_t hi, lo;
+        split_bf16x2(v0, v1, hi, lo);
+        seg[(I - J) * 32 + lane] = hi;
+        seg[(NT - J + I - J) * 32 + lane] = lo;
+      }
+      seg += 2 * (NT - J) * 32;
+    }
   }
   // W_triu = X^T: W tile (J, I) = X_IJ^T for I >= J, zero below; lanes write
   // 8 consecutive columns of 4 rows per store
@@ -752,8 +807,8 @@ extern "C" int lakde_pack_tiles(int dtype, int64_t N, int64_t D, const void *src
 
 extern "C" int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D, const void *SP, const void *nu_0,
                                             const void *a, const void *b, void *jitter, double eps, void *W_triu,
-                                            void *X_tiles, void *logdet_W, int32_t *info, const void *T_tiles,
-                                            void *trace, void *stream) {
+                                            void *X_tiles, void *W_cores, void *logdet_W, int32_t *info,
+                                            const void *T_tiles, void *trace, void *stream) {
   clear_error();
   if (dtype != LAKDE_F32) {
     set_error("posterior_factor_tiled: float32 values only");
@@ -764,7 +819,8 @@ extern "C" int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D, con
     return LAKDE_EUNSUPPORTED;
   }
   if (N == 0) return LAKDE_OK;
-  if (!SP || !nu_0 || !a || !b || !jitter || (!W_triu && !X_tiles) || !logdet_W || !info || (T_tiles && !trace)) {
+  if (!SP || !nu_0 || !a || !b || !jitter || (!W_triu && !X_tiles && !W_cores) || !logdet_W || !info ||
+      (T_tiles && !trace)) {
     set_error("posterior_factor_tiled: missing buffer");
     return LAKDE_EINVAL;
   }
@@ -772,12 +828,13 @@ extern "C" int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D, con
     set_error("posterior_factor_tiled: N too large");
     return LAKDE_EUNSUPPORTED;
   }
-  if ((reinterpret_cast<uintptr_t>(SP) | reinterpret_cast<uintptr_t>(T_tiles)) & 15u) {
-    set_error("posterior_factor_tiled: SP and T_tiles must be 16-byte aligned");
+  if ((reinterpret_cast<uintptr_t>(SP) | reinterpret_cast<uintptr_t>(T_tiles) | reinterpret_cast<uintptr_t>(W_cores)) &
+      15u) {
+    set_error("posterior_factor_tiled: SP, T_tiles and W_cores must be 16-byte aligned");
     return LAKDE_EINVAL;
   }
   if (int st = bind_device("posterior_factor_tiled",
-                           {SP, W_triu, X_tiles, nu_0, a, b, jitter, logdet_W, info, T_tiles, trace}))
+                           {SP, W_triu, X_tiles, W_cores, nu_0, a, b, jitter, logdet_W, info, T_tiles, trace}))
     return st;
   FactorArgs<float> g{};
   g.SP = static_cast<const float *>(SP);
@@ -789,6 +846,7 @@ extern "C" int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D, con
   g.eps = eps;
   g.W = static_cast<float *>(W_triu);
   g.Xt = static_cast<float *>(X_tiles);
+  g.Wc = static_cast<uint32_t *>(W_cores);
   g.logdet = static_cast<float *>(logdet_W);
   g.info = info;
   g.T_lower = 1;

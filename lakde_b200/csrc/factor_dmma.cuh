@@ -65,7 +65,12 @@ __device__ __forceinline__ bool diag_tile(double *t, double *rdiag, double *lt, 
 #pragma unroll
   for (int i = 0; i < 8; ++i)
 #pragma unroll
-    for (int j = 0; j <= i; ++j) a[i * (i + 1) / 2 + j] = t[i * 8 + j];
+    for (int j = 0; j <= i; j += 2) {
+      // pairs (j, j + 1); the element right of the diagonal of an even row is not kept
+      const double2 v = *reinterpret_cast<const double2 *>(t + i * 8 + j);
+      a[i * (i + 1) / 2 + j] = v.x;
+      if (j + 1 <= i) a[i * (i + 1) / 2 + j + 1] = v.y;
+    }
   bool ok = true;
   double rd[8];
 #pragma unroll
@@ -107,14 +112,17 @@ __device__ __forceinline__ bool diag_tile(double *t, double *rdiag, double *lt, 
     a[j * (j + 1) / 2 + j] = rd[j];
   }
   __syncwarp();
-  // lane 0 writes: every lane holds the same values
+  // lane 0 writes, in pairs: every lane holds the same values
   if (lane == 0) {
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
 #pragma unroll
-      for (int j = 0; j < 8; ++j) t[i * 8 + j] = (j <= i) ? a[i * (i + 1) / 2 + j] : 0.0;
-      rdiag[i] = rd[i];
+      for (int j = 0; j < 8; j += 2)
+        *reinterpret_cast<double2 *>(t + i * 8 + j) =
+            make_double2((j <= i) ? a[i * (i + 1) / 2 + j] : 0.0, (j + 1 <= i) ? a[i * (i + 1) / 2 + j + 1] : 0.0);
     }
+#pragma unroll
+    for (int i = 0; i < 8; i += 2) *reinterpret_cast<double2 *>(rdiag + i) = make_double2(rd[i], rd[i + 1]);
   }
   __syncwarp();
   return ok;

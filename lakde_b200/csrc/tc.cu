@@ -132,7 +132,8 @@ struct TcArgs {
   float *nu_out;        // M-step output
   int lower_only;       // M-step: write only j <= i of S_n
   float *SPo;           // M-step: S_n as lower 8 x 8 tiles into the S halves of SP
-  const float *Xt;      // E-step: W_triu_n^T as lower 8 x 8 tiles (instead of W)
+  const uint32_t *Wc;   // E-step: W_triu_n as bf16 hi / lo B-operand core segments (instead of W)
+  int nt;               // E-step with Wc: 8-row tile blocks of the tiled layout
   int ntile;
   float nu0;
   int64_t npts;
@@ -153,10 +154,35 @@ struct EsmCfg {
   static constexpr uint32_t bytes = off_c + MT * 4 + 128;
 };
 
+// Bulk copy of W_triu_n's B cores (WC layout) into B_hi / B_lo: segment J
+// (cores I = J .. nt - 1, hi then lo) lands at core (J, J) of each, i.e.
+// J * (KG + 1) * 128 bytes in.  One thread issues; the cores above the block
+// diagonal and outside nt stay zero from the kernel's start.
+__device__ __forceinline__ void issue_b_cores(const uint32_t *src, int nt, uint32_t bhi, uint32_t blo,
+                                              uint64_t *bar) {
+  const uint32_t total = (uint32_t)(nt * (nt + 1) / 2) * 256u;
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(total) : "memory");
+  const unsigned char *p = reinterpret_cast<const unsigned char *>(src);
+  for (int J = 0; J < nt; ++J) {
+    const uint32_t bytes = (uint32_t)(nt - J) * 128u, o = (uint32_t)J * (KG + 1) * 128u;
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     bhi + o),
+                 "l"(p), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     blo + o),
+                 "l"(p + bytes), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+    p += 2 * bytes;
+  }
+}
+
+template <bool WC>
 __global__ void __launch_bounds__(128, 4) estep_tc_kernel(TcArgs g) {
   using C = EsmCfg;
   extern __shared__ __align__(128) unsigned char sm[];
   __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t bbar;
   __shared__ uint32_t s_tmem;
   __shared__ float s_cst, s_expo;
   unsigned char *Ahi = sm + C::off_Ahi, *Alo = sm + C::off_Alo, *Bhi = sm + C::off_Bhi, *Blo = sm + C::off_Blo;
@@ -165,12 +191,28 @@ __global__ void __launch_bounds__(128, 4) estep_tc_kernel(TcArgs g) {
   const int D = g.D;
 
   if (warp == 0) tmem_alloc(&s_tmem, 64);
-  if (tid == 0) mbar_init(&mbar);
+  if (tid == 0) {
+    mbar_init(&mbar);
+    if (WC) {
+      mbar_init(&bbar);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+  }
+  if (WC) {
+    // B cores that no copy writes (above the block diagonal, outside nt) are
+    // zero; the copied ones are left to the copies
+    uint4 *bz = reinterpret_cast<uint4 *>(Bhi);
+    for (int e = tid; e < (int)(2 * C::B_BYTES / 16); e += 128) {
+      const int core = (e >> 3) & (KG * KG - 1), J = core / KG, I = core % KG;
+      if (I < J || I >= g.nt || J >= g.nt) bz[e] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    fence_async_smem();
+  }
   fence_before();
   __syncthreads();
   fence_after();
   const uint32_t tmem = s_tmem;
-  uint32_t phase = 0;
+  uint32_t phase = 0, bphase = 0;
   bool alive = true;
 
   // A: K-major, pair groups 8 * 128 bytes apart (SBO), K groups 128 bytes apart (LBO)
@@ -201,20 +243,12 @@ __global__ void __launch_bounds__(128, 4) estep_tc_kernel(TcArgs g) {
     // B = [K = j][N = i], hi and lo), this thread's coordinates of x_n, and
     // nu_n / logdet_n for warp 0
     float wv[DP * DP / 256][2];
-    if (g.Xt) {
-      // W[j][i] = X[i][j]: element (i % 8, j % 8) of tile (i / 8, j / 8) of X,
-      // zero above the block diagonal (the tiles are zero outside D)
-      const float *Xn_t = g.Xt + n * (int64_t)(g.ntile * 64);
-#pragma unroll
-      for (int m = 0; m < DP * DP / 256; ++m) {
-        const int e = tid + 128 * m;
-        const int q = e >> 5, ln = e & 31;
-        const int j = 8 * (q / KG) + (ln >> 2), i = 8 * (q % KG) + 2 * (ln & 3);
-        const int I = i >> 3, J = j >> 3;
-        const bool in = I >= J && i < D && j < D;
-        const float *tp = Xn_t + (in ? (I * (I + 1) / 2 + J) * 64 + (i & 7) * 8 + (j & 7) : 0);
-        wv[m][0] = in ? tp[0] : 0.f;
-        wv[m][1] = (in && i + 1 < D) ? tp[8] : 0.f;
+    if (WC) {
+      // W_triu_n's cores by bulk copy: the previous row's MMAs have completed
+      // (their mbarrier wait) and every thread has passed the row-end barrier
+      if (tid == 0 && end > start) {
+        fence_async_smem();
+        issue_b_cores(g.Wc + n * (int64_t)(g.ntile * 64), g.nt, smem_u32(Bhi), smem_u32(Blo), &bbar);
       }
     } else {
       const float *Wn = g.W + n * (int64_t)D * D;
@@ -242,7 +276,7 @@ __global__ void __launch_bounds__(128, 4) estep_tc_kernel(TcArgs g) {
     }
     // B is written once per row: the previous row's last MMAs have completed
     // (their mbarrier wait) and every thread has passed the row-end barrier
-    if (end > start) {
+    if (!WC && end > start) {
 #pragma unroll
       for (int m = 0; m < DP * DP / 256; ++m) {
         const int e = tid + 128 * m;
@@ -319,7 +353,20 @@ __global__ void __launch_bounds__(128, 4) estep_tc_kernel(TcArgs g) {
       }
       fence_async_smem();
       fence_before();
-      __syncthreads();
+      if (WC && base == start) {
+        // the row's B cores have landed (every thread observes the mbarrier)
+        const bool bok = __syncthreads_and(mbar_wait(&bbar, bphase) ? 1 : 0) != 0;
+        bphase ^= 1;
+        if (!bok) {
+          // a copy still in flight may land later: wait once more before leaving
+          mbar_wait(&bbar, bphase ^ 1);
+          if (tid == 0) atomicExch(g.err, 1);
+          alive = false;
+          break;
+        }
+      } else {
+        __syncthreads();
+      }
       if (tid == 0) {
         fence_after();
         const uint32_t ahi = smem_u32(Ahi), alo = smem_u32(Alo), bhi = smem_u32(Bhi), blo = smem_u32(Blo);
@@ -875,14 +922,14 @@ extern "C" int lakde_estep_tc(int dtype, int64_t N, int64_t D, int64_t npts, con
   g.D = (int)D;
   g.err = err;
   const size_t smem = tc::EsmCfg::bytes;
-  cudaError_t e = cudaFuncSetAttribute(tc::estep_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(tc::estep_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) {
     set_error("estep_tc: %s", cudaGetErrorString(e));
     return LAKDE_ECUDA;
   }
   unsigned grid;
   tc_grid(smem, 64, N, &grid);
-  tc::estep_tc_kernel<<<grid, 128, smem, as_stream(stream)>>>(g);
+  tc::estep_tc_kernel<false><<<grid, 128, smem, as_stream(stream)>>>(g);
   return check_launch("estep_tc");
 }
 
@@ -1042,7 +1089,7 @@ extern "C" int lakde_mstep_tc_tiled(int dtype, int64_t N, int64_t D, int64_t npt
 
 extern "C" int lakde_estep_tc_tiled(int dtype, int64_t N, int64_t D, int64_t npts, const void *rowptr,
                                     const void *col, const void *order, const void *X, int64_t kernel_offset,
-                                    const void *X_tiles, const void *nu, const void *logdet_W, void *logrho,
+                                    const void *W_cores, const void *nu, const void *logdet_W, void *logrho,
                                     int32_t *err, void *stream) {
   clear_error();
   if (int st = tc_common_checks("estep_tc_tiled", dtype, N, D, npts, kernel_offset)) return st;
@@ -1051,18 +1098,23 @@ extern "C" int lakde_estep_tc_tiled(int dtype, int64_t N, int64_t D, int64_t npt
     return LAKDE_EUNSUPPORTED;
   }
   if (N == 0) return LAKDE_OK;
-  if (!rowptr || !col || !X || !X_tiles || !nu || !logdet_W || !logrho || !err) {
+  if (!rowptr || !col || !X || !W_cores || !nu || !logdet_W || !logrho || !err) {
     set_error("estep_tc_tiled: null pointer");
     return LAKDE_EINVAL;
   }
-  if (int st = bind_device("estep_tc_tiled", {logrho, rowptr, col, order, X, X_tiles, nu, logdet_W, err})) return st;
+  if (reinterpret_cast<uintptr_t>(W_cores) & 15u) {
+    set_error("estep_tc_tiled: W_cores must be 16-byte aligned");
+    return LAKDE_EINVAL;
+  }
+  if (int st = bind_device("estep_tc_tiled", {logrho, rowptr, col, order, X, W_cores, nu, logdet_W, err})) return st;
   tc::TcArgs g{};
   g.rowptr = static_cast<const int64_t *>(rowptr);
   g.col = static_cast<const int32_t *>(col);
   g.order = static_cast<const int32_t *>(order);
   g.X = static_cast<const float *>(X);
-  g.Xt = static_cast<const float *>(X_tiles);
+  g.Wc = static_cast<const uint32_t *>(W_cores);
   g.ntile = (int)lakde_tile_count(D);
+  while ((g.nt + 1) * (g.nt + 2) / 2 <= g.ntile) ++g.nt;
   g.nu = static_cast<const float *>(nu);
   g.logdet = static_cast<const float *>(logdet_W);
   g.logrho = static_cast<float *>(logrho);
@@ -1072,13 +1124,13 @@ extern "C" int lakde_estep_tc_tiled(int dtype, int64_t N, int64_t D, int64_t npt
   g.D = (int)D;
   g.err = err;
   const size_t smem = tc::EsmCfg::bytes;
-  cudaError_t e = cudaFuncSetAttribute(tc::estep_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(tc::estep_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) {
     set_error("estep_tc_tiled: %s", cudaGetErrorString(e));
     return LAKDE_ECUDA;
   }
   unsigned grid;
   tc_grid(smem, 64, N, &grid);
-  tc::estep_tc_kernel<<<grid, 128, smem, as_stream(stream)>>>(g);
+  tc::estep_tc_kernel<true><<<grid, 128, smem, as_stream(stream)>>>(g);
   return check_launch("estep_tc_tiled");
 }

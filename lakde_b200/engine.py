@@ -106,7 +106,7 @@ class FusedVI:
     # factor as tiles (Tt): set by models whose prior is per kernel
     SP = None
     Tt = None
-    Ut = None  # W_triu^T as tiles (the tiled factor's output, the tiled E-step's input)
+    Wc = None  # W_triu as the E-step's bf16 B-operand cores (the tiled factor's output, the tiled E-step's input)
 
     def mstep(self):
         rowptr, col = self._tri()
@@ -123,7 +123,7 @@ class FusedVI:
         if self.precision == "mixed" and self.SP is not None:
             K.posterior_factor_tiled(self.SP, self.D, self.W_inv_jitter, self.eps, self.nu_0_t, self.a, self.b,
                                      None, self.logdet_W, self.info, T_tiles=self.Tt if with_trace else None,
-                                     trace=self.trace if with_trace else None, X_tiles=self.Ut)
+                                     trace=self.trace if with_trace else None, W_cores=self.Wc)
             torch.minimum(self.failed, self.info.min(), out=self.failed)
             return
         P, T = self._prior()
@@ -137,8 +137,8 @@ class FusedVI:
     def estep_numerators(self):
         """log rho of every pair of the pattern (the E-step before the normaliser)."""
         rowptr, col = self._tri()
-        if self.precision == "mixed" and self.Ut is not None:
-            K.estep_tc_tiled(rowptr, col, self.X, self.Ut, self.nu, self.logdet_W, self.err, order=self.pattern.order,
+        if self.precision == "mixed" and self.Wc is not None:
+            K.estep_tc_tiled(rowptr, col, self.X, self.Wc, self.nu, self.logdet_W, self.err, order=self.pattern.order,
                              out=self.logrho)
         elif self.precision == "mixed":
             K.estep_tc(rowptr, col, self.X, self.U, self.nu, self.logdet_W, self.err, order=self.pattern.order,
@@ -148,8 +148,8 @@ class FusedVI:
 
     def estep(self, mode):
         rowptr, col = self._tri()
-        if self.precision == "mixed" and self.Ut is not None:
-            K.estep_tc_tiled(rowptr, col, self.X, self.Ut, self.nu, self.logdet_W, self.err, order=self.pattern.order,
+        if self.precision == "mixed" and self.Wc is not None:
+            K.estep_tc_tiled(rowptr, col, self.X, self.Wc, self.nu, self.logdet_W, self.err, order=self.pattern.order,
                              out=self.logrho)
         elif self.precision == "mixed":
             K.estep_tc(rowptr, col, self.X, self.U, self.nu, self.logdet_W, self.err, order=self.pattern.order,
@@ -258,7 +258,7 @@ class FusedKNN(FusedVI):
             nt = K.tile_count(self.D)
             self.SP = torch.zeros(self.N, nt * 128, dtype=self.dtype, device=self.device)
             self.Tt = torch.zeros(self.N, nt * 64, dtype=self.dtype, device=self.device)
-            self.Ut = torch.zeros(self.N, nt * 64, dtype=self.dtype, device=self.device)
+            self.Wc = torch.zeros(self.N, nt * 128, dtype=torch.bfloat16, device=self.device)
             K.pack_tiles(sigma_0, self.SP, 128, 64)
             K.pack_tiles(L0, self.Tt, 64, 0)
 

@@ -362,33 +362,43 @@ def mstep_tc_tiled(rowptr, col, r, X, nu_0, err, SP, nu, order=None, kernel_offs
     )
 
 
+def w_cores_like(D, N, device):
+    """Buffer for the W cores of N kernels (bf16 hi / lo B-operand cores; see include/lakde_b200.h)."""
+    return torch.empty(N, tile_count(D) * 128, dtype=torch.bfloat16, device=device)
+
+
 def posterior_factor_tiled(SP, D, jitter, eps, nu_0, a, b, out, logdet, info, T_tiles=None, trace=None,
-                           X_tiles=None):
+                           X_tiles=None, W_cores=None):
     """posterior_factor from the tiled SP (and T) layout (see include/lakde_b200.h); writes W_triu to
-    ``out`` and / or X = W_triu^T as tiles to ``X_tiles`` (either may be None)."""
-    nat.require_cuda(SP, jitter, nu_0, a, b, out, X_tiles, logdet, info, T_tiles, trace,
+    ``out``, X = W_triu^T as tiles to ``X_tiles`` and / or the E-step's W cores to ``W_cores``
+    (any two may be None)."""
+    nat.require_cuda(SP, jitter, nu_0, a, b, out, X_tiles, W_cores, logdet, info, T_tiles, trace,
                      op="posterior_factor_tiled")
     N = jitter.numel()
+    if W_cores is not None:
+        assert W_cores.dtype == torch.bfloat16 and W_cores.is_contiguous()
+        assert W_cores.numel() == N * tile_count(D) * 128
     nat.check(
         nat.lib().lakde_posterior_factor_tiled(
             nat.dtype_code(SP), N, int(D), nat.ptr(SP), nat.ptr(nu_0), nat.ptr(a), nat.ptr(b), nat.ptr(jitter),
-            float(eps), nat.ptr(out), nat.ptr(X_tiles), nat.ptr(logdet), nat.ptr(info), nat.ptr(T_tiles),
-            nat.ptr(trace), nat.stream_of(SP),
+            float(eps), nat.ptr(out), nat.ptr(X_tiles), nat.ptr(W_cores), nat.ptr(logdet), nat.ptr(info),
+            nat.ptr(T_tiles), nat.ptr(trace), nat.stream_of(SP),
         ),
         "posterior_factor_tiled",
     )
 
 
-def estep_tc_tiled(rowptr, col, X, X_tiles, nu, logdet_W, err, order=None, out=None, kernel_offset=0):
-    """Tensor-core E-step numerators with W_triu^T given as tiles (see include/lakde_b200.h)."""
-    nat.require_cuda(rowptr, col, X, X_tiles, nu, logdet_W, err, order, op="estep_tc_tiled")
+def estep_tc_tiled(rowptr, col, X, W_cores, nu, logdet_W, err, order=None, out=None, kernel_offset=0):
+    """Tensor-core E-step numerators with W_triu given as W cores (see include/lakde_b200.h)."""
+    nat.require_cuda(rowptr, col, X, W_cores, nu, logdet_W, err, order, op="estep_tc_tiled")
     assert rowptr.dtype == torch.int64 and col.dtype == torch.int32 and err.dtype == torch.int32
+    assert W_cores.dtype == torch.bfloat16 and W_cores.is_contiguous()
     N = rowptr.numel() - 1
     out = X.new_empty(col.numel()) if out is None else out
     nat.check(
         nat.lib().lakde_estep_tc_tiled(
             nat.dtype_code(X), N, X.size(1), X.size(0), nat.ptr(rowptr), nat.ptr(col), nat.ptr(order), nat.ptr(X),
-            int(kernel_offset), nat.ptr(X_tiles), nat.ptr(nu), nat.ptr(logdet_W), nat.ptr(out), nat.ptr(err),
+            int(kernel_offset), nat.ptr(W_cores), nat.ptr(nu), nat.ptr(logdet_W), nat.ptr(out), nat.ptr(err),
             nat.stream_of(X),
         ),
         "estep_tc_tiled",

@@ -455,6 +455,23 @@ def test_log_pred_density_tc_matches_fp64(K, D, Nq):
 
 
 # ------------------------------------------------------------ tiled layout
+def w_cores_ref(W, D):
+    """The W-cores layout of W_triu [N, D, D] (float32, on the device) built with
+    torch: bf16 hi / lo split (round to nearest even) and the core segments."""
+    N = W.shape[0]
+    nt = {16: 2, 24: 3, 32: 4, 48: 6, 64: 8}[next(p for p in (16, 24, 32, 48, 64) if D <= p)]
+    Wp = torch.zeros(N, 8 * nt, 8 * nt, device=W.device)
+    Wp[:, :D, :D] = W
+    hi = Wp.to(torch.bfloat16)
+    lo = (Wp - hi.float()).to(torch.bfloat16)
+    segs = []
+    for J in range(nt):
+        for part in (hi, lo):
+            for I in range(J, nt):
+                segs.append(part[:, 8 * J:8 * J + 8, 8 * I:8 * I + 8].reshape(N, 64))
+    return torch.cat(segs, dim=1).contiguous()
+
+
 def spd_lowrank(rng, N, D, rank):
     A = rng.standard_normal((N, D, rank))
     return A @ np.swapaxes(A, 1, 2) / rank
@@ -488,12 +505,21 @@ def test_factor_tiled_equals_dense_layout(K, D):
     W2, ld2, tr2 = torch.empty_like(W1), torch.empty_like(ld1), torch.empty_like(tr1)
     info2 = torch.empty_like(info1)
     Xt = torch.full((N, nt * 64), 5.0, device=DEV)
+    Wc = torch.full((N, nt * 128), 5.0, dtype=torch.bfloat16, device=DEV)
     K.posterior_factor_tiled(SP, D, jit2, 1.2e-7, nu0, t(a), t(b), W2, ld2, info2, T_tiles=Tt, trace=tr2,
-                             X_tiles=Xt)
+                             X_tiles=Xt, W_cores=Wc)
     # X = W_triu^T as lower tiles
     ref = torch.zeros(N, nt * 64, device=DEV)
     K.pack_tiles(W1.mT.contiguous(), ref, 64, 0)
     torch.testing.assert_close(Xt, ref, rtol=0, atol=0)
+    # the E-step's bf16 cores of W_triu
+    torch.testing.assert_close(Wc, w_cores_ref(W1, D), rtol=0, atol=0, equal_nan=True)
+    # the cores alone (no dense or tiled float output)
+    Wc2 = torch.zeros_like(Wc)
+    jit3 = t(np.zeros(N, np.float32))
+    K.posterior_factor_tiled(SP, D, jit3, 1.2e-7, nu0, t(a), t(b), None, torch.empty_like(ld1),
+                             torch.empty_like(info1), W_cores=Wc2)
+    torch.testing.assert_close(Wc2, Wc, rtol=0, atol=0, equal_nan=True)
     assert (jit1[20:25] > 0).all()
     torch.testing.assert_close(info2, info1, rtol=0, atol=0)
     torch.testing.assert_close(jit2, jit1, rtol=0, atol=0)
@@ -531,9 +557,13 @@ def test_estep_tc_tiled_equals_dense(K, D):
     logdet = O.chol_logdet(W).astype(np.float32)
     err = torch.zeros(1, dtype=torch.int32, device=DEV)
     lr = K.estep_tc(t(rowptr), t(cols, torch.int32), t(X), t(W), t(nu), t(logdet), err)
-    nt = K.tile_count(D)
-    Xt = torch.zeros(N, nt * 64, device=DEV)
-    K.pack_tiles(t(W).mT.contiguous(), Xt, 64, 0)
-    lr2 = K.estep_tc_tiled(t(rowptr), t(cols, torch.int32), t(X), Xt, t(nu), t(logdet), err)
+    Wc = w_cores_ref(t(W), D)
+    lr2 = K.estep_tc_tiled(t(rowptr), t(cols, torch.int32), t(X), Wc, t(nu), t(logdet), err)
     assert int(err) == 0
     torch.testing.assert_close(lr2, lr, rtol=0, atol=0)
+    # the kernels from an offset into the pattern (a second launch over the
+    # same cores, rows 7.. of the CSR): same values
+    lr3 = K.estep_tc_tiled(t(rowptr[7:] - rowptr[7]), t(cols[rowptr[7]:], torch.int32), t(X), Wc[7:].contiguous(),
+                           t(nu[7:]), t(logdet[7:]), err, kernel_offset=7)
+    assert int(err) == 0
+    torch.testing.assert_close(lr3, lr[rowptr[7]:], rtol=0, atol=0)
