@@ -421,11 +421,15 @@ __global__ void __launch_bounds__(128, 4) estep_tc_kernel(TcArgs g) {
 }
 
 // --------------------------------------------------------------------- M-step
-// smem: G = [MT pairs x (hi | lo) 2 DP] bf16 (core rows of 16 groups),
-// reduction buffer [DP x DP] fp32 reusing G after the MMAs, mbarrier, slot.
+// smem: G = [MT pairs x (hi | lo) 2 DP] bf16 (core rows of 16 groups); after
+// the MMAs the accumulator rows [128 x RSTR] fp32 reuse it.
 struct MsmCfg {
   static constexpr uint32_t G_BYTES = MT * 2 * DP * 2;  // 32 KB
-  static constexpr uint32_t bytes = G_BYTES + 128;
+  // row stride of the accumulator copy: 68 floats keeps the 16-byte row
+  // writes of 8 consecutive threads on distinct bank groups
+  static constexpr int RSTR = DP + 4;
+  static constexpr uint32_t RED_BYTES = 128 * RSTR * 4;  // 34 KB
+  static constexpr uint32_t bytes = (G_BYTES > RED_BYTES ? G_BYTES : RED_BYTES) + 128;
 };
 
 __global__ void __launch_bounds__(128, 4) mstep_tc_kernel(TcArgs g) {
@@ -435,11 +439,12 @@ __global__ void __launch_bounds__(128, 4) mstep_tc_kernel(TcArgs g) {
   __shared__ uint32_t s_tmem;
   __shared__ float s_rs[4];
   unsigned char *G = sm;
-  float *red = reinterpret_cast<float *>(sm);  // [DP][DP + 1] after the MMAs
+  float *red = reinterpret_cast<float *>(sm);  // [128][RSTR] after the MMAs
+  constexpr int RSTR = C::RSTR;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int D = g.D;
 
-  if (warp == 0) tmem_alloc(&s_tmem, 128);
+  if (warp == 0) tmem_alloc(&s_tmem, 64);
   if (tid == 0) mbar_init(&mbar);
   fence_before();
   __syncthreads();
@@ -449,9 +454,11 @@ __global__ void __launch_bounds__(128, 4) mstep_tc_kernel(TcArgs g) {
   bool alive = true;
 
   // G rows are pairs: core (pair group, dim group 0..15), dim groups 0-7 hi, 8-15 lo.
-  // As A = [G_hi^T; G_lo^T] (M = 128 dims, K = pairs) and B = G_hi or G_lo
-  // (K = pairs, N = 64 dims) both are MN-major: MN groups 128 bytes apart (SBO),
-  // K (pair) groups 16 * 128 bytes apart (LBO).
+  // As A = [G_hi^T; G_lo^T] (M = 128 dims, K = pairs) and B = G_hi (K = pairs,
+  // N = 64 dims) both are MN-major: MN groups 128 bytes apart (SBO), K (pair)
+  // groups 16 * 128 bytes apart (LBO).  The accumulator holds H = G_hi^T G_hi
+  // (rows 0-63) and B = G_lo^T G_hi (rows 64-127); G_hi^T G_lo = B^T, so
+  // S = H + B + B^T (the lo * lo term is below the split's precision).
   constexpr uint32_t RS = 2 * KG * 128;  // pair-group stride
   constexpr uint32_t SBO = 128, LBO = RS;
   const uint32_t idesc = idesc_bf16(128, DP, 1, 1);
@@ -547,9 +554,8 @@ __global__ void __launch_bounds__(128, 4) mstep_tc_kernel(TcArgs g) {
         for (int s = 0; s < MT / 16; ++s) {
           const uint32_t ko = 2 * s * LBO;
           const uint32_t acc = (ntile > 0 || s > 0) ? 1u : 0u;
-          // D1 += [G_hi; G_lo]^T G_hi, D2 += [G_hi; G_lo]^T G_lo
+          // [H; B] += [G_hi; G_lo]^T G_hi
           mma(tmem, desc(g0 + ko, LBO, SBO), desc(g0 + ko, LBO, SBO), idesc, acc);
-          mma(tmem + 64, desc(g0 + ko, LBO, SBO), desc(g0 + ko + KG * 128, LBO, SBO), idesc, acc);
         }
         commit(&mbar);
       }
@@ -569,61 +575,44 @@ __global__ void __launch_bounds__(128, 4) mstep_tc_kernel(TcArgs g) {
     rsum = warp_sum(rsum);
     const bool any_bad = __syncthreads_or(bad ? 1 : 0);
     if (lane == 0) s_rs[warp] = rsum;
-    // S = D1[0:64] + D1[64:128] + D2[0:64]; rows 64..127 go through shared memory
-    float v1[16], v2[16];
+    // every thread copies its accumulator row (H row tid, or B row tid - 64)
+    // to shared memory; then S_ij = H_ij + B_ij + B_ji
     const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
-    if (end > start) {
-      if (warp >= 2) {
-        const int i = tid - 64;
 #pragma unroll
-        for (int c0 = 0; c0 < DP; c0 += 16) {
-          tmem_ld16(taddr + c0, v1);
+    for (int c0 = 0; c0 < DP; c0 += 16) {
+      float v1[16];
+      if (end > start) {
+        tmem_ld16(taddr + c0, v1);
+      } else {
 #pragma unroll
-          for (int k = 0; k < 16; ++k) red[i * (DP + 1) + c0 + k] = v1[k];
-        }
+        for (int k = 0; k < 16; ++k) v1[k] = 0.f;
       }
+#pragma unroll
+      for (int k = 0; k < 16; k += 4)
+        *reinterpret_cast<float4 *>(red + tid * RSTR + c0 + k) = make_float4(v1[k], v1[k + 1], v1[k + 2], v1[k + 3]);
     }
     __syncthreads();
     if (tid == 0) {
       const float nv = g.nu0 + (s_rs[0] + s_rs[1] + s_rs[2] + s_rs[3]);
       g.nu_out[n] = any_bad ? NAN : nv;
     }
-    if (warp < 2) {
-      // row i of S into shared memory (row stride DP + 1: conflict-free both
-      // here, a thread per row, and below, a warp per row)
-      const int i = tid;
-#pragma unroll
-      for (int c0 = 0; c0 < DP; c0 += 16) {
-        if (end > start) {
-          tmem_ld16(taddr + c0, v1);
-          tmem_ld16(taddr + 64 + c0, v2);
-        } else {
-#pragma unroll
-          for (int k = 0; k < 16; ++k) v1[k] = v2[k] = 0.f;
-        }
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          float *rv = red + i * (DP + 1) + c0 + k;
-          *rv = (end > start) ? v1[k] + *rv + v2[k] : 0.f;
-        }
-      }
-    }
-    fence_before();
-    __syncthreads();
+    const float *H = red, *Bm = red + 64 * RSTR;
     if (g.SPo) {
       // tiled: warp w writes tiles w, w + 4, ... (256 contiguous bytes each),
       // zero outside D and above the diagonal
       float *dst = g.SPo + n * (int64_t)(g.ntile * 128);
-      for (int t = warp; t < g.ntile; t += 4) {
-        int I = 0;
-        while ((I + 1) * (I + 2) / 2 <= t) ++I;
-        const int J = t - I * (I + 1) / 2;
+      int t = 0;
+      for (int I = 0; I < g.nt; ++I) {
+        for (int J = 0; J <= I; ++J, ++t) {
+          if ((t & 3) != warp) continue;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int e = lane + 32 * h;
-          const int i = 8 * I + (e >> 3), j = 8 * J + (e & 7);
-          const float v = (i < D && j <= i) ? red[i * (DP + 1) + j] : 0.f;
-          dst[t * 128 + e] = any_bad ? NAN : v;
+          for (int h = 0; h < 2; ++h) {
+            const int e = lane + 32 * h;
+            const int i = 8 * I + (e >> 3), j = 8 * J + (e & 7);
+            float v = 0.f;
+            if (i < D && j <= i) v = (H[i * RSTR + j] + Bm[i * RSTR + j]) + Bm[j * RSTR + i];
+            dst[t * 128 + e] = any_bad ? NAN : v;
+          }
         }
       }
     } else {
@@ -631,14 +620,16 @@ __global__ void __launch_bounds__(128, 4) mstep_tc_kernel(TcArgs g) {
       float *Sn = g.S + n * (int64_t)D * D;
       for (int i = warp; i < D; i += 4) {
         const int jend = g.lower_only ? i + 1 : D;
-        for (int j = lane; j < jend; j += 32) Sn[(int64_t)i * D + j] = any_bad ? NAN : red[i * (DP + 1) + j];
+        for (int j = lane; j < jend; j += 32)
+          Sn[(int64_t)i * D + j] = any_bad ? NAN : (H[i * RSTR + j] + Bm[i * RSTR + j]) + Bm[j * RSTR + i];
       }
     }
+    fence_before();
     __syncthreads();
   }
   __syncthreads();
   fence_after();
-  if (warp == 0) tmem_dealloc(tmem, 128);
+  if (warp == 0) tmem_dealloc(tmem, 64);
 }
 
 // ------------------------------------------------------- predictive density
@@ -880,14 +871,22 @@ static int tc_common_checks(const char *what, int dtype, int64_t N, int64_t D, i
   return LAKDE_OK;
 }
 
-// Persistent grid: CTAs per SM limited by shared memory (228 KB per SM, 1 KB
-// reserved per CTA) and tensor memory (512 columns per SM).
-static int tc_grid(size_t smem, int tmem_cols, int64_t N, unsigned *grid) {
+// Persistent grid: the CTAs that are resident at once, limited by shared
+// memory (228 KB per SM, 1 KB reserved per CTA), tensor memory (512 columns
+// per SM) and registers (64 K per SM), so that no CTA waits for a second wave.
+template <typename Kern>
+static int tc_grid(Kern kern, size_t smem, int tmem_cols, int64_t N, unsigned *grid) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
   int per_sm = (int)((228u * 1024u) / (smem + 1024u + 512u));
   if (per_sm > 512 / tmem_cols) per_sm = 512 / tmem_cols;
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, kern) == cudaSuccess && fa.numRegs > 0) {
+    const int regs_warp = ((fa.numRegs * 32 + 255) / 256) * 256;  // allocated per warp in units of 256
+    const int by_regs = 65536 / (4 * regs_warp);
+    if (per_sm > by_regs) per_sm = by_regs;
+  }
   if (per_sm > 8) per_sm = 8;
   if (per_sm < 1) per_sm = 1;
   int64_t g = (int64_t)sms * per_sm;
@@ -928,7 +927,7 @@ extern "C" int lakde_estep_tc(int dtype, int64_t N, int64_t D, int64_t npts, con
     return LAKDE_ECUDA;
   }
   unsigned grid;
-  tc_grid(smem, 64, N, &grid);
+  tc_grid(tc::estep_tc_kernel<false>, smem, 64, N, &grid);
   tc::estep_tc_kernel<false><<<grid, 128, smem, as_stream(stream)>>>(g);
   return check_launch("estep_tc");
 }
@@ -966,7 +965,7 @@ extern "C" int lakde_mstep_tc(int dtype, int64_t N, int64_t D, int64_t npts, con
     return LAKDE_ECUDA;
   }
   unsigned grid;
-  tc_grid(smem, 128, N, &grid);
+  tc_grid(tc::mstep_tc_kernel, smem, 64, N, &grid);
   tc::mstep_tc_kernel<<<grid, 128, smem, as_stream(stream)>>>(g);
   return check_launch("mstep_tc");
 }
@@ -1068,6 +1067,7 @@ extern "C" int lakde_mstep_tc_tiled(int dtype, int64_t N, int64_t D, int64_t npt
   g.X = static_cast<const float *>(X);
   g.SPo = static_cast<float *>(SP);
   g.ntile = (int)lakde_tile_count(D);
+  while ((g.nt + 1) * (g.nt + 2) / 2 <= g.ntile) ++g.nt;
   g.nu_out = static_cast<float *>(nu);
   g.nu0 = (float)nu_0;
   g.npts = npts;
@@ -1082,7 +1082,7 @@ extern "C" int lakde_mstep_tc_tiled(int dtype, int64_t N, int64_t D, int64_t npt
     return LAKDE_ECUDA;
   }
   unsigned grid;
-  tc_grid(smem, 128, N, &grid);
+  tc_grid(tc::mstep_tc_kernel, smem, 64, N, &grid);
   tc::mstep_tc_kernel<<<grid, 128, smem, as_stream(stream)>>>(g);
   return check_launch("mstep_tc_tiled");
 }
@@ -1130,7 +1130,7 @@ extern "C" int lakde_estep_tc_tiled(int dtype, int64_t N, int64_t D, int64_t npt
     return LAKDE_ECUDA;
   }
   unsigned grid;
-  tc_grid(smem, 64, N, &grid);
+  tc_grid(tc::estep_tc_kernel<true>, smem, 64, N, &grid);
   tc::estep_tc_kernel<true><<<grid, 128, smem, as_stream(stream)>>>(g);
   return check_launch("estep_tc_tiled");
 }

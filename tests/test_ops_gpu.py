@@ -528,27 +528,29 @@ def test_factor_tiled_equals_dense_layout(K, D):
     torch.testing.assert_close(tr2, tr1, rtol=0, atol=0, equal_nan=True)
 
 
-@pytest.mark.parametrize("D", [21, 63])
+@pytest.mark.parametrize("D", [13, 21, 36, 43, 63, 64])
 def test_mstep_tc_tiled_equals_rows(K, D):
+    """The tiled M-step equals the dense one bit for bit (every tile written,
+    zero outside D and above the diagonal)."""
     rng, X, rowptr, cols = tc_problem(D, seed=5)
     N = len(X)
     r = rng.uniform(0, 1, size=len(cols)).astype(np.float32)
     err = torch.zeros(1, dtype=torch.int32, device=DEV)
     S, nu = K.mstep_tc(t(rowptr), t(cols, torch.int32), t(r), t(X), D + 1.0, err)
     nt = K.tile_count(D)
+    ref = torch.zeros(N, nt * 128, device=DEV)
+    K.pack_tiles(S, ref, 128, 0)
     SP = torch.full((N, nt * 128), 3.0, device=DEV)
     nu2 = torch.empty_like(nu)
     K.mstep_tc_tiled(t(rowptr), t(cols, torch.int32), t(r), t(X), D + 1.0, err, SP, nu2)
     assert int(err) == 0
-    ref = torch.zeros(N, nt * 128, device=DEV)
-    K.pack_tiles(S, ref, 128, 0)
     view = SP.view(N, nt, 2, 64)
     torch.testing.assert_close(view[:, :, 0], ref.view(N, nt, 2, 64)[:, :, 0], rtol=0, atol=0)
     assert (view[:, :, 1] == 3.0).all()  # the P halves are left alone
     torch.testing.assert_close(nu2, nu, rtol=0, atol=0)
 
 
-@pytest.mark.parametrize("D", [21, 43, 63])
+@pytest.mark.parametrize("D", [13, 21, 36, 43, 63, 64])
 def test_estep_tc_tiled_equals_dense(K, D):
     rng, X, rowptr, cols = tc_problem(D, seed=9)
     N = len(X)
