@@ -513,22 +513,25 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
     // contiguous core.  Segment J holds the hi cores I = J .. NT - 1, then the
     // lo cores.
     const int l = lane >> 2, p = 2 * (lane & 3);
-    uint32_t *seg = Wc;
-#pragma unroll 1
+    const double *src = M + p * 8 + l;
+#pragma unroll
     for (int J = 0; J < NT; ++J) {
-#pragma unroll 2
+      // segment J starts after the 2 (NT - J') cores of every J' < J
+      uint32_t *seg = Wc + 64 * (J * NT - J * (J - 1) / 2);
+#pragma unroll
       for (int I = J; I < NT; ++I) {
-        // X is zero above the diagonal; its identity padding (i >= D) is masked
-        const double *tile = M + dmma::tix(I, J);
-        const int i0 = 8 * I + p;
-        const float v0 = i0 < D ? (float)tile[p * 8 + l] : 0.f;
-        const float v1 = i0 + 1 < D ? (float)tile[(p + 1) * 8 + l] : 0.f;
+        float v0 = (float)src[dmma::tix(I, J)], v1 = (float)src[dmma::tix(I, J) + 8];
+        if (8 * I + 8 > D) {
+          // X is zero above the diagonal; its identity padding (i >= D) is masked
+          const int i0 = 8 * I + p;
+          v0 = i0 < D ? v0 : 0.f;
+          v1 = i0 + 1 < D ? v1 : 0.f;
+        }
         uint32_t hi, lo;
         split_bf16x2(v0, v1, hi, lo);
         seg[(I - J) * 32 + lane] = hi;
         seg[(NT - J + I - J) * 32 + lane] = lo;
       }
-      seg += 2 * (NT - J) * 32;
     }
   }
   // W_triu = X^T: W tile (J, I) = X_IJ^T for I >= J, zero below; lanes write
