@@ -813,13 +813,14 @@ __global__ void __launch_bounds__(128, 2) pred_tc_kernel(PredArgs g) {
           for (int k = 0; k < 16; ++k) q = fmaf(vv[k], vv[k], q);
         }
         if (qi < g.qn) {
-          const float lp = lc[kk] - hh[kk] * log1pf(q);
+          // hardware log and exp: a few 1e-5 nats at most on the density
+          const float lp = lc[kk] - hh[kk] * __logf(1.f + q);
           const float m = pm[qi];
           if (lp > m) {
-            ps[qi] = ps[qi] * expf(m - lp) + 1.f;
+            ps[qi] = ps[qi] * __expf(m - lp) + 1.f;
             pm[qi] = lp;
           } else {
-            ps[qi] += expf(lp - m);
+            ps[qi] += __expf(lp - m);
           }
         }
       }
