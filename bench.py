@@ -369,14 +369,24 @@ def run_sharded(args, world, rank, dev):
     clocks.__exit__(None, None, None)
     # phase split on this rank (the normaliser includes its all-reduces)
     reps = max(3, args.steps // 2)
-    split = {
-        ("mstep_tc" if eng.precision == "mixed" else "mstep"): timed(eng._mstep, reps),
-        "posterior_factor": timed(eng._factor, reps),
-        ("estep_tc" if eng.precision == "mixed" else "estep_logrho"): timed(
-            lambda: eng.ops.estep(eng.pat, eng.X, eng.lo, eng.U, eng.nu, eng.logdet_W, eng.logrho, eng.precision,
-                                  eng.err), reps),
-        "estep_normalise_stages+allreduce": timed(lambda: eng._normalise(1), reps),
-    }
+    if D <= 8:
+        # the fused per-row pass of the shard (what eng.step runs for D <= 8)
+        split = {
+            "vi_rows": timed(
+                lambda: eng.ops.vi_rows(eng.pat, eng.r, eng.X, eng.lo, eng.nu_0, eng.a, eng.b, eng.b_0,
+                                        eng.W_inv_jitter, eng.eps, eng.nu, eng.logdet_W, eng.info, eng.logrho,
+                                        eng.sigma_0, eng.sigma_0_tril, eng.mm), reps),
+            "estep_normalise_stages+allreduce": timed(lambda: eng._normalise(1), reps),
+        }
+    else:
+        split = {
+            ("mstep_tc" if eng.precision == "mixed" else "mstep"): timed(eng._mstep, reps),
+            "posterior_factor": timed(eng._factor, reps),
+            ("estep_tc" if eng.precision == "mixed" else "estep_logrho"): timed(
+                lambda: eng.ops.estep(eng.pat, eng.X, eng.lo, eng.U, eng.nu, eng.logdet_W, eng.logrho,
+                                      eng.precision, eng.err), reps),
+            "estep_normalise_stages+allreduce": timed(lambda: eng._normalise(1), reps),
+        }
     t = torch.tensor([ms], device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

@@ -172,12 +172,15 @@ LAKDE_API int lakde_estep_logrho(int dtype, int64_t N, int64_t D, int64_t npts,
  * lakde/local_knn_kde.py:220-236 for the batch schedule.  rowptr I64 [N+1],
  * col I32 [nnz], order I32 [N] (visiting order, may be NULL), r / logrho [nnz],
  * P and T [D,D] blocks with batch strides (0 = shared), a, b (in/out), jitter
- * (in/out), nu, logdet_W, mm [N] (mm may be NULL), info [N].
+ * (in/out), nu, logdet_W, mm [N] (mm may be NULL), info [N].  Row n is the
+ * kernel centred on point n + kernel_offset of X (a shard's rows; npts >=
+ * N + kernel_offset); the per-kernel arrays are indexed by n.
  */
 LAKDE_API int lakde_vi_rows(int dtype, int64_t N, int64_t D, int64_t npts,
                             const void *rowptr, const void *col,
                             const void *order, const void *r, const void *X,
-                            double nu_0, const void *P, int64_t P_batch_stride,
+                            int64_t kernel_offset, double nu_0,
+                            const void *P, int64_t P_batch_stride,
                             const void *T, int64_t T_batch_stride,
                             const void *a, void *b, double b_0, void *jitter,
                             double eps, void *nu, void *logdet_W, void *mm,
@@ -192,7 +195,8 @@ LAKDE_API int lakde_vi_rows(int dtype, int64_t N, int64_t D, int64_t npts,
 LAKDE_API int lakde_vi_cta(int dtype, int64_t N, int64_t D, int64_t npts,
                            const void *rowptr, const void *col,
                            const void *order, const void *r, const void *X,
-                           double nu_0, const void *P, int64_t P_batch_stride,
+                           int64_t kernel_offset, double nu_0,
+                           const void *P, int64_t P_batch_stride,
                            const void *T, int64_t T_batch_stride, const void *a,
                            void *b, double b_0, void *jitter, double eps,
                            void *nu, void *logdet_W, void *mm, int32_t *info,

@@ -50,12 +50,12 @@ _SIGNATURES = {
         _c_int,
     ),
     "lakde_vi_rows": (
-        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_vp, _c_i64, _c_vp, _c_i64,
+        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64, _c_dbl, _c_vp, _c_i64, _c_vp, _c_i64,
          _c_vp, _c_vp, _c_dbl, _c_vp, _c_dbl, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
         _c_int,
     ),
     "lakde_vi_cta": (
-        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_vp, _c_i64, _c_vp, _c_i64,
+        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64, _c_dbl, _c_vp, _c_i64, _c_vp, _c_i64,
          _c_vp, _c_vp, _c_dbl, _c_vp, _c_dbl, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
         _c_int,
     ),

@@ -62,6 +62,7 @@ struct CtaArgs {
   int32_t *info;
   float *logrho;
   int64_t N;
+  int64_t koff;  // row n is kernel (point) n + koff of X
   int D;
 };
 
@@ -128,7 +129,7 @@ __global__ void __launch_bounds__(128) vi_cta_kernel(CtaArgs g) {
     s_bad = end < start ? 1 : 0;
     s_vsum = 0.f;
   }
-  for (int d = tid; d < C::LDD; d += C::THREADS) xn[d] = d < D ? g.X[n * D + d] : 0.f;
+  for (int d = tid; d < C::LDD; d += C::THREADS) xn[d] = d < D ? g.X[(n + g.koff) * D + d] : 0.f;
 
   // my 4x4 blocks of the lower triangle
   int bi[C::BPT], bj[C::BPT];
@@ -343,7 +344,7 @@ __global__ void __launch_bounds__(128) vi_cta_kernel(CtaArgs g) {
         }
         const float q = quad_tri<float, DP>(Upk, delta);
         out = __fadd_rn(__fmul_rn(q, expo), cst);
-        if ((int64_t)c == n) out = -INFINITY;
+        if ((int64_t)c == n + g.koff) out = -INFINITY;
       }
       g.logrho[base + pp] = out;
     }
@@ -356,13 +357,15 @@ __global__ void __launch_bounds__(128) vi_cta_kernel(CtaArgs g) {
 using namespace lakde;
 
 extern "C" int lakde_vi_cta(int dtype, int64_t N, int64_t D, int64_t npts, const void *rowptr, const void *col,
-                            const void *order, const void *r, const void *X, double nu_0, const void *P,
+                            const void *order, const void *r, const void *X, int64_t kernel_offset, double nu_0,
+                            const void *P,
                             int64_t P_batch_stride, const void *T, int64_t T_batch_stride, const void *a, void *b,
                             double b_0, void *jitter, double eps, void *nu, void *logdet_W, void *mm,
                             int32_t *info, void *logrho, void *stream) {
   clear_error();
-  if (N < 0 || D < 1 || npts < N) {
-    set_error("vi_cta: invalid sizes (N=%lld, D=%lld, npts=%lld)", (long long)N, (long long)D, (long long)npts);
+  if (N < 0 || D < 1 || kernel_offset < 0 || npts < N + kernel_offset) {
+    set_error("vi_cta: invalid sizes (N=%lld, D=%lld, npts=%lld, kernel_offset=%lld)", (long long)N, (long long)D,
+              (long long)npts, (long long)kernel_offset);
     return LAKDE_EINVAL;
   }
   if (N == 0) return LAKDE_OK;
@@ -407,6 +410,7 @@ extern "C" int lakde_vi_cta(int dtype, int64_t N, int64_t D, int64_t npts, const
   g.info = info;
   g.logrho = static_cast<float *>(logrho);
   g.N = N;
+  g.koff = kernel_offset;
   g.D = (int)D;
   auto launch = [&](auto dp) -> int {
     constexpr int DP = decltype(dp)::value;

@@ -43,6 +43,7 @@ struct RowArgs {
   int32_t *info;
   T *logrho;
   int64_t N;
+  int64_t koff;  // row n is kernel (point) n + koff of X
   int D;
 };
 
@@ -146,7 +147,7 @@ __global__ void __launch_bounds__(128, (sizeof(T) == 4 && DP == 8) ? 3 : 1) vi_r
   bool bad = end < start;
 
   T xn[DP];
-  load_row<T, DP>(g.X, n, D, xn);
+  load_row<T, DP>(g.X, n + g.koff, D, xn);
 
   // ---------------------------------------------------------------- M-step
   // pairs in batches of U: the indices, then the point rows of a batch are
@@ -306,7 +307,7 @@ __global__ void __launch_bounds__(128, (sizeof(T) == 4 && DP == 8) ? 3 : 1) vi_r
         q = fma(y[i], y[i], q);
       }
       T lr = f_add(f_mul(q, expo), cst);
-      if (c[u] == n) lr = neg_inf<T>();
+      if (c[u] == n + g.koff) lr = neg_inf<T>();
       g.logrho[p0 + u] = lr;
     }
   }
@@ -317,13 +318,15 @@ __global__ void __launch_bounds__(128, (sizeof(T) == 4 && DP == 8) ? 3 : 1) vi_r
 using namespace lakde;
 
 extern "C" int lakde_vi_rows(int dtype, int64_t N, int64_t D, int64_t npts, const void *rowptr, const void *col,
-                             const void *order, const void *r, const void *X, double nu_0, const void *P,
+                             const void *order, const void *r, const void *X, int64_t kernel_offset, double nu_0,
+                             const void *P,
                              int64_t P_batch_stride, const void *T, int64_t T_batch_stride, const void *a, void *b,
                              double b_0, void *jitter, double eps, void *nu, void *logdet_W, void *mm,
                              int32_t *info, void *logrho, void *stream) {
   clear_error();
-  if (N < 0 || D < 1 || npts < N) {
-    set_error("vi_rows: invalid sizes (N=%lld, D=%lld, npts=%lld)", (long long)N, (long long)D, (long long)npts);
+  if (N < 0 || D < 1 || kernel_offset < 0 || npts < N + kernel_offset) {
+    set_error("vi_rows: invalid sizes (N=%lld, D=%lld, npts=%lld, kernel_offset=%lld)", (long long)N, (long long)D,
+              (long long)npts, (long long)kernel_offset);
     return LAKDE_EINVAL;
   }
   if (N == 0) return LAKDE_OK;
@@ -362,6 +365,7 @@ extern "C" int lakde_vi_rows(int dtype, int64_t N, int64_t D, int64_t npts, cons
     g.info = info;
     g.logrho = static_cast<TT *>(logrho);
     g.N = N;
+    g.koff = kernel_offset;
     g.D = (int)D;
     const unsigned blocks = (unsigned)((N + 127) / 128);
     if (D <= 2)

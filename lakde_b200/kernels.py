@@ -240,10 +240,11 @@ def estep_logrho(rowptr, col, X, W_triu, nu, logdet_W, kernel_offset=0, out=None
 
 
 def vi_rows(rowptr, col, r, X, nu_0, a, b, b_0, jitter, eps, nu, logdet_W, info, logrho, P=None, T=None,
-            order=None, mm=None):
+            order=None, mm=None, kernel_offset=0):
     """Fused per-kernel pass of one VI iteration (see include/lakde_b200.h):
     one thread per row for D <= 8 (lakde_vi_rows), one CTA per row for
-    8 < D <= 64 (lakde_vi_cta, float32)."""
+    8 < D <= 64 (lakde_vi_cta, float32).  Row n is the kernel centred on
+    X[n + kernel_offset] (a shard's rows)."""
     nat.require_cuda(rowptr, col, r, X, a, b, jitter, nu, logdet_W, info, logrho, P, T, order, mm, op="vi_rows")
     entry = nat.lib().lakde_vi_rows if X.size(1) <= 8 else nat.lib().lakde_vi_cta
     N = rowptr.numel() - 1
@@ -255,7 +256,8 @@ def vi_rows(rowptr, col, r, X, nu_0, a, b, b_0, jitter, eps, nu, logdet_W, info,
     nat.check(
         entry(
             nat.dtype_code(X), N, D, X.size(0), nat.ptr(rowptr), nat.ptr(col), nat.ptr(order), nat.ptr(r),
-            nat.ptr(X), float(nu_0), nat.ptr(P), pbs, nat.ptr(T), tbs, nat.ptr(a), nat.ptr(b), float(b_0),
+            nat.ptr(X), int(kernel_offset), float(nu_0), nat.ptr(P), pbs, nat.ptr(T), tbs, nat.ptr(a), nat.ptr(b),
+            float(b_0),
             nat.ptr(jitter), float(eps), nat.ptr(nu), nat.ptr(logdet_W), nat.ptr(mm), nat.ptr(info), nat.ptr(logrho),
             nat.stream_of(X),
         ),

@@ -133,6 +133,12 @@ class CudaShardOps:
     def normalise_stage(self, stage, pat, logrho, r, c, rsum, red, red2, mode, threshold):
         self.K.estep_normalise_stage(stage, pat.cptr, pat.pos, logrho, r, c, rsum, red, red2, mode, threshold)
 
+    def vi_rows(self, pat, r, X, lo, nu_0, a, b, b_0, jitter, eps, nu, logdet, info, logrho, P, T, mm):
+        """M-step, factorisation, b update and log rho of this shard's rows in
+        one pass (D <= 8)."""
+        self.K.vi_rows(pat.rowptr, pat.col, r, X, nu_0, a, b, b_0, jitter, eps, nu, logdet, info, logrho, P=P, T=T,
+                       order=pat.order, mm=mm, kernel_offset=lo)
+
     def pred(self, Xk, U, nu, logdet, Y, precision, err):
         """-log n + logsumexp over these n kernels, per query."""
         lc = self.K.pred_coeff(nu, logdet, Xk.size(1))
@@ -250,6 +256,15 @@ class ShardedKNN:
 
     def step(self):
         """lakde/local_knn_kde.py:209-254 at block_size = N."""
+        if self.D <= 8 and hasattr(self.ops, "vi_rows"):
+            # the shard's rows in one fused pass, then the reduced per-point pass
+            if self.n:
+                self.ops.vi_rows(self.pat, self.r, self.X, self.lo, self.nu_0, self.a, self.b, self.b_0,
+                                 self.W_inv_jitter, self.eps, self.nu, self.logdet_W, self.info, self.logrho,
+                                 self.sigma_0, self.sigma_0_tril, self.mm)
+                torch.minimum(self.failed, self.info.min(), out=self.failed)
+            self._normalise(1)
+            return
         self._mstep()
         self._factor()
         self._estep(mode=1)

@@ -36,7 +36,7 @@ def test_header_and_library_agree(nat):
 
 def test_metadata(nat):
     lib = nat.lib()
-    assert lib.lakde_abi_version() == 3
+    assert lib.lakde_abi_version() == 4
     assert lib.lakde_max_dim() == 64
 
 

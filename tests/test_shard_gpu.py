@@ -78,20 +78,61 @@ def test_tc_kernels_honour_the_kernel_offset(D):
     assert torch.isneginf(lr2[t(self_pair)]).all()
 
 
-@pytest.mark.parametrize("precision", ["fp32", "mixed"])
-def test_world_of_one_matches_the_fused_engine(precision):
+@pytest.mark.parametrize("D", [5, 13])
+def test_fused_row_kernels_honour_the_kernel_offset(D):
+    """lakde_vi_rows (D <= 8) and lakde_vi_cta on a shard's rows (kernel_offset)
+    give the rows of the full launch bit for bit."""
+    from lakde_b200 import kernels as K
+
+    rng = np.random.default_rng(D + 1)
+    N, k = 400, 24
+    X = (rng.standard_normal((N, D)) * 2 + 5).astype(np.float32)
+    graph = O.knn_graph(X, k)
+    ((rows, cols),) = O.knn_pattern(graph)
+    rowptr = O.ind2ptr(rows, N)
+    r = rng.uniform(0, 1, cols.size).astype(np.float32)
+    A = rng.standard_normal((N, D, D + 3))
+    P = (A @ np.swapaxes(A, 1, 2) / (D + 3) + 0.1 * np.eye(D)).astype(np.float32)
+    T = np.linalg.cholesky(P.astype(np.float64)).astype(np.float32)
+    a = np.full(N, 1.0 + D / 2, np.float32)
+    b = rng.uniform(0.5, 2.0, N).astype(np.float32)
+
+    def run(lo, hi):
+        p0, p1 = rowptr[lo], rowptr[hi]
+        n = hi - lo
+        out = dict(b=t(b[lo:hi].copy()), jitter=t(np.zeros(n, np.float32)), nu=t(np.zeros(n, np.float32)),
+                   logdet=t(np.zeros(n, np.float32)), info=t(np.zeros(n, np.int32)),
+                   logrho=t(np.zeros(p1 - p0, np.float32)), mm=t(np.zeros(n, np.float32)))
+        K.vi_rows(t(rowptr[lo:hi + 1] - p0), t(cols[p0:p1], torch.int32), t(r[p0:p1]), t(X), float(D), t(a[lo:hi]),
+                  out["b"], 1e-6, out["jitter"], 1.2e-7, out["nu"], out["logdet"], out["info"], out["logrho"],
+                  P=t(P[lo:hi]), T=t(T[lo:hi]), mm=out["mm"], kernel_offset=lo)
+        return out
+
+    full = run(0, N)
+    lo, hi = 123, 301
+    part = run(lo, hi)
+    p0, p1 = rowptr[lo], rowptr[hi]
+    for key in ("b", "jitter", "nu", "logdet", "info", "mm"):
+        torch.testing.assert_close(part[key], full[key][lo:hi], rtol=0, atol=0)
+    torch.testing.assert_close(part["logrho"], full["logrho"][p0:p1], rtol=0, atol=0)
+    self_pair = cols[p0:p1] == np.repeat(np.arange(lo, hi), np.diff(rowptr[lo:hi + 1]))
+    assert torch.isneginf(part["logrho"][t(self_pair)]).all()
+
+
+@pytest.mark.parametrize("precision,d", [("fp32", 13), ("mixed", 13), ("fp32", 5)])
+def test_world_of_one_matches_the_fused_engine(precision, d):
     from lakde_b200.engine import FusedKNN
     from lakde_b200.shard import ShardedKNN
     from lakde_b200.sparse_util import PairPattern
     from lakde_b200.synthetic import heavy_tail_mixture
     from lakde_b200.utils import compute_knn_graph
 
-    Xn, Yn = heavy_tail_mixture(seed=2, n_train=3000, n_test=200, d=13)
+    Xn, Yn = heavy_tail_mixture(seed=2, n_train=3000, n_test=200, d=d)
     X, Y = t(Xn.astype(np.float32)), t(Yn.astype(np.float32))
     graph = compute_knn_graph(X, 16)
     pattern = PairPattern.from_knn_graph(graph)
     tiny = torch.tensor(1e-6, device=DEV)
-    kw = dict(nu_0=13.0, a_0=tiny, b_0=tiny, threshold=5e-4, init_k=16, precision=precision)
+    kw = dict(nu_0=float(d), a_0=tiny, b_0=tiny, threshold=5e-4, init_k=16, precision=precision)
     ref = FusedKNN(X, graph, pattern, **kw)
     sh = ShardedKNN(X, graph, pattern, **kw)
     ref.init_summaries()
