@@ -382,6 +382,22 @@ LAKDE_API size_t lakde_knn_elbo_workspace(void);
  * mm = nu * trace [N] and the per-point normaliser c [N], written to *out (one
  * double on the device).  Deterministic reduction order.
  */
+/*
+ * The same sums over separate counts: the kernel terms of kernels
+ * 0..n_kernels-1 (a .. mm indexed by kernel) plus the point terms of points
+ * 0..n_points-1 (c), plus `tail` (lakde_knn_elbo passes -N log(N - 1)).
+ * A sharded caller sums the kernel terms of its rows over the ranks and adds
+ * the point terms once.  Either count may be 0 (its arrays may then be NULL).
+ */
+LAKDE_API int lakde_knn_elbo_parts(int dtype, int64_t n_kernels, int64_t n_points,
+                                   int64_t D, const void *a, const void *b,
+                                   const void *nu, const void *logdet_W,
+                                   const void *logdet_sigma_0, const void *mm,
+                                   const void *c, double a_0, double b_0,
+                                   double nu_0, double tail, void *workspace,
+                                   size_t workspace_bytes, double *out,
+                                   void *stream);
+
 LAKDE_API int lakde_knn_elbo(int dtype, int64_t N, int64_t D, const void *a,
                              const void *b, const void *nu, const void *logdet_W,
                              const void *logdet_sigma_0, const void *mm,

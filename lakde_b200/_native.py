@@ -118,6 +118,11 @@ _SIGNATURES = {
          ctypes.c_size_t, _c_vp, _c_vp],
         _c_int,
     ),
+    "lakde_knn_elbo_parts": (
+        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_dbl, _c_dbl,
+         _c_dbl, _c_vp, ctypes.c_size_t, _c_vp, _c_vp],
+        _c_int,
+    ),
     "lakde_log_pred_density_tc": (
         [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, ctypes.c_size_t, _c_vp,
          _c_vp],

@@ -427,6 +427,32 @@ def knn_elbo(a, b, nu, logdet_W, logdet_sigma_0, mm, c, a_0, b_0, nu_0, D, out=N
     return out
 
 
+def knn_elbo_parts(D, a_0, b_0, nu_0, a=None, b=None, nu=None, logdet_W=None, logdet_sigma_0=None, mm=None, c=None,
+                   tail=0.0, out=None, workspace=None, device=None):
+    """float64 sum of the ELBO's kernel terms (a .. mm given) and / or point
+    terms (c given) plus `tail`, as a 0-dim device tensor (see include/lakde_b200.h)."""
+    nat.require_cuda(a, b, nu, logdet_W, logdet_sigma_0, mm, c, op="knn_elbo_parts")
+    ref = a if a is not None else c
+    dev = ref.device if ref is not None else device
+    out = torch.empty((), dtype=torch.float64, device=dev) if out is None else out
+    need = nat.lib().lakde_knn_elbo_workspace()
+    if workspace is None or workspace.numel() < need:
+        workspace = torch.empty(need, dtype=torch.uint8, device=dev)
+    nk = 0 if a is None else a.numel()
+    npts = 0 if c is None else c.numel()
+    dtype = nat.dtype_code(ref) if ref is not None else nat.F32
+    with torch.cuda.device(dev):
+        nat.check(
+            nat.lib().lakde_knn_elbo_parts(
+                dtype, nk, npts, int(D), nat.ptr(a), nat.ptr(b), nat.ptr(nu), nat.ptr(logdet_W),
+                nat.ptr(logdet_sigma_0), nat.ptr(mm), nat.ptr(c), float(a_0), float(b_0), float(nu_0), float(tail),
+                nat.ptr(workspace), workspace.numel(), nat.ptr(out), nat.stream_of(out),
+            ),
+            "knn_elbo_parts",
+        )
+    return out
+
+
 def log_pred_density_tc(X, W_triu, nu, log_coeff, Y, err, out=None, workspace=None):
     """log_pred_density with the quad forms on the tensor cores (bf16 hi + lo),
     float32, D <= 64 (see include/lakde_b200.h)."""

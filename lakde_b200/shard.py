@@ -27,10 +27,8 @@ import math
 
 import torch
 
-from .linalg_util import lgamma, mvdigamma, mvlgamma
 from .sparse_util import PairPattern
 
-LOG2 = math.log(2.0)
 
 
 def balanced_ranges(rowptr, world):
@@ -132,6 +130,17 @@ class CudaShardOps:
 
     def normalise_stage(self, stage, pat, logrho, r, c, rsum, red, red2, mode, threshold):
         self.K.estep_normalise_stage(stage, pat.cptr, pat.pos, logrho, r, c, rsum, red, red2, mode, threshold)
+
+    def elbo_kernel_terms(self, a, b, nu, logdet_W, logdet_sigma_0, mm, D, a_0, b_0, nu_0):
+        """float64 sum of the ELBO's per-kernel terms of this shard's kernels, shape (1,)."""
+        if a.numel() == 0:
+            return torch.zeros(1, dtype=torch.float64, device=a.device)
+        return self.K.knn_elbo_parts(D, a_0, b_0, nu_0, a=a, b=b, nu=nu, logdet_W=logdet_W,
+                                     logdet_sigma_0=logdet_sigma_0, mm=mm).reshape(1)
+
+    def elbo_point_terms(self, c, D, tail):
+        """float64 sum of the ELBO's per-point terms plus tail (0-dim)."""
+        return self.K.knn_elbo_parts(D, 0.0, 1.0, 1.0, c=c, tail=tail)
 
     def vi_rows(self, pat, r, X, lo, nu_0, a, b, b_0, jitter, eps, nu, logdet, info, logrho, P, T, mm):
         """M-step, factorisation, b update and log rho of this shard's rows in
@@ -285,26 +294,10 @@ class ShardedKNN:
         """lakde/local_knn_kde.py:256-341 in float64: per-kernel terms summed
         over the ranks, per-point terms (identical on every rank) added once."""
         N, D = self.N, self.D
-        f = lambda t: t.double()  # noqa: E731
-        a, b, nu = f(self.a), f(self.b), f(self.nu)
-        dev = self.device
-        a_0 = torch.tensor(self.a_0, dtype=torch.float64, device=dev)
-        b_0 = torch.tensor(self.b_0, dtype=torch.float64, device=dev)
-        nu_0 = torch.tensor(self.nu_0, dtype=torch.float64, device=dev)
-        e_tau = a / b
-        e_log_tau = torch.digamma(a) - torch.log(b)
-        e_logdet = mvdigamma(nu / 2, D) + D * LOG2 + f(self.logdet_W)
-        p_tau = torch.sum(-lgamma(a_0) + a_0 * torch.log(b_0) + (a_0 - 1) * e_log_tau - b_0 * e_tau)
-        q_tau = torch.sum(-lgamma(a) + a * torch.log(b) + (a - 1) * e_log_tau - b * e_tau)
-        B_p = -nu_0 / 2 * (D * LOG2 - f(self.logdet_sigma_0) - D * e_log_tau - D * torch.log(nu_0)) - mvlgamma(
-            nu_0 / 2, D)
-        p_lam = torch.sum(B_p + (nu_0 - D - 1) * e_logdet / 2 - e_tau * nu_0 * f(self.mm) / 2)
-        B_q = -nu / 2 * (f(self.logdet_W) + D * LOG2) - mvlgamma(nu / 2, D)
-        q_lam = torch.sum(B_q + (nu - D - 1) * e_logdet / 2 - nu / 2 * D)
-        kern = ((p_lam - q_lam) + (p_tau - q_tau)).reshape(1)
+        kern = self.ops.elbo_kernel_terms(self.a, self.b, self.nu, self.logdet_W, self.logdet_sigma_0, self.mm, D,
+                                          self.a_0, self.b_0, self.nu_0)
         self.comm.sum_(kern)
-        ll = torch.sum(-D / 2 * math.log(2 * math.pi) + f(self.c))
-        return ll + kern[0] - N * math.log(N - 1)
+        return kern[0] + self.ops.elbo_point_terms(self.c, D, -N * math.log(N - 1))
 
     def log_pred_density(self, Y):
         """lakde/local_adaptive_kde.py:200-223 over the kernels of all ranks:

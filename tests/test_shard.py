@@ -10,6 +10,7 @@ same pair pattern.
 """
 
 import datetime
+import math
 import os
 import socket
 import tempfile
@@ -125,6 +126,29 @@ class NumpyShardOps:
     def pred(self, Xk, U, nu, logdet, Y, precision=None, err=None):
         return torch.from_numpy(O.log_pred_density_from_factors(self._np(Xk), self._np(Y), self._np(U),
                                                                 self._np(nu), self._np(logdet)))
+
+    def elbo_kernel_terms(self, a, b, nu, logdet_W, logdet_sigma_0, mm, D, a_0, b_0, nu_0):
+        """lakde/local_knn_kde.py:256-341, the per-kernel terms in float64 (torch on the host)."""
+        from lakde_b200.linalg_util import lgamma, mvdigamma, mvlgamma
+
+        f = lambda t: t.double()  # noqa: E731
+        a, b, nu = f(a), f(b), f(nu)
+        a_0, b_0, nu_0 = (torch.tensor(v, dtype=torch.float64) for v in (a_0, b_0, nu_0))
+        log2 = math.log(2.0)
+        e_tau = a / b
+        e_log_tau = torch.digamma(a) - torch.log(b)
+        e_logdet = mvdigamma(nu / 2, D) + D * log2 + f(logdet_W)
+        p_tau = torch.sum(-lgamma(a_0) + a_0 * torch.log(b_0) + (a_0 - 1) * e_log_tau - b_0 * e_tau)
+        q_tau = torch.sum(-lgamma(a) + a * torch.log(b) + (a - 1) * e_log_tau - b * e_tau)
+        B_p = -nu_0 / 2 * (D * log2 - f(logdet_sigma_0) - D * e_log_tau - D * torch.log(nu_0)) - mvlgamma(
+            nu_0 / 2, D)
+        p_lam = torch.sum(B_p + (nu_0 - D - 1) * e_logdet / 2 - e_tau * nu_0 * f(mm) / 2)
+        B_q = -nu / 2 * (f(logdet_W) + D * log2) - mvlgamma(nu / 2, D)
+        q_lam = torch.sum(B_q + (nu - D - 1) * e_logdet / 2 - nu / 2 * D)
+        return ((p_lam - q_lam) + (p_tau - q_tau)).reshape(1)
+
+    def elbo_point_terms(self, c, D, tail):
+        return torch.sum(-D / 2 * math.log(2 * math.pi) + c.double()) + tail
 
 
 ITERS, THR = 4, 1e-4
