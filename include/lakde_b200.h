@@ -121,7 +121,9 @@ LAKDE_API int lakde_W_inv(int dtype, const void *rowptr, int rowptr_dtype, const
  * jitter [N] is read and updated in place.  Outputs: W_triu [N,D,D],
  * L [N,D,D] (optional), logdet_W [N], info [N] (int32: 0 ok, -1 ladder failed),
  * trace [N] (optional).  All value arrays have `dtype` (F32/F64); a, b, nu_0
- * too.  D <= lakde_max_dim().
+ * too.  D <= lakde_max_dim().  W_cores (optional, float32 only, 16-byte
+ * aligned): W_triu_n also as the W cores of the tensor-core kernels
+ * (lakde_pack_w_cores layout; NaN for a matrix whose ladder failed).
  */
 LAKDE_API int lakde_posterior_factor(int dtype, int64_t N, int64_t D, const void *S,
                            const void *P, int64_t P_batch_stride,
@@ -129,7 +131,7 @@ LAKDE_API int lakde_posterior_factor(int dtype, int64_t N, int64_t D, const void
                            void *jitter, double eps, void *W_triu, void *L,
                            void *logdet_W, int32_t *info, const void *T,
                            int64_t T_batch_stride, int T_lower, void *trace,
-                           void *stream);
+                           void *W_cores, void *stream);
 
 /*
  * Fused-path M-step: the scatter covariance of lakde_W_inv for kernels
@@ -187,49 +189,65 @@ LAKDE_API int lakde_vi_rows(int dtype, int64_t N, int64_t D, int64_t npts,
                             int32_t *info, void *logrho, void *stream);
 
 /*
- * The same per-kernel pass as lakde_vi_rows for 8 < D <= 64 (float32 values),
- * one CTA per kernel row: differences gathered once per chunk of 128 pairs
- * into shared memory, M-step by 4x4 register blocks, FP64 Cholesky, inverse
- * and trace in shared memory, E-step quad forms against the packed W_triu.
+ * Mixed-precision tensor-core kernels (tcgen05.mma kind::tf32), float32
+ * values, D <= 64.  The centred differences (x_m - x_n, and for the M-step
+ * sqrt(r) (x_m - x_n)) and W_triu are split as x = hi + lo with
+ * hi = tf32(x), lo = tf32(x - hi) (round to nearest); every product is
+ * hi*hi + lo*hi + hi*lo with fp32 accumulation in tensor memory, within about
+ * 2^-22 of the exact product (close to plain fp32 arithmetic).
+ *
+ * Point rows are moved by bulk copies, so X (and Y) must have 16-byte
+ * aligned rows: base 16-byte aligned, row stride ldx (elements) a multiple
+ * of 4 and >= D rounded up to 4; columns past D are never used.  Rows are
+ * visited in `order` (may be NULL) through an atomic work queue: `queue`
+ * is one device int32 the call resets to zero on `stream` before the launch
+ * (NULL: a static stride over the grid).  *err is set to 1 if a completion
+ * wait of the kernel times out; the affected rows are then left unwritten.
+ * No counterpart in the reference (its ops run on CUDA cores, lakde/kernels.py).
  */
-LAKDE_API int lakde_vi_cta(int dtype, int64_t N, int64_t D, int64_t npts,
-                           const void *rowptr, const void *col,
-                           const void *order, const void *r, const void *X,
-                           int64_t kernel_offset, double nu_0,
-                           const void *P, int64_t P_batch_stride,
-                           const void *T, int64_t T_batch_stride, const void *a,
-                           void *b, double b_0, void *jitter, double eps,
-                           void *nu, void *logdet_W, void *mm, int32_t *info,
-                           void *logrho, void *stream);
 
 /*
- * Mixed-precision tensor-core E-step (tcgen05, bf16 hi + lo split, fp32
- * accumulation in tensor memory), D <= 64, float32 values: the logrho of
- * lakde_estep_logrho for rows n = 0..N-1, row n being kernel n + kernel_offset
- * of X, rows visited in `order` (may be NULL).  *err is set to 1 if a
- * tensor-core completion wait times out (the affected rows are left unwritten).
+ * "W cores": X_n = L_n^-1 = W_triu_n^T (lower) as the K-major 8 x 4 core
+ * matrices of the tensor-core B operand, float32.  With NT = 8-row blocks
+ * (those of lakde_tile_count for D > 8, one block for D <= 8), per kernel,
+ * for column block J = 0..NT-1 the row blocks I = J..NT-1, each as two cores
+ * (columns 8J..8J+3, then 8J+4..8J+7) of 32 floats: element X[i][j] at
+ * 32 ((j % 8) / 4) + 4 (i % 8) + j % 4.  Zero outside D and above the
+ * diagonal.  lakde_w_cores_floats(D) floats per kernel.
+ */
+LAKDE_API size_t lakde_w_cores_floats(int64_t D);
+
+/* W cores of N kernels from W_triu [N, D, D] (dense, upper; float32). */
+LAKDE_API int lakde_pack_w_cores(int dtype, int64_t N, int64_t D,
+                                 const void *W_triu, void *W_cores,
+                                 void *stream);
+
+/*
+ * Tensor-core E-step: the logrho of lakde_estep_logrho for rows n = 0..N-1,
+ * row n being kernel n + kernel_offset of X [npts, ldx], W_triu given as W
+ * cores (16-byte aligned).  Restates lakde/local_adaptive_kde.py:36-44 on a
+ * pair pattern.
  */
 LAKDE_API int lakde_estep_tc(int dtype, int64_t N, int64_t D, int64_t npts,
                              const void *rowptr, const void *col,
-                             const void *order, const void *X,
-                             int64_t kernel_offset, const void *W_triu,
+                             const void *order, const void *X, int64_t ldx,
+                             int64_t kernel_offset, const void *W_cores,
                              const void *nu, const void *logdet_W, void *logrho,
-                             int32_t *err, void *stream);
+                             int32_t *queue, int32_t *err, void *stream);
 
 /*
- * Mixed-precision tensor-core M-step (tcgen05): S_n and nu_n of lakde_mstep
- * for rows n = 0..N-1, row n being kernel n + kernel_offset of X, D <= 64,
- * float32 values (S is symmetric up to the
+ * Tensor-core M-step: S_n and nu_n of lakde_mstep for rows n = 0..N-1, row n
+ * being kernel n + kernel_offset of X [npts, ldx] (S symmetric up to the
  * order of the fp32 accumulation).  lower_only != 0 writes only the lower
  * triangle (j <= i) of each S_n and leaves the rest untouched (all
- * lakde_posterior_factor reads).  *err as in lakde_estep_tc.
+ * lakde_posterior_factor reads).  Restates lakde/local_adaptive_kde.py:66-81.
  */
 LAKDE_API int lakde_mstep_tc(int dtype, int64_t N, int64_t D, int64_t npts,
                              const void *rowptr, const void *col,
                              const void *order, const void *r, const void *X,
-                             int64_t kernel_offset, double nu_0, void *S,
-                             void *nu, int lower_only, int32_t *err,
-                             void *stream);
+                             int64_t ldx, int64_t kernel_offset, double nu_0,
+                             void *S, void *nu, int lower_only, int32_t *queue,
+                             int32_t *err, void *stream);
 
 /*
  * Per-point normaliser, responsibilities and rebalance over a pair pattern
@@ -323,35 +341,15 @@ LAKDE_API int lakde_pack_tiles(int dtype, int64_t N, int64_t D, const void *src,
 
 /*
  * lakde_mstep_tc with S_n written as tiles into the S halves of SP (per
- * kernel 128 * tiles floats); nu as in lakde_mstep_tc.
+ * kernel 128 * tiles floats); nu as in lakde_mstep_tc.  8 < D <= 64.
  */
 LAKDE_API int lakde_mstep_tc_tiled(int dtype, int64_t N, int64_t D, int64_t npts,
                                    const void *rowptr, const void *col,
                                    const void *order, const void *r,
-                                   const void *X, int64_t kernel_offset,
-                                   double nu_0, void *SP, void *nu,
-                                   int32_t *err, void *stream);
-
-/*
- * "W cores": W_triu_n split into bf16 hi = bf16(w) and lo = bf16(w - hi)
- * (round to nearest), laid out as the 8 x 8 core matrices (J, I), I >= J, of
- * the E-step's B operand B[j][i] = W_triu_n[j][i]: core (J, I) is 64 bf16,
- * element (j % 8, i % 8) at 8 (j % 8) + i % 8.  Per kernel, for J = 0 .. NT-1,
- * the hi cores I = J .. NT-1 then the lo cores I = J .. NT-1: 128 * tiles
- * bf16 (the bytes of the float32 tiles), zero outside D.
- */
-
-/*
- * lakde_estep_tc with W_triu_n given as W cores (W_cores, 16-byte aligned, as
- * lakde_posterior_factor_tiled writes them): one bulk copy per core segment
- * instead of the split of W_triu_n in the kernel.
- */
-LAKDE_API int lakde_estep_tc_tiled(int dtype, int64_t N, int64_t D, int64_t npts,
-                                   const void *rowptr, const void *col,
-                                   const void *order, const void *X,
-                                   int64_t kernel_offset, const void *W_cores,
-                                   const void *nu, const void *logdet_W,
-                                   void *logrho, int32_t *err, void *stream);
+                                   const void *X, int64_t ldx,
+                                   int64_t kernel_offset, double nu_0, void *SP,
+                                   void *nu, int32_t *queue, int32_t *err,
+                                   void *stream);
 
 /*
  * lakde_posterior_factor from tiled inputs: A_n = nu_0 a_n / b_n P_n + S_n
@@ -360,8 +358,8 @@ LAKDE_API int lakde_estep_tc_tiled(int dtype, int64_t N, int64_t D, int64_t npts
  * 8 < D <= 64, SP and T_tiles 16-byte aligned.  Outputs as in
  * lakde_posterior_factor (no L), W_triu dense [N, D, D], X_tiles:
  * X_n = L_n^-1 = W_triu_n^T as lower tiles (64 * tiles floats per kernel)
- * and / or W_cores (16-byte aligned, 128 * tiles bf16 per kernel; NaN for a
- * failed matrix); any two may be NULL.  info_n = -2 marks a matrix whose
+ * and / or W_cores (16-byte aligned, lakde_w_cores_floats(D) floats per
+ * kernel; NaN for a failed matrix); any two may be NULL.  info_n = -2 marks a matrix whose
  * input copy did not complete within the wait limit.
  */
 LAKDE_API int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D,
@@ -410,17 +408,17 @@ LAKDE_API size_t lakde_log_pred_density_tc_workspace(int64_t N, int64_t Nq,
                                                      int64_t D);
 
 /*
- * lakde_log_pred_density with the quad forms on the tensor cores (tcgen05,
- * bf16 hi + lo split of the centred differences and of W_triu, fp32
- * accumulation in tensor memory), float32 values, D <= 64
- * (lakde/local_adaptive_kde.py:200-223).  *err is set to 1 if a tensor-core
- * completion wait times out.
+ * lakde_log_pred_density with the quad forms on the tensor cores (the tf32
+ * hi / lo kernels above; queries in blocks of 2048, every query of a block
+ * against every kernel), float32 values, D <= 64, X [N, ldx] and Y [Nq, ldy]
+ * with 16-byte aligned rows, W_triu given as W cores
+ * (lakde/local_adaptive_kde.py:200-223).  *err as for the tensor-core E-step.
  */
 LAKDE_API int lakde_log_pred_density_tc(int dtype, int64_t N, int64_t Nq,
-                                        int64_t D, const void *X,
-                                        const void *W_triu, const void *nu,
+                                        int64_t D, const void *X, int64_t ldx,
+                                        const void *W_cores, const void *nu,
                                         const void *log_coeff, const void *Y,
-                                        void *out, void *workspace,
+                                        int64_t ldy, void *out, void *workspace,
                                         size_t workspace_bytes, int32_t *err,
                                         void *stream);
 

@@ -10,9 +10,8 @@ numerical kernels run in the in-tree CUDA library lakde_b200/_lib/liblakde_b200.
 (C ABI in include/lakde_b200.h); there is no CPU fallback.
 """
 
-from .callbacks import ELBOCallback, LikelihoodCallback
 from .local_hierarchical_kde import LocalHierarchicalKDE
 from .local_knn_kde import LocalKNearestKDE
 from .sparse_util import PairPattern
 
-__all__ = ["LocalKNearestKDE", "LocalHierarchicalKDE", "ELBOCallback", "LikelihoodCallback", "PairPattern"]
+__all__ = ["LocalKNearestKDE", "LocalHierarchicalKDE", "PairPattern"]

@@ -41,7 +41,7 @@ _SIGNATURES = {
     ),
     "lakde_posterior_factor": (
         [_c_int, _c_i64, _c_i64, _c_vp, _c_vp, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_vp, _c_vp,
-         _c_vp, _c_vp, _c_vp, _c_i64, _c_int, _c_vp, _c_vp],
+         _c_vp, _c_vp, _c_vp, _c_i64, _c_int, _c_vp, _c_vp, _c_vp],
         _c_int,
     ),
     "lakde_estep_logrho": (
@@ -54,21 +54,18 @@ _SIGNATURES = {
          _c_vp, _c_vp, _c_dbl, _c_vp, _c_dbl, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
         _c_int,
     ),
-    "lakde_vi_cta": (
-        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64, _c_dbl, _c_vp, _c_i64, _c_vp, _c_i64,
-         _c_vp, _c_vp, _c_dbl, _c_vp, _c_dbl, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
-        _c_int,
-    ),
     "lakde_estep_tc": (
-        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
-         _c_vp],
+        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp,
+         _c_vp, _c_vp, _c_vp],
         _c_int,
     ),
     "lakde_mstep_tc": (
-        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64, _c_dbl, _c_vp, _c_vp, _c_int,
-         _c_vp, _c_vp],
+        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64, _c_i64, _c_dbl, _c_vp, _c_vp,
+         _c_int, _c_vp, _c_vp, _c_vp],
         _c_int,
     ),
+    "lakde_w_cores_floats": ([_c_i64], ctypes.c_size_t),
+    "lakde_pack_w_cores": ([_c_int, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp], _c_int),
     "lakde_estep_normalise": (
         [_c_int, _c_i64, _c_vp, _c_vp, _c_int, _c_vp, _c_vp, _c_vp, _c_vp, _c_int, _c_dbl, _c_vp],
         _c_int,
@@ -99,18 +96,13 @@ _SIGNATURES = {
     "lakde_tile_count": ([_c_i64], _c_i64),
     "lakde_pack_tiles": ([_c_int, _c_i64, _c_i64, _c_vp, _c_i64, _c_vp, _c_i64, _c_i64, _c_i64, _c_vp], _c_int),
     "lakde_mstep_tc_tiled": (
-        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64, _c_dbl, _c_vp, _c_vp, _c_vp,
-         _c_vp],
+        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64, _c_i64, _c_dbl, _c_vp, _c_vp,
+         _c_vp, _c_vp, _c_vp],
         _c_int,
     ),
     "lakde_posterior_factor_tiled": (
         [_c_int, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
          _c_vp, _c_vp, _c_vp],
-        _c_int,
-    ),
-    "lakde_estep_tc_tiled": (
-        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
-         _c_vp],
         _c_int,
     ),
     "lakde_knn_elbo": (
@@ -124,8 +116,8 @@ _SIGNATURES = {
         _c_int,
     ),
     "lakde_log_pred_density_tc": (
-        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, ctypes.c_size_t, _c_vp,
-         _c_vp],
+        [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64, _c_vp, _c_vp,
+         ctypes.c_size_t, _c_vp, _c_vp],
         _c_int,
     ),
 }

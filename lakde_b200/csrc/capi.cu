@@ -65,6 +65,6 @@ int bind_device(const char *what, std::initializer_list<const void *> ptrs) {
 
 extern "C" const char *lakde_last_error(void) { return lakde::g_last_error; }
 
-extern "C" int lakde_abi_version(void) { return 4; }
+extern "C" int lakde_abi_version(void) { return 5; }
 
 extern "C" int lakde_max_dim(void) { return lakde::kMaxDim; }

@@ -9,8 +9,6 @@
 // m8n8k4 f64): blocked right-looking Cholesky over 8 x 8 lower tiles in shared
 // memory, in-place blocked triangular inverse, trace by tile products
 // (factor_dmma.cuh).
-#include <cuda_bf16.h>
-
 #include "common.cuh"
 #include "factor_dmma.cuh"
 
@@ -39,9 +37,9 @@ struct FactorArgs {
   const float *SP;
   const float *Tt;
   float *Xt;  // optional output: X = L^-1 (= W_triu^T) as lower tiles, 64 floats per tile
-  // optional output: W_triu as the bf16 hi / lo core matrices of the tensor-core
-  // E-step's B operand, 64 32-bit words per tile (layout at lakde_posterior_factor_tiled)
-  uint32_t *Wc;
+  // optional output: X = L^-1 (= W_triu^T) as the W cores of the tensor-core
+  // E-step's B operand, 64 floats per tile (layout at lakde_pack_w_cores)
+  float *Wc;
   int64_t N;
   int D;
 };
@@ -287,15 +285,6 @@ __device__ __forceinline__ void assemble_tiles(const FactorArgs<T> &g, int64_t n
 // ---- tiled inputs: one bulk copy per matrix, converted in place ----------
 __device__ __forceinline__ uint32_t sm_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// hi = bf16(x), lo = bf16(x - hi), round to nearest, packed pairwise (x0 in the
-// low half): the operand split of the tensor-core kernels
-__device__ __forceinline__ void split_bf16x2(float x0, float x1, uint32_t &hi, uint32_t &lo) {
-  const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
-  const float2 hf = __bfloat1622float2(h);
-  const __nv_bfloat162 lw = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
-  hi = *reinterpret_cast<const uint32_t *>(&h);
-  lo = *reinterpret_cast<const uint32_t *>(&lw);
-}
 constexpr uint32_t kBulkSpinLimit = 1u << 24;
 
 // Waits for the mbarrier phase; false after kBulkSpinLimit polls.
@@ -463,7 +452,7 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
   const T nanv = T(NAN);
   T *W = g.W ? g.W + n * (int64_t)D * D : nullptr;
   float *Xt = g.Xt ? g.Xt + n * (int64_t)(C::NTILE * 64) : nullptr;
-  uint32_t *Wc = g.Wc ? g.Wc + n * (int64_t)(C::NTILE * 64) : nullptr;
+  float *Wc = g.Wc ? g.Wc + n * (int64_t)(C::NTILE * 64) : nullptr;
   if (!ok) {
     for (int e = lane; e < D * D; e += 32) {
       if (W) W[e] = nanv;
@@ -472,7 +461,7 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
     if (Xt)
       for (int e = lane; e < C::NTILE * 64; e += 32) Xt[e] = NAN;
     if (Wc)
-      for (int e = lane; e < C::NTILE * 64; e += 32) Wc[e] = 0x7fc07fc0u;  // bf16 NaN pairs
+      for (int e = lane; e < C::NTILE * 64; e += 32) Wc[e] = NAN;
     if (lane == 0) {
       g.logdet[n] = nanv;
       if (g.Tm || g.Tt) g.trace[n] = nanv;
@@ -507,30 +496,23 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
       }
   }
   if (Wc) {
-    // B[j][i] = W_triu[j][i] = X[i][j] as core matrices (j / 8, i / 8), i / 8 >= j / 8:
-    // line j % 8, element i % 8.  Lane t packs elements i % 8 = 2 (t % 4) and
-    // + 1 of line t / 4, which is word t of the core, so a warp store is one
-    // contiguous core.  Segment J holds the hi cores I = J .. NT - 1, then the
-    // lo cores.
-    const int l = lane >> 2, p = 2 * (lane & 3);
-    const double *src = M + p * 8 + l;
+    // segment J holds the tiles I = J .. NT - 1 of column block J, each as two
+    // K-major cores (columns 8 J .. 8 J + 3, then 8 J + 4 .. 8 J + 7); lane l
+    // writes row l / 4, column l % 4 of a core, so a warp store is one
+    // contiguous 128-byte core.  Rows i >= D (the identity padding) are zero.
+    const int rr = lane >> 2, cc = lane & 3;
 #pragma unroll
     for (int J = 0; J < NT; ++J) {
-      // segment J starts after the 2 (NT - J') cores of every J' < J
-      uint32_t *seg = Wc + 64 * (J * NT - J * (J - 1) / 2);
+      float *seg = Wc + 64 * (J * NT - J * (J - 1) / 2);
 #pragma unroll
       for (int I = J; I < NT; ++I) {
-        float v0 = (float)src[dmma::tix(I, J)], v1 = (float)src[dmma::tix(I, J) + 8];
-        if (8 * I + 8 > D) {
-          // X is zero above the diagonal; its identity padding (i >= D) is masked
-          const int i0 = 8 * I + p;
-          v0 = i0 < D ? v0 : 0.f;
-          v1 = i0 + 1 < D ? v1 : 0.f;
+        const int i = 8 * I + rr;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int j = 8 * J + 4 * h + cc;
+          const double v = M[dmma::tix(I, J) + rr * 8 + 4 * h + cc];
+          seg[(I - J) * 64 + h * 32 + lane] = (i < D && j <= i) ? (float)v : 0.f;
         }
-        uint32_t hi, lo;
-        split_bf16x2(v0, v1, hi, lo);
-        seg[(I - J) * 32 + lane] = hi;
-        seg[(NT - J + I - J) * 32 + lane] = lo;
       }
     }
   }
@@ -698,7 +680,7 @@ extern "C" int lakde_posterior_factor(int dtype, int64_t N, int64_t D, const voi
                                       int64_t P_batch_stride, const void *nu_0, const void *a, const void *b,
                                       void *jitter, double eps, void *W_triu, void *L, void *logdet_W,
                                       int32_t *info, const void *T, int64_t T_batch_stride, int T_lower,
-                                      void *trace, void *stream) {
+                                      void *trace, void *W_cores, void *stream) {
   clear_error();
   if (N < 0 || D < 1) {
     set_error("posterior_factor: invalid sizes (N=%lld, D=%lld)", (long long)N, (long long)D);
@@ -713,7 +695,12 @@ extern "C" int lakde_posterior_factor(int dtype, int64_t N, int64_t D, const voi
     set_error("posterior_factor: N too large");
     return LAKDE_EUNSUPPORTED;
   }
-  if (int st = bind_device("posterior_factor", {W_triu, S, P, nu_0, a, b, jitter, L, logdet_W, info, T, trace}))
+  if (W_cores && (dtype != LAKDE_F32 || (reinterpret_cast<uintptr_t>(W_cores) & 15u))) {
+    set_error("posterior_factor: W_cores needs float32 values and a 16-byte aligned buffer");
+    return LAKDE_EINVAL;
+  }
+  if (int st = bind_device("posterior_factor",
+                           {W_triu, S, P, nu_0, a, b, jitter, L, logdet_W, info, T, trace, W_cores}))
     return st;
   return dispatch_float(dtype, [&](auto t0) {
     using TT = decltype(t0);
@@ -734,16 +721,20 @@ extern "C" int lakde_posterior_factor(int dtype, int64_t N, int64_t D, const voi
     g.Tbs = T_batch_stride;
     g.T_lower = T_lower != 0;
     g.trace = static_cast<TT *>(trace);
+    if constexpr (sizeof(TT) == 4) g.Wc = static_cast<float *>(W_cores);
     g.N = N;
     g.D = (int)D;
     return dispatch_dp(D, [&](auto dp) {
       constexpr int DP = decltype(dp)::value;
       if constexpr (DP <= 8) {
         factor_thread_kernel<TT, DP><<<(unsigned)((N + 127) / 128), 128, 0, as_stream(stream)>>>(g);
+        if (int st = check_launch("posterior_factor")) return st;
+        // the register kernel writes W_triu only: its cores by the packing kernel
+        if (W_cores) return lakde_pack_w_cores(LAKDE_F32, N, D, W_triu, W_cores, stream);
+        return (int)LAKDE_OK;
       } else {
         return launch_factor_dmma<TT, DP>(g, N, stream);
       }
-      return check_launch("posterior_factor");
     });
   });
 }
@@ -849,7 +840,7 @@ extern "C" int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D, con
   g.eps = eps;
   g.W = static_cast<float *>(W_triu);
   g.Xt = static_cast<float *>(X_tiles);
-  g.Wc = static_cast<uint32_t *>(W_cores);
+  g.Wc = static_cast<float *>(W_cores);
   g.logdet = static_cast<float *>(logdet_W);
   g.info = info;
   g.T_lower = 1;

@@ -54,8 +54,8 @@ class FusedVI:
         self.c = torch.full((N,), -math.inf, dtype=self.dtype, device=self.device)
         self.rsum = torch.zeros(N, dtype=self.dtype, device=self.device)
         self.logrho = new(pattern.nnz)
-        self.S = new(N, D, D)
-        self.U = new(N, D, D)
+        self._S = None  # dense S and W_triu, allocated by the paths that use them
+        self._U = None
         self.nu = new(N)
         self.logdet_W = new(N)
         self.trace = new(N)
@@ -66,13 +66,28 @@ class FusedVI:
         self.b = self.a.clone()
         self.graph = None
         self.err = torch.zeros(1, dtype=torch.int32, device=self.device)
-        # "mixed": tensor-core (tcgen05, bf16 hi + lo) contractions for 8 < D <= 64;
-        # "fp32": the plain FP32 kernels.  Factorisations are FP64 either way.
+        # "mixed": the E- and M-step contractions on the tensor cores (tcgen05
+        # kind::tf32, hi + lo split of the centred differences and of W_triu,
+        # fp32 accumulation); "fp32": the plain FP32 kernels.  Factorisations are
+        # FP64 either way.  "auto" takes the tensor cores for 8 < D <= 64; at
+        # D <= 8 the one-pass register kernel (fp32) is faster.
         if precision == "auto":
             precision = "mixed" if (8 < D <= 64 and self.dtype == torch.float32) else "fp32"
+        if precision not in ("mixed", "fp32"):
+            raise ValueError(f"unknown precision {precision!r}")
         if precision == "mixed" and not (D <= 64 and self.dtype == torch.float32):
             raise ValueError("precision='mixed' needs float32 data with D <= 64")
         self.precision = precision
+        # tensor-core inputs: rows of X padded to 16 bytes (refreshed from X at
+        # the start of every step, so writes into X are seen), the atomic row
+        # counter of their work queue, W_triu as W cores
+        self.queue = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self.Xp = None
+        self.Wc = None
+        if self.dtype == torch.float32 and D <= 64:
+            self._Xp_separate = not (D % 4 == 0 and X.is_contiguous() and X.data_ptr() % 16 == 0)
+            self.Xp = K.pad_rows(X) if self._Xp_separate else X
+            self.Wc = K.w_cores_like(D, N, self.device)
 
     # ------------------------------------------------------------------ setup
     def _initial_responsibilities(self, init_graph, init_k):
@@ -94,6 +109,23 @@ class FusedVI:
     def _tri(self):
         return self.pattern.rowptr, self.pattern.col
 
+    @property
+    def S(self):
+        if self._S is None:
+            self._S = torch.empty(self.N, self.D, self.D, dtype=self.dtype, device=self.device)
+        return self._S
+
+    @property
+    def U(self):
+        if self._U is None:
+            self._U = torch.empty(self.N, self.D, self.D, dtype=self.dtype, device=self.device)
+        return self._U
+
+    def refresh_points(self):
+        """Copies X into the padded rows the tensor-core kernels read."""
+        if self.precision == "mixed" and self._Xp_separate:
+            self.Xp.copy_(self.X)
+
     # whether the trace factor T of _prior() is lower triangular
     _T_lower = False
 
@@ -106,21 +138,21 @@ class FusedVI:
     # factor as tiles (Tt): set by models whose prior is per kernel
     SP = None
     Tt = None
-    Wc = None  # W_triu as the E-step's bf16 B-operand cores (the tiled factor's output, the tiled E-step's input)
 
     def mstep(self):
         rowptr, col = self._tri()
         if self.precision == "mixed" and self.SP is not None:
-            K.mstep_tc_tiled(rowptr, col, self.r, self.X, self.nu_0, self.err, self.SP, self.nu,
-                             order=self.pattern.order)
+            K.mstep_tc_tiled(rowptr, col, self.r, self.Xp, self.nu_0, self.err, self.SP, self.nu,
+                             order=self.pattern.order, queue=self.queue)
         elif self.precision == "mixed":
-            K.mstep_tc(rowptr, col, self.r, self.X, self.nu_0, self.err, order=self.pattern.order, S=self.S, nu=self.nu,
-                       lower_only=True)
+            K.mstep_tc(rowptr, col, self.r, self.Xp, self.nu_0, self.err, order=self.pattern.order, S=self.S,
+                       nu=self.nu, lower_only=True, queue=self.queue)
         else:
             K.mstep(rowptr, col, self.r, self.X, self.nu_0, S=self.S, nu=self.nu)
 
     def factor(self, with_trace=True):
-        if self.precision == "mixed" and self.SP is not None:
+        mixed = self.precision == "mixed"
+        if mixed and self.SP is not None:
             K.posterior_factor_tiled(self.SP, self.D, self.W_inv_jitter, self.eps, self.nu_0_t, self.a, self.b,
                                      None, self.logdet_W, self.info, T_tiles=self.Tt if with_trace else None,
                                      trace=self.trace if with_trace else None, W_cores=self.Wc)
@@ -130,32 +162,21 @@ class FusedVI:
         K.posterior_factor(
             self.S, self.W_inv_jitter, self.eps, P=P, nu_0=self.nu_0_t, a=self.a, b=self.b,
             T=T if with_trace else None, info=self.info, out=self.U, logdet=self.logdet_W,
-            trace=self.trace if with_trace else None, T_lower=self._T_lower,
+            trace=self.trace if with_trace else None, T_lower=self._T_lower, W_cores=self.Wc if mixed else None,
         )
         torch.minimum(self.failed, self.info.min(), out=self.failed)
 
     def estep_numerators(self):
         """log rho of every pair of the pattern (the E-step before the normaliser)."""
         rowptr, col = self._tri()
-        if self.precision == "mixed" and self.Wc is not None:
-            K.estep_tc_tiled(rowptr, col, self.X, self.Wc, self.nu, self.logdet_W, self.err, order=self.pattern.order,
-                             out=self.logrho)
-        elif self.precision == "mixed":
-            K.estep_tc(rowptr, col, self.X, self.U, self.nu, self.logdet_W, self.err, order=self.pattern.order,
-                       out=self.logrho)
+        if self.precision == "mixed":
+            K.estep_tc(rowptr, col, self.Xp, self.Wc, self.nu, self.logdet_W, self.err, order=self.pattern.order,
+                       out=self.logrho, queue=self.queue)
         else:
             K.estep_logrho(rowptr, col, self.X, self.U, self.nu, self.logdet_W, out=self.logrho)
 
     def estep(self, mode):
-        rowptr, col = self._tri()
-        if self.precision == "mixed" and self.Wc is not None:
-            K.estep_tc_tiled(rowptr, col, self.X, self.Wc, self.nu, self.logdet_W, self.err, order=self.pattern.order,
-                             out=self.logrho)
-        elif self.precision == "mixed":
-            K.estep_tc(rowptr, col, self.X, self.U, self.nu, self.logdet_W, self.err, order=self.pattern.order,
-                       out=self.logrho)
-        else:
-            K.estep_logrho(rowptr, col, self.X, self.U, self.nu, self.logdet_W, out=self.logrho)
+        self.estep_numerators()
         K.estep_normalise(self.pattern.cptr, self.pattern.pos, self.logrho, self.r, self.c, self.rsum, mode,
                           self.threshold)
 
@@ -179,23 +200,38 @@ class FusedVI:
     # ------------------------------------------------------------ prediction
     def log_pred_density(self, Y):
         """lakde/local_adaptive_kde.py:200-223: posterior from the current r, then
-        the fused Student-t mixture kernel."""
-        S = torch.empty_like(self.S)
+        the fused Student-t mixture kernel.  The mixed path recomputes S and the
+        factorisation into the buffers the next iteration overwrites first (the
+        S halves of SP, or S, and the W cores), so it allocates no per-kernel
+        matrices; nu and logdet_W of the model are left as they are."""
         nu = torch.empty_like(self.nu)
+        logdet = torch.empty_like(self.logdet_W)
+        info = torch.empty_like(self.info)
         rowptr, col = self._tri()
         if self.precision == "mixed":
-            K.mstep_tc(rowptr, col, self.r, self.X, self.nu_0, self.err, order=self.pattern.order, S=S, nu=nu,
-                       lower_only=True)
-        else:
-            K.mstep(rowptr, col, self.r, self.X, self.nu_0, S=S, nu=nu)
+            self.refresh_points()
+            if self.SP is not None:
+                K.mstep_tc_tiled(rowptr, col, self.r, self.Xp, self.nu_0, self.err, self.SP, nu,
+                                 order=self.pattern.order, queue=self.queue)
+                K.posterior_factor_tiled(self.SP, self.D, self.W_inv_jitter, self.eps, self.nu_0_t, self.a, self.b,
+                                         None, logdet, info, W_cores=self.Wc)
+            else:
+                K.mstep_tc(rowptr, col, self.r, self.Xp, self.nu_0, self.err, order=self.pattern.order, S=self.S,
+                           nu=nu, lower_only=True, queue=self.queue)
+                P, _ = self._prior()
+                K.posterior_factor(self.S, self.W_inv_jitter, self.eps, P=P, nu_0=self.nu_0_t, a=self.a, b=self.b,
+                                   info=info, out=self.U, logdet=logdet, W_cores=self.Wc)
+            torch.minimum(self.failed, info.min(), out=self.failed)
+            lc = K.pred_coeff(nu, logdet, self.D)
+            return K.log_pred_density_tc(self.Xp, self.Wc, nu, lc, Y.to(self.dtype), self.err)
+        S = torch.empty_like(self.S)
+        K.mstep(rowptr, col, self.r, self.X, self.nu_0, S=S, nu=nu)
         P, _ = self._prior()
         W, logdet, info, _, _ = K.posterior_factor(S, self.W_inv_jitter, self.eps, P=P, nu_0=self.nu_0_t, a=self.a,
-                                                   b=self.b)
+                                                   b=self.b, logdet=logdet, info=info)
         del S
         torch.minimum(self.failed, info.min(), out=self.failed)
         lc = K.pred_coeff(nu, logdet, self.D)
-        if self.precision == "mixed":
-            return K.log_pred_density_tc(self.X, W, nu, lc, Y.to(self.dtype), self.err)
         return K.log_pred_density(self.X, W, nu, lc, Y.to(self.dtype))
 
     def posterior_factors(self):
@@ -258,7 +294,6 @@ class FusedKNN(FusedVI):
             nt = K.tile_count(self.D)
             self.SP = torch.zeros(self.N, nt * 128, dtype=self.dtype, device=self.device)
             self.Tt = torch.zeros(self.N, nt * 64, dtype=self.dtype, device=self.device)
-            self.Wc = torch.zeros(self.N, nt * 128, dtype=torch.bfloat16, device=self.device)
             K.pack_tiles(sigma_0, self.SP, 128, 64)
             K.pack_tiles(L0, self.Tt, 64, 0)
 
@@ -270,6 +305,7 @@ class FusedKNN(FusedVI):
     def init_summaries(self):
         """lakde/local_knn_kde.py:140-193 at block_size = N."""
         self.init_prior()
+        self.refresh_points()
         self.mstep()
         self.factor()
         torch.mul(self.nu, self.trace, out=self.sigma_0_lambda_mm_trace)
@@ -277,7 +313,7 @@ class FusedKNN(FusedVI):
 
     def step(self):
         """lakde/local_knn_kde.py:209-254 at block_size = N."""
-        if self.D <= 8:
+        if self.D <= 8 and self.precision == "fp32":
             # M-step, factorisation, summaries, b update and log rho in one pass
             p = self.pattern
             K.vi_rows(p.rowptr, p.col, self.r, self.X, self.nu_0, self.a, self.b, self.b_0_f, self.W_inv_jitter,
@@ -286,6 +322,7 @@ class FusedKNN(FusedVI):
             torch.minimum(self.failed, self.info.min(), out=self.failed)
             K.estep_normalise(p.cptr, p.pos, self.logrho, self.r, self.c, self.rsum, 1, self.threshold)
             return
+        self.refresh_points()
         self.mstep()
         self.factor()
         self.estep(mode=1)
@@ -345,6 +382,7 @@ class FusedHier(FusedVI):
 
     def init_summaries(self):
         """lakde/local_hierarchical_kde.py:198-258 at block_size = N."""
+        self.refresh_points()
         self.mstep()
         self.factor(with_trace=False)
         e_tau = self.a / self.b
@@ -353,6 +391,7 @@ class FusedHier(FusedVI):
 
     def step(self):
         """lakde/local_hierarchical_kde.py:273-332 at block_size = N."""
+        self.refresh_points()
         self.mstep()
         self.factor()
         self.estep(mode=1)

@@ -177,13 +177,15 @@ def mstep(rowptr, col, r, X, nu_0, kernel_offset=0, S=None, nu=None):
 
 
 def posterior_factor(S, jitter, eps, P=None, nu_0=None, a=None, b=None, T=None, want_L=False, info=None, out=None,
-                     logdet=None, trace=None, L=None, T_lower=False):
+                     logdet=None, trace=None, L=None, T_lower=False, W_cores=None):
     """FP64 jittered Cholesky of A_n = nu_0 a_n / b_n P_n + S_n (see include/lakde_b200.h).
 
     Returns (W_triu, logdet_W, info, L or None, trace or None); ``jitter`` is
     updated in place.  ``P`` and ``T`` may be [D, D] (shared) or [N, D, D].
     Output buffers may be passed in (out, logdet, info, trace, L).
     ``T_lower=True`` declares T lower triangular (its upper part is not read).
+    ``W_cores`` (float32, from ``w_cores_like``) also receives W_triu as the
+    tensor-core kernels' W cores.
     """
     nat.require_cuda(S, jitter, P, nu_0, a, b, T, op="posterior_factor")
     N, D, _ = S.shape
@@ -215,7 +217,7 @@ def posterior_factor(S, jitter, eps, P=None, nu_0=None, a=None, b=None, T=None, 
         nat.lib().lakde_posterior_factor(
             nat.dtype_code(S), N, D, nat.ptr(S), nat.ptr(P), pbs, nat.ptr(nu_0), nat.ptr(a), nat.ptr(b),
             nat.ptr(jitter), float(eps), nat.ptr(W), nat.ptr(L), nat.ptr(logdet), nat.ptr(info), nat.ptr(T), tbs,
-            int(bool(T_lower)), nat.ptr(trace), nat.stream_of(S),
+            int(bool(T_lower)), nat.ptr(trace), nat.ptr(W_cores), nat.stream_of(S),
         ),
         "posterior_factor",
     )
@@ -241,12 +243,11 @@ def estep_logrho(rowptr, col, X, W_triu, nu, logdet_W, kernel_offset=0, out=None
 
 def vi_rows(rowptr, col, r, X, nu_0, a, b, b_0, jitter, eps, nu, logdet_W, info, logrho, P=None, T=None,
             order=None, mm=None, kernel_offset=0):
-    """Fused per-kernel pass of one VI iteration (see include/lakde_b200.h):
-    one thread per row for D <= 8 (lakde_vi_rows), one CTA per row for
-    8 < D <= 64 (lakde_vi_cta, float32).  Row n is the kernel centred on
-    X[n + kernel_offset] (a shard's rows)."""
+    """Fused per-kernel pass of one VI iteration, one thread per kernel row,
+    D <= 8 (lakde_vi_rows, see include/lakde_b200.h).  Row n is the kernel
+    centred on X[n + kernel_offset] (a shard's rows)."""
     nat.require_cuda(rowptr, col, r, X, a, b, jitter, nu, logdet_W, info, logrho, P, T, order, mm, op="vi_rows")
-    entry = nat.lib().lakde_vi_rows if X.size(1) <= 8 else nat.lib().lakde_vi_cta
+    entry = nat.lib().lakde_vi_rows
     N = rowptr.numel() - 1
     D = X.size(1)
     assert rowptr.dtype == torch.int64 and col.dtype == torch.int32
@@ -350,36 +351,71 @@ def pack_tiles(src, dst, dst_tile_stride, dst_offset):
     return dst
 
 
-def mstep_tc_tiled(rowptr, col, r, X, nu_0, err, SP, nu, order=None, kernel_offset=0):
+def rows16(X):
+    """(tensor, row stride) with 16-byte aligned rows for the tensor-core kernels:
+    X itself when its rows already are (contiguous columns, a row stride that is
+    a multiple of 4 floats, an aligned base), else a zero-padded copy."""
+    D = X.size(1)
+    if (X.stride(1) == 1 and X.stride(0) % 4 == 0 and X.stride(0) >= ((D + 3) // 4) * 4
+            and X.data_ptr() % 16 == 0):
+        return X, X.stride(0)
+    Xp = pad_rows(X)
+    return Xp, Xp.stride(0)
+
+
+def pad_rows(X, out=None):
+    """X [n, D] copied into the first D columns of a zero-padded [n, D rounded up
+    to 4] buffer (returned as that view); ``out`` reuses such a buffer."""
+    n, D = X.shape
+    if out is None:
+        out = X.new_zeros(n, ((D + 3) // 4) * 4)[:, :D]
+    out.copy_(X)
+    return out
+
+
+def w_cores_like(D, N, device):
+    """Buffer for the W cores of N kernels (float32; layout at lakde_pack_w_cores)."""
+    return torch.empty(N, int(nat.lib().lakde_w_cores_floats(int(D))), dtype=torch.float32, device=device)
+
+
+def pack_w_cores(W_triu, out=None):
+    """W cores of W_triu [N, D, D] (dense upper triangles, float32)."""
+    nat.require_cuda(W_triu, out, op="pack_w_cores")
+    N, D, _ = W_triu.shape
+    W_triu = W_triu.contiguous()
+    out = w_cores_like(D, N, W_triu.device) if out is None else out
+    nat.check(nat.lib().lakde_pack_w_cores(nat.dtype_code(W_triu), N, D, nat.ptr(W_triu), nat.ptr(out),
+                                           nat.stream_of(W_triu)), "pack_w_cores")
+    return out
+
+
+def mstep_tc_tiled(rowptr, col, r, X, nu_0, err, SP, nu, order=None, kernel_offset=0, queue=None):
     """Tensor-core M-step writing S_n as tiles into the S halves of SP (see include/lakde_b200.h)."""
-    nat.require_cuda(rowptr, col, r, X, err, SP, nu, order, op="mstep_tc_tiled")
+    nat.require_cuda(rowptr, col, r, X, err, SP, nu, order, queue, op="mstep_tc_tiled")
     assert rowptr.dtype == torch.int64 and col.dtype == torch.int32 and err.dtype == torch.int32
     N = rowptr.numel() - 1
+    Xr, ldx = rows16(X)
     nat.check(
         nat.lib().lakde_mstep_tc_tiled(
             nat.dtype_code(X), N, X.size(1), X.size(0), nat.ptr(rowptr), nat.ptr(col), nat.ptr(order), nat.ptr(r),
-            nat.ptr(X), int(kernel_offset), float(nu_0), nat.ptr(SP), nat.ptr(nu), nat.ptr(err), nat.stream_of(X),
+            nat.ptr(Xr), ldx, int(kernel_offset), float(nu_0), nat.ptr(SP), nat.ptr(nu), nat.ptr(queue),
+            nat.ptr(err), nat.stream_of(X),
         ),
         "mstep_tc_tiled",
     )
 
 
-def w_cores_like(D, N, device):
-    """Buffer for the W cores of N kernels (bf16 hi / lo B-operand cores; see include/lakde_b200.h)."""
-    return torch.empty(N, tile_count(D) * 128, dtype=torch.bfloat16, device=device)
-
-
 def posterior_factor_tiled(SP, D, jitter, eps, nu_0, a, b, out, logdet, info, T_tiles=None, trace=None,
                            X_tiles=None, W_cores=None):
     """posterior_factor from the tiled SP (and T) layout (see include/lakde_b200.h); writes W_triu to
-    ``out``, X = W_triu^T as tiles to ``X_tiles`` and / or the E-step's W cores to ``W_cores``
+    ``out``, X = W_triu^T as tiles to ``X_tiles`` and / or the W cores to ``W_cores``
     (any two may be None)."""
     nat.require_cuda(SP, jitter, nu_0, a, b, out, X_tiles, W_cores, logdet, info, T_tiles, trace,
                      op="posterior_factor_tiled")
     N = jitter.numel()
     if W_cores is not None:
-        assert W_cores.dtype == torch.bfloat16 and W_cores.is_contiguous()
-        assert W_cores.numel() == N * tile_count(D) * 128
+        assert W_cores.dtype == torch.float32 and W_cores.is_contiguous()
+        assert W_cores.numel() == N * int(nat.lib().lakde_w_cores_floats(int(D)))
     nat.check(
         nat.lib().lakde_posterior_factor_tiled(
             nat.dtype_code(SP), N, int(D), nat.ptr(SP), nat.ptr(nu_0), nat.ptr(a), nat.ptr(b), nat.ptr(jitter),
@@ -388,24 +424,6 @@ def posterior_factor_tiled(SP, D, jitter, eps, nu_0, a, b, out, logdet, info, T_
         ),
         "posterior_factor_tiled",
     )
-
-
-def estep_tc_tiled(rowptr, col, X, W_cores, nu, logdet_W, err, order=None, out=None, kernel_offset=0):
-    """Tensor-core E-step numerators with W_triu given as W cores (see include/lakde_b200.h)."""
-    nat.require_cuda(rowptr, col, X, W_cores, nu, logdet_W, err, order, op="estep_tc_tiled")
-    assert rowptr.dtype == torch.int64 and col.dtype == torch.int32 and err.dtype == torch.int32
-    assert W_cores.dtype == torch.bfloat16 and W_cores.is_contiguous()
-    N = rowptr.numel() - 1
-    out = X.new_empty(col.numel()) if out is None else out
-    nat.check(
-        nat.lib().lakde_estep_tc_tiled(
-            nat.dtype_code(X), N, X.size(1), X.size(0), nat.ptr(rowptr), nat.ptr(col), nat.ptr(order), nat.ptr(X),
-            int(kernel_offset), nat.ptr(W_cores), nat.ptr(nu), nat.ptr(logdet_W), nat.ptr(out), nat.ptr(err),
-            nat.stream_of(X),
-        ),
-        "estep_tc_tiled",
-    )
-    return out
 
 
 def knn_elbo(a, b, nu, logdet_W, logdet_sigma_0, mm, c, a_0, b_0, nu_0, D, out=None, workspace=None):
@@ -453,23 +471,24 @@ def knn_elbo_parts(D, a_0, b_0, nu_0, a=None, b=None, nu=None, logdet_W=None, lo
     return out
 
 
-def log_pred_density_tc(X, W_triu, nu, log_coeff, Y, err, out=None, workspace=None):
-    """log_pred_density with the quad forms on the tensor cores (bf16 hi + lo),
-    float32, D <= 64 (see include/lakde_b200.h)."""
-    nat.require_cuda(X, W_triu, nu, log_coeff, Y, err, op="log_pred_density_tc")
+def log_pred_density_tc(X, W_cores, nu, log_coeff, Y, err, out=None, workspace=None):
+    """log_pred_density with the quad forms on the tensor cores (tf32 hi / lo),
+    float32, D <= 64, W_triu given as W cores (see include/lakde_b200.h)."""
+    nat.require_cuda(X, W_cores, nu, log_coeff, Y, err, op="log_pred_density_tc")
     N, D = X.shape
-    Y = Y.contiguous()
     Nq = Y.size(0)
     out = Y.new_empty(Nq) if out is None else out
     if Nq == 0:
         return out
+    Xr, ldx = rows16(X)
+    Yr, ldy = rows16(Y.to(X.dtype))
     need = nat.lib().lakde_log_pred_density_tc_workspace(N, Nq, D)
     if workspace is None or workspace.numel() < need:
         workspace = torch.empty(need, dtype=torch.uint8, device=X.device)
     nat.check(
         nat.lib().lakde_log_pred_density_tc(
-            nat.dtype_code(X), N, Nq, D, nat.ptr(X), nat.ptr(W_triu), nat.ptr(nu), nat.ptr(log_coeff),
-            nat.ptr(Y), nat.ptr(out), nat.ptr(workspace), workspace.numel(), nat.ptr(err), nat.stream_of(X),
+            nat.dtype_code(X), N, Nq, D, nat.ptr(Xr), ldx, nat.ptr(W_cores), nat.ptr(nu), nat.ptr(log_coeff),
+            nat.ptr(Yr), ldy, nat.ptr(out), nat.ptr(workspace), workspace.numel(), nat.ptr(err), nat.stream_of(X),
         ),
         "log_pred_density_tc",
     )
@@ -504,40 +523,44 @@ def log_pred_density_bwd(X, W_triu, nu, log_coeff, Y, out, grad_out):
     return gY, sw, S_c
 
 
-def estep_tc(rowptr, col, X, W_triu, nu, logdet_W, err, order=None, out=None, kernel_offset=0):
-    """Tensor-core (bf16 hi + lo) E-step numerators, D <= 64 (see include/lakde_b200.h).
-    Row n of rowptr is kernel n + kernel_offset of X."""
-    nat.require_cuda(rowptr, col, X, W_triu, nu, logdet_W, err, order, op="estep_tc")
+def estep_tc(rowptr, col, X, W_cores, nu, logdet_W, err, order=None, out=None, kernel_offset=0, queue=None):
+    """Tensor-core (tf32 hi / lo) E-step numerators, D <= 64, W_triu given as W
+    cores (see include/lakde_b200.h).  Row n of rowptr is kernel n + kernel_offset of X."""
+    nat.require_cuda(rowptr, col, X, W_cores, nu, logdet_W, err, order, queue, op="estep_tc")
     assert rowptr.dtype == torch.int64 and col.dtype == torch.int32 and err.dtype == torch.int32
+    assert W_cores.dtype == torch.float32 and W_cores.is_contiguous()
     N = rowptr.numel() - 1
     out = X.new_empty(col.numel()) if out is None else out
+    Xr, ldx = rows16(X)
     nat.check(
         nat.lib().lakde_estep_tc(
-            nat.dtype_code(X), N, X.size(1), X.size(0), nat.ptr(rowptr), nat.ptr(col), nat.ptr(order), nat.ptr(X),
-            int(kernel_offset), nat.ptr(W_triu), nat.ptr(nu), nat.ptr(logdet_W), nat.ptr(out), nat.ptr(err),
-            nat.stream_of(X),
+            nat.dtype_code(X), N, X.size(1), X.size(0), nat.ptr(rowptr), nat.ptr(col), nat.ptr(order), nat.ptr(Xr),
+            ldx, int(kernel_offset), nat.ptr(W_cores), nat.ptr(nu), nat.ptr(logdet_W), nat.ptr(out),
+            nat.ptr(queue), nat.ptr(err), nat.stream_of(X),
         ),
         "estep_tc",
     )
     return out
 
 
-def mstep_tc(rowptr, col, r, X, nu_0, err, order=None, S=None, nu=None, lower_only=False, kernel_offset=0):
-    """Tensor-core (bf16 hi + lo) M-step S and nu, D <= 64 (see include/lakde_b200.h).
+def mstep_tc(rowptr, col, r, X, nu_0, err, order=None, S=None, nu=None, lower_only=False, kernel_offset=0,
+             queue=None):
+    """Tensor-core (tf32 hi / lo) M-step S and nu, D <= 64 (see include/lakde_b200.h).
 
     ``lower_only=True`` writes only the lower triangle of each S_n; row n of
     rowptr is kernel n + kernel_offset of X."""
-    nat.require_cuda(rowptr, col, r, X, err, order, op="mstep_tc")
+    nat.require_cuda(rowptr, col, r, X, err, order, queue, op="mstep_tc")
     assert rowptr.dtype == torch.int64 and col.dtype == torch.int32 and err.dtype == torch.int32
     N = rowptr.numel() - 1
     D = X.size(1)
     S = X.new_empty(N, D, D) if S is None else S
     nu = X.new_empty(N) if nu is None else nu
+    Xr, ldx = rows16(X)
     nat.check(
         nat.lib().lakde_mstep_tc(
             nat.dtype_code(X), N, D, X.size(0), nat.ptr(rowptr), nat.ptr(col), nat.ptr(order), nat.ptr(r),
-            nat.ptr(X), int(kernel_offset), float(nu_0), nat.ptr(S), nat.ptr(nu), int(bool(lower_only)), nat.ptr(err),
-            nat.stream_of(X),
+            nat.ptr(Xr), ldx, int(kernel_offset), float(nu_0), nat.ptr(S), nat.ptr(nu), int(bool(lower_only)),
+            nat.ptr(queue), nat.ptr(err), nat.stream_of(X),
         ),
         "mstep_tc",
     )

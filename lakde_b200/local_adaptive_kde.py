@@ -20,7 +20,7 @@ from abc import ABC, abstractmethod
 import torch
 
 from . import kernels as K
-from .kdes import AbstractKDE
+from .kdes import VIModel
 from .linalg_util import chol_logdet, lgamma, logsubexp, mvdigamma, xlogx
 from .sparse_util import cat_sparse
 
@@ -45,7 +45,7 @@ def calc_log_rho_block(X_test, X_train, nu, W_triu, logdet_W):
     return Q
 
 
-class LocallyAdaptiveKDE(AbstractKDE, ABC):
+class LocallyAdaptiveKDE(VIModel, ABC):
     def __init__(self, nu_0, a_0, b_0, block_size, verbose, logs, fused=False, candidates="knn", cuda_graph=True):
         super().__init__(block_size, verbose, logs)
         self.nu_0 = nu_0

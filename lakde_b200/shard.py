@@ -99,6 +99,19 @@ class CudaShardOps:
         from . import kernels
 
         self.K = kernels
+        self._Xp = None
+
+    def _rows(self, X):
+        """X with 16-byte aligned rows for the tensor-core kernels: X itself, or a
+        padded copy refreshed from X on every call."""
+        D = X.size(1)
+        if D % 4 == 0 and X.is_contiguous() and X.data_ptr() % 16 == 0:
+            return X
+        if self._Xp is None or self._Xp.shape != X.shape or self._Xp.device != X.device:
+            self._Xp = self.K.pad_rows(X)
+        else:
+            self._Xp.copy_(X)
+        return self._Xp
 
     def prior(self, X, graph_rows, lo, jitter, eps):
         """Sigma0 of kernels lo.. (with jitter), its factor, log det and the
@@ -111,20 +124,22 @@ class CudaShardOps:
         sigma_0.diagonal(dim1=-2, dim2=-1).add_(jitter[:, None])
         return sigma_0, L0, -logdet_inv, info.min()
 
-    def mstep(self, pat, r, X, lo, nu_0, S, nu, precision, err):
+    def mstep(self, pat, r, X, lo, nu_0, S, nu, precision, err, queue=None):
         if precision == "mixed":
-            self.K.mstep_tc(pat.rowptr, pat.col, r, X, nu_0, err, order=pat.order, S=S, nu=nu, lower_only=True,
-                            kernel_offset=lo)
+            self.K.mstep_tc(pat.rowptr, pat.col, r, self._rows(X), nu_0, err, order=pat.order, S=S, nu=nu,
+                            lower_only=True, kernel_offset=lo, queue=queue)
         else:
             self.K.mstep(pat.rowptr, pat.col, r, X, nu_0, kernel_offset=lo, S=S, nu=nu)
 
-    def factor(self, S, jitter, eps, P, nu_0, a, b, T, U, logdet, trace, info):
+    def factor(self, S, jitter, eps, P, nu_0, a, b, T, U, logdet, trace, info, W_cores=None):
         self.K.posterior_factor(S, jitter, eps, P=P, nu_0=nu_0, a=a, b=b, T=T, info=info, out=U, logdet=logdet,
-                                trace=trace, T_lower=True)
+                                trace=trace, T_lower=True, W_cores=W_cores)
 
-    def estep(self, pat, X, lo, U, nu, logdet, out, precision, err):
+    def estep(self, pat, X, lo, U, nu, logdet, out, precision, err, W_cores=None, queue=None):
         if precision == "mixed":
-            self.K.estep_tc(pat.rowptr, pat.col, X, U, nu, logdet, err, order=pat.order, out=out, kernel_offset=lo)
+            Wc = W_cores if W_cores is not None else self.K.pack_w_cores(U)
+            self.K.estep_tc(pat.rowptr, pat.col, self._rows(X), Wc, nu, logdet, err, order=pat.order, out=out,
+                            kernel_offset=lo, queue=queue)
         else:
             self.K.estep_logrho(pat.rowptr, pat.col, X, U, nu, logdet, kernel_offset=lo, out=out)
 
@@ -152,7 +167,7 @@ class CudaShardOps:
         """-log n + logsumexp over these n kernels, per query."""
         lc = self.K.pred_coeff(nu, logdet, Xk.size(1))
         if precision == "mixed":
-            return self.K.log_pred_density_tc(Xk, U, nu, lc, Y, err)
+            return self.K.log_pred_density_tc(Xk, self.K.pack_w_cores(U), nu, lc, Y, err)
         return self.K.log_pred_density(Xk, U, nu, lc, Y)
 
 
@@ -201,6 +216,13 @@ class ShardedKNN:
         self.b = self.a.clone()
         self.mm = new(n)
         self.err = torch.zeros(1, dtype=torch.int32, device=self.device)
+        # tensor-core path: W_triu of the shard's kernels as W cores, the work-queue counter
+        self.Wc = self.queue = None
+        if precision == "mixed":
+            from . import kernels
+
+            self.Wc = kernels.w_cores_like(D, max(n, 1), self.device)[:n]
+            self.queue = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.failed = torch.zeros((), dtype=torch.int32, device=self.device)
 
     def _initial_responsibilities(self, knn_graph, init_k):
@@ -224,18 +246,27 @@ class ShardedKNN:
 
     # ------------------------------------------------------------- iteration
     def _mstep(self):
-        self.ops.mstep(self.pat, self.r, self.X, self.lo, self.nu_0, self.S, self.nu, self.precision, self.err)
+        self.ops.mstep(self.pat, self.r, self.X, self.lo, self.nu_0, self.S, self.nu, self.precision, self.err,
+                       **self._tc_kw())
 
     def _factor(self):
         self.ops.factor(self.S, self.W_inv_jitter, self.eps, self.sigma_0, self.nu_0_t, self.a, self.b,
-                        self.sigma_0_tril, self.U, self.logdet_W, self.trace, self.info)
+                        self.sigma_0_tril, self.U, self.logdet_W, self.trace, self.info,
+                        **({"W_cores": self.Wc} if self.Wc is not None else {}))
         if self.n:
             torch.minimum(self.failed, self.info.min(), out=self.failed)
 
     def _estep(self, mode):
         self.ops.estep(self.pat, self.X, self.lo, self.U, self.nu, self.logdet_W, self.logrho, self.precision,
-                       self.err)
+                       self.err, **self._tc_kw(W_cores=self.Wc))
         self._normalise(mode)
+
+    def _tc_kw(self, **kw):
+        """Extra arguments of the tensor-core path (none for the plain kernels)."""
+        if self.precision != "mixed":
+            return {}
+        kw["queue"] = self.queue
+        return kw
 
     def _normalise(self, mode):
         """The per-point pass, reduced over the ranks between its stages."""

@@ -5,7 +5,8 @@ LAKDE_NO_EXT=1) on small seeded inputs and stores inputs and outputs as
 .npz files next to this script.  Only this script reads the reference
 checkout; the tests read the .npz files.
 
-    python tests/golden/make_golden.py [path/to/lakde checkout]
+    python tests/golden/make_golden.py path/to/lakde-checkout
+    LAKDE_REFERENCE=path/to/lakde-checkout python tests/golden/make_golden.py
 """
 
 import os
@@ -14,7 +15,9 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LAKDE_REFERENCE")
+if not REF or not os.path.isdir(os.path.join(REF, "lakde")):
+    sys.exit("usage: make_golden.py path/to/lakde-checkout (or set LAKDE_REFERENCE)")
 os.environ["LAKDE_NO_EXT"] = "1"
 sys.path.insert(0, REF)
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))

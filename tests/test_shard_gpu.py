@@ -62,13 +62,14 @@ def test_tc_kernels_honour_the_kernel_offset(D):
     logdet = O.chol_logdet(W).astype(np.float32)
     err = torch.zeros(1, dtype=torch.int32, device=DEV)
     S, nuo = K.mstep_tc(t(rowptr), t(cols, torch.int32), t(r), t(X), D + 1.0, err)
-    lr = K.estep_tc(t(rowptr), t(cols, torch.int32), t(X), t(W), t(nu), t(logdet), err)
+    Wc = K.pack_w_cores(t(W))
+    lr = K.estep_tc(t(rowptr), t(cols, torch.int32), t(X), Wc, t(nu), t(logdet), err)
     lo, hi = 123, 301
     p0, p1 = rowptr[lo], rowptr[hi]
     rp = rowptr[lo : hi + 1] - p0
     S2, nu2 = K.mstep_tc(t(rp), t(cols[p0:p1], torch.int32), t(r[p0:p1]), t(X), D + 1.0, err, kernel_offset=lo)
-    lr2 = K.estep_tc(t(rp), t(cols[p0:p1], torch.int32), t(X), t(W[lo:hi]), t(nu[lo:hi]), t(logdet[lo:hi]), err,
-                     kernel_offset=lo)
+    lr2 = K.estep_tc(t(rp), t(cols[p0:p1], torch.int32), t(X), Wc[lo:hi].contiguous(), t(nu[lo:hi]),
+                     t(logdet[lo:hi]), err, kernel_offset=lo)
     assert int(err) == 0
     torch.testing.assert_close(S2, S[lo:hi], rtol=0, atol=0)
     torch.testing.assert_close(nu2, nuo[lo:hi], rtol=0, atol=0)
@@ -78,10 +79,10 @@ def test_tc_kernels_honour_the_kernel_offset(D):
     assert torch.isneginf(lr2[t(self_pair)]).all()
 
 
-@pytest.mark.parametrize("D", [5, 13])
+@pytest.mark.parametrize("D", [3, 5, 8])
 def test_fused_row_kernels_honour_the_kernel_offset(D):
-    """lakde_vi_rows (D <= 8) and lakde_vi_cta on a shard's rows (kernel_offset)
-    give the rows of the full launch bit for bit."""
+    """lakde_vi_rows (D <= 8) on a shard's rows (kernel_offset) gives the rows
+    of the full launch bit for bit."""
     from lakde_b200 import kernels as K
 
     rng = np.random.default_rng(D + 1)
