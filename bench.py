@@ -1,15 +1,20 @@
 """Benchmark of the lakde VI hot path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload gas8|bsds63|...]
-                    [--impl reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload bsds63|gas8|...]
+                    [--impl reference] [--no-fp64-check] [--no-cpu-baseline]
 
 A step is one VI iteration of LocalKNearestKDE over all N kernels (fused
 batch schedule on the kNN candidate pattern), on seeded synthetic data with
-the shape of the named workload.  Inputs are resident in HBM; L2 is flushed
-between timed steps.  Rank 0 prints one JSON line with the whole-job
-throughput, the roofline of the dominant kernel, the end-to-end number
-through the public API with host buffers, the CPU baseline (the oracle port
-timed on a bounded sample) and the SM clocks sampled during the timed region.
+the shape of the named workload; the default is the d=63, N=1,000,000, K=100
+decaying-spectrum mixture in mixed precision (tensor-core tf32 hi / lo
+contractions, FP64 factorisations).  Inputs are resident in HBM; L2 is
+flushed between timed steps.  Rank 0 prints one JSON line with the whole-job
+throughput, the roofline of the dominant kernel, the plain-FP32 arm timed
+from the same state, the held-out log density of mixed precision, plain FP32
+and FP64 after the same iterations from the same initialisation, the
+end-to-end number through the public API with host buffers, the CPU baseline
+(the same sparse schedule restated in numpy, timed on a bounded sample on all
+host cores) and the SM clocks sampled during the timed region.
 Under torchrun (N > 1), or with --sharded, the kernels are sharded over the
 ranks (lakde_b200.shard: one VI iteration of the whole data set per step, the
 per-point normaliser all-reduced over NCCL), so N GPUs share one problem
@@ -39,7 +44,7 @@ WORKLOADS = {
              "LocalKNearestKDE d=8 N_train=200000 N_test=20000 K=50 (10-component heavy-tail mixture)"),
     "bsds63": (dict(n_train=1_000_000, n_test=16_384), 100, 5e-4,
                "LocalKNearestKDE d=63 N_train=1000000 N_test=16384 K=100 (20-component decaying-spectrum mixture)"),
-    "bsds63s": (dict(n_train=50_000, n_test=1_024), 100, 5e-4,
+    "bsds63s": (dict(n_train=50_000, n_test=2_048), 100, 5e-4,
                 "LocalKNearestKDE d=63 N_train=50000 N_test=1024 K=100 (the bsds63 mixture, small case for "
                 "profiling)"),
     "spec21": (dict(n_train=300_000, n_test=4_096), 64, 5e-4,
@@ -186,7 +191,7 @@ def kernel_split(eng, reps, flush, torch):
 
     stream = torch.cuda.current_stream()
     p = eng.pattern
-    if eng.D <= 8:
+    if eng.D <= 8 and eng.precision == "fp32":
         launches = {
             "vi_rows": lambda: K.vi_rows(p.rowptr, p.col, eng.r, eng.X, eng.nu_0, eng.a, eng.b, eng.b_0_f,
                                          eng.W_inv_jitter, eng.eps, eng.nu, eng.logdet_W, eng.info, eng.logrho,
@@ -212,72 +217,144 @@ def kernel_split(eng, reps, flush, torch):
     return {k: v / reps for k, v in out.items()}
 
 
-def cpu_baseline(Xtr, graph, k, thr, budget_s=20.0):
-    """The reference algorithm (oracle port, numpy) timed on a bounded sample of
-    one VI iteration of its block schedule (blocks of 512 kernels, dense E-step
-    against every point): the posterior of one kernel block, then as many of
-    its point blocks of the dense E-step as fit the time budget; extrapolated
-    to all point blocks and all kernel blocks."""
+def _cpu_rows(job):
+    """One chunk of kernel rows of a VI iteration on the kNN pattern, in the
+    oracle's numpy restatement of the reference arithmetic: M-step (scatter
+    covariance and nu), jittered FP64 Cholesky, triangular inverse, log det and
+    trace, then the E-step numerators of the rows' pairs.  Returns the seconds
+    it took (run in a spawned worker process)."""
+    import time as _time
+
     from oracle import lakde_oracle as O
 
-    N, D = Xtr.shape
-    B = 512
-    m = O.KNNKDEOracle(k=graph.astype(np.int64), block_size=B)
-    m.init_parameters_(Xtr, thr)
-    m.rnm_log_consts[:] = 0.0
-    t0 = time.perf_counter()
-    S, nu = m._posterior_contribs(Xtr, 0)
-    sigma_0, _ = m.prior_cov(Xtr, 0)
-    W = m._posterior(0, N, sigma_0, S)
-    t_post = time.perf_counter() - t0
+    Xs, rowptr, col, r, self_idx, sigma0, L0, nu0, scale = job
+    t0 = _time.perf_counter()
+    Xn = Xs[self_idx]
+    S = O.calc_W_inv(rowptr, col, r, Xn, Xs)
+    nu = nu0 + np.add.reduceat(r, rowptr[:-1]) if len(r) else np.full(len(self_idx), nu0)
+    A = (sigma0 * scale[:, None, None] + S).astype(np.float64)
+    L, _ = O.stabilized_cholesky(A, eps=float(np.finfo(np.float32).eps))
+    W = np.swapaxes(O.tril_inverse(L), -1, -2)
     logdet = O.chol_logdet(W)
-    n_pb = (N - 1) // B + 1
-    done = 0
-    t1 = time.perf_counter()
-    while done < n_pb and (done < 1 or time.perf_counter() - t1 < budget_s):
-        js = done * B
-        lr = O.calc_log_rho_block(Xtr[js:js + B], Xtr[:B], nu, W, logdet)
-        c = O.logsumexp0(lr)
-        r = np.exp(lr - c[None, :])
-        if thr:
-            r = np.where(r > thr, r, 0)
-        np.nonzero(r)
-        done += 1
-    t_block = (time.perf_counter() - t1) / done
-    per_step = t_post + n_pb * t_block
-    n_kb = (N - 1) // B + 1
+    O.chol_mm_trace(L0.astype(np.float64), W)
+    rows = O._rows_of(rowptr)
+    delta = Xs[col] - Xn[rows]
+    y = np.einsum("pji,pj->pi", np.triu(W)[rows], delta, optimize=True)
+    Q = (y * y).sum(-1)
+    _ = Q * (-0.5 * nu[rows]) + O.log_rho_const(nu, logdet, Xs.shape[1])[rows]
+    return _time.perf_counter() - t0
+
+
+def cpu_baseline(Xtr, rows_source, sigma0_fn, n_rows, nnz, k, thr, nu0, budget_s=20.0, procs=None,
+                 order_note="in the GPU's longest-first order"):
+    """The same sparse schedule as the GPU step, restated in numpy (the oracle),
+    timed on a bounded sample on the host cores.  rows_source(start, count)
+    gives kernel rows in the GPU's visiting order (longest first) as (rows,
+    CSR pointer, pair points); chunks of rows go to a pool of spawned worker
+    processes, one chunk each, until the budget is spent, and the normaliser
+    pass is timed on as many pairs.  One VI iteration = the per-row time scaled
+    to all n_rows rows plus the normaliser scaled to all nnz pairs."""
+    import multiprocessing as mp
+
+    from oracle import lakde_oracle as O
+
+    D = Xtr.shape[1]
+    procs = procs or os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    rows_per_job = 64 if D > 32 else 256
+    done_rows = done_pairs = 0
+    wall = 0.0
+    rng = np.random.default_rng(0)
+    with ctx.Pool(procs) as pool:
+        start = 0
+        while wall < budget_s and start < n_rows:
+            jobs = []
+            for _ in range(procs):
+                rows, sub_ptr, pts = rows_source(start, rows_per_job)
+                start += rows_per_job
+                if len(rows) == 0:
+                    break
+                uniq, inv = np.unique(np.concatenate([rows, pts]), return_inverse=True)
+                Xs = Xtr[uniq].astype(np.float32)
+                sig0, L0 = sigma0_fn(rows)
+                r = rng.uniform(0.0, 2.0 / k, len(pts)).astype(np.float32)
+                scale = np.full(len(rows), nu0, np.float32)
+                jobs.append((Xs, sub_ptr, inv[len(rows):], r, inv[:len(rows)], sig0, L0, nu0, scale))
+                done_rows += len(rows)
+                done_pairs += len(pts)
+            if not jobs:
+                break
+            t0 = time.perf_counter()
+            pool.map(_cpu_rows, jobs)
+            wall += time.perf_counter() - t0
+    # the normaliser over as many pairs as the sample had (scatter / gather passes)
+    m = max(1, min(done_pairs, nnz))
+    npt = max(1, m // k)
+    colm = rng.integers(0, npt, m)
+    lr = rng.normal(-5, 3, m).astype(np.float32)
+    t0 = time.perf_counter()
+    O.sparse_normalise(colm, lr, np.zeros(npt, np.float32), np.ones(npt, np.float32), npt, 1, thr)
+    t_norm = time.perf_counter() - t0
+    per_iter = wall * n_rows / max(done_rows, 1) + t_norm * nnz / m
     return {
-        "value": 1.0 / (per_step * n_kb),
+        "value": 1.0 / per_iter,
         "unit": "VI iters/s",
-        "cores": os.cpu_count(),
+        "cores": procs,
         "kind": "port",
-        "sample": (f"posterior of one 512-kernel block ({t_post:.2f} s) + {done} of {n_pb} point blocks of its "
-                   f"dense E-step ({t_block:.3f} s each), numpy oracle; extrapolated to {n_pb} point blocks x "
-                   f"{n_kb} kernel blocks"),
+        "sample": (f"the GPU step's sparse schedule (kNN pattern, block = N) in the oracle's numpy restatement: "
+                   f"{done_rows} of {n_rows} kernel rows {order_note} ({done_pairs} pairs: "
+                   f"M-step, FP64 jittered Cholesky, inverse, trace, E-step numerators) in {wall:.1f} s on {procs} "
+                   f"spawned processes, plus the normaliser on {m} pairs ({t_norm:.2f} s); scaled to {n_rows} "
+                   f"rows and {nnz} pairs"),
     }
 
 
+def pattern_rows_source(rowptr, col, order):
+    """rows_source of cpu_baseline over a host copy of the engine's pattern."""
+    def source(start, count):
+        rows = order[start:start + count].astype(np.int64)
+        lo, hi = rowptr[rows], rowptr[rows + 1]
+        ptr = np.concatenate([[0], np.cumsum(hi - lo)]).astype(np.int64)
+        pts = np.concatenate([col[a:b] for a, b in zip(lo, hi)]) if len(rows) else np.zeros(0, np.int64)
+        return rows, ptr, pts.astype(np.int64)
+    return source
+
+
 def run_reference(args):
+    """The reference arm: the CPU restatement of the same sparse schedule timed
+    on the host cores (rank 0 only); each step is one bounded sample.  Kernel
+    rows of the sample take the k nearest neighbours of their centre among a
+    pool of 50,000 points as their pairs (the pattern's rows hold k pairs on
+    average), and a kNN covariance of the same pool as their prior."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     Xtr, Xte, k, thr, desc = make_data(args.workload)
-    from oracle import lakde_oracle as O
-
-    # kNN graph for the sample: exact ranks of the first block's neighbourhoods only
-    N = len(Xtr)
-    graph = np.empty((N, k), dtype=np.int64)
+    N, D = Xtr.shape
     rng = np.random.default_rng(0)
-    # the sampled steps read the graph rows of their own blocks only; other rows
-    # get random neighbours (they do not enter the timed work)
-    graph[:] = rng.integers(0, N, size=(N, k))
-    graph[:1024] = O.knn_graph(Xtr, k)[:1024] if N <= 1024 else _block_knn(Xtr, k, 1024)
-    # each timed step is one bounded sample; stop after ~90 s
+    perm = rng.permutation(N)
+    pool = Xtr[: min(N, 50_000)].astype(np.float64)
+
+    def source(start, count):
+        rows = perm[start:start + count].astype(np.int64)
+        d = ((Xtr[rows, None, :].astype(np.float64) - pool[None]) ** 2).sum(-1)
+        nbr = np.argpartition(d, k, axis=1)[:, :k]
+        ptr = np.arange(0, (len(rows) + 1) * k, k, dtype=np.int64)
+        return rows, ptr, nbr.reshape(-1).astype(np.int64)
+
+    def sigma0_fn(rows):
+        d = ((Xtr[rows, None, :].astype(np.float64) - pool[None]) ** 2).sum(-1)
+        nbr = np.argpartition(d, k, axis=1)[:, :k]
+        diff = pool[nbr] - Xtr[rows][:, None, :]
+        sig = np.einsum("nki,nkj->nij", diff, diff) / k + 1e-6 * np.eye(D)
+        return sig.astype(np.float32), np.linalg.cholesky(sig).astype(np.float32)
+
     vals = []
     t0 = time.perf_counter()
     for _ in range(max(1, args.steps)):
-        vals.append(cpu_baseline(Xtr, graph, k, thr, budget_s=5.0))
-        if time.perf_counter() - t0 > 90.0:
+        vals.append(cpu_baseline(Xtr, source, sigma0_fn, N, N * k, k, thr, float(D), budget_s=8.0,
+                                 order_note="in random order, each with its k nearest neighbours as pairs"))
+        if time.perf_counter() - t0 > 100.0:
             break
     v = statistics.median([x["value"] for x in vals])
     cb = dict(vals[-1])
@@ -287,7 +364,8 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "VI iters/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.workload}: {desc}", "schedule": "block_size=512, dense E-step"},
+        "config": {"workload": f"{args.workload}: {desc}",
+                   "schedule": "fused batch VI (block_size=N) on the kNN candidate pattern, numpy restatement"},
         "cpu_baseline": cb,
         "e2e": {"value": v, "unit": "VI iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -303,6 +381,32 @@ def _block_knn(X, k, rows):
         part = np.argpartition(d, k, axis=1)[:, :k]
         dd = np.take_along_axis(d, part, 1)
         out[s:s + 256] = np.take_along_axis(part, np.argsort(dd, axis=1, kind="stable"), 1)
+    return out
+
+
+def fp64_check(Xtr, Xte, graph, thr, iters, dev):
+    """Held-out mean log density and ELBO after `iters` VI iterations from the
+    same initialisation (same data, kNN graph and pattern) in mixed precision,
+    plain FP32 and FP64; each model is freed before the next is built."""
+    import torch
+
+    from lakde_b200 import LocalKNearestKDE
+
+    out = {"iterations": iters, "queries": int(len(Xte))}
+    for name, dt, prec in (("mixed", torch.float32, "mixed"), ("plain_fp32", torch.float32, "fp32"),
+                           ("fp64", torch.float64, "fp32")):
+        X = torch.tensor(Xtr, dtype=dt, device=dev)
+        Y = torch.tensor(Xte, dtype=dt, device=dev)
+        m = LocalKNearestKDE(k_or_knn_graph=graph, fused=True, cuda_graph=True, precision=prec)
+        m.fit(X, iterations=iters, sparsity_threshold=thr)
+        ll = m.log_pred_density(X, Y).double()
+        out[name] = {"mean_log_density": float(ll.mean()), "elbo": float(m.compute_elbo(X))}
+        m.check_errors_()
+        del m, X, Y, ll
+        torch.cuda.empty_cache()
+    ref = out["fp64"]["mean_log_density"]
+    out["mixed_vs_fp64_nats"] = abs(out["mixed"]["mean_log_density"] - ref)
+    out["plain_fp32_vs_fp64_nats"] = abs(out["plain_fp32"]["mean_log_density"] - ref)
     return out
 
 
@@ -384,7 +488,7 @@ def run_sharded(args, world, rank, dev):
             "posterior_factor": timed(eng._factor, reps),
             ("estep_tc" if eng.precision == "mixed" else "estep_logrho"): timed(
                 lambda: eng.ops.estep(eng.pat, eng.X, eng.lo, eng.U, eng.nu, eng.logdet_W, eng.logrho,
-                                      eng.precision, eng.err), reps),
+                                      eng.precision, eng.err, **eng._tc_kw(W_cores=eng.Wc)), reps),
             "estep_normalise_stages+allreduce": timed(lambda: eng._normalise(1), reps),
         }
     t = torch.tensor([ms], device=dev)
@@ -436,7 +540,7 @@ def run_sharded(args, world, rank, dev):
                                  "queries": len(Xte), "kernels": N, "mean_log_density": float(lpd.mean())},
             "e2e": {"value": 1000.0 / e2e_ms, "unit": "VI iters/s", "h2d_bytes_per_step": X.numel() * 4,
                     "d2h_bytes_per_step": 8, "elbo": elbo},
-            "gpu_launches": 7 * args.steps,
+            "gpu_launches": (7 if D > 8 else 5) * args.steps,
             "clocks": clocks.summary(),
             "cpu_baseline": None,
         }
@@ -448,9 +552,10 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="gas8", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="bsds63", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-check", action="store_true", help="skip the mixed / FP32 / FP64 held-out comparison")
     ap.add_argument("--precision", default="auto", choices=["auto", "mixed", "fp32"])
     ap.add_argument("--sharded", action="store_true", help="the sharded engine also with one GPU")
     args = ap.parse_args()
@@ -478,6 +583,30 @@ def main():
             dist.destroy_process_group()
         return
 
+    run_single(args, dev, local)
+
+
+def roofline_fields(durations, N, D, nnz, workload, precision):
+    """Roofline of the dominant kernel (HBM: algorithmic bytes / event time
+    against the measured copy bandwidth) and the tensor-core kernels' rates."""
+    dom = max(durations, key=durations.get)
+    ab = alg_bytes(N, D, nnz)
+    peak, peak_kind = load_peaks()
+    achieved = ab[dom] / (durations[dom] * 1e-3) / 1e9
+    fl = alg_flops(N, D, nnz)
+    tflops = {k_: round(fl.get(k_, 0) / (v * 1e-3) / 1e12, 3) for k_, v in durations.items()}
+    return {
+        "kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": achieved / peak, "traffic": load_traffic(dom, workload), "peak_source": f"{peak_kind} hbm_gbs",
+        "alg_bytes_per_launch": ab[dom], "kernel_ms": {k_: round(v, 5) for k_, v in durations.items()},
+        "kernel_alg_tflops": tflops,
+        "kernel_hbm_frac": {k_: round(ab[k_] / (v * 1e-3) / 1e9 / peak, 4) for k_, v in durations.items() if k_ in ab},
+    }
+
+
+def run_single(args, dev, local):
+    import torch
+
     from lakde_b200 import LocalKNearestKDE
 
     Xtr, Xte, k, thr, desc = make_data(args.workload)
@@ -496,58 +625,46 @@ def main():
     torch.cuda.synchronize()
     snap = eng.snapshot()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
-
-    if world > 1:
-        dist.barrier()
     torch.cuda.synchronize()
     clocks = ClockSampler(local).__enter__()
 
     def busy():
-        for _ in range(20):
+        for _ in range(5):
             eng.step()
         torch.cuda.synchronize()
 
-    clocks.wait_for_samples(3, 20.0, busy)
+    clocks.wait_for_samples(3, 30.0, busy)
     n_before = len(clocks.samples)
     total_ms = timed_steps(eng, args.steps, flush, torch)
     torch.cuda.synchronize()
-    clocks.wait_for_samples(n_before + 2, 20.0, busy)
+    clocks.wait_for_samples(n_before + 2, 30.0, busy)
     clocks.__exit__(None, None, None)
     durations = kernel_split(eng, max(3, args.steps // 2), flush, torch)
     ms_per_step = total_ms / args.steps
-    if world > 1:
-        t = torch.tensor([ms_per_step], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_per_step = float(t)
-    value = world * 1000.0 / ms_per_step
+    value = 1000.0 / ms_per_step
+    roofline = roofline_fields(durations, N, D, nnz, args.workload, eng.precision)
 
-    # the roofline of the dominant kernel (HBM: compulsory bytes; the quad
-    # forms and the scatter at large D are gathers of whole point rows, so
-    # they are bound by memory, not by the tensor pipe)
-    dom = max(durations, key=durations.get)
-    ab = alg_bytes(N, D, nnz)
-    peak, peak_kind = load_peaks()
-    achieved = ab[dom] / (durations[dom] * 1e-3) / 1e9
-    traffic = load_traffic(dom, args.workload)
-    tflops = {k_: alg_flops(N, D, nnz).get(k_, 0) / (v * 1e-3) / 1e12 for k_, v in durations.items()}
-
-    # plain FP32 against mixed precision: the same number of iterations from the
-    # same saved state, timed the same way (large D only)
+    # the other precision from the same saved state, the same iterations,
+    # timed the same way (the plain FP32 kernels against mixed precision)
     plain = None
-    if D > 8 and eng.precision == "mixed":
+    if eng.precision == "mixed" or D > 8:
         n_cmp = max(3, args.steps // 2)
         lpd = {}
         ms = {}
-        for prec in ("mixed", "fp32"):
+        first = eng.precision
+        for prec in (first, "fp32" if first == "mixed" else "mixed"):
             eng.restore(snap)
             eng.precision = prec
             ms[prec] = timed_steps(eng, n_cmp, flush, torch) / n_cmp
             lpd[prec] = model.log_pred_density(X, Y).double()
+        eng.precision = "fp32"
         plain_split = kernel_split(eng, 3, flush, torch)
-        eng.precision = "mixed"
+        eng.precision = first
+        eng.restore(snap)
         plain = {
             "value": 1000.0 / ms["fp32"], "unit": "VI iters/s", "ms_per_step": ms["fp32"],
             "kernel_ms": {k_: round(v, 4) for k_, v in plain_split.items()},
+            "mixed_value": 1000.0 / ms["mixed"],
             "mixed_speedup": ms["fp32"] / ms["mixed"],
             "held_out_mean_log_density": {
                 "iterations_from_same_state": n_cmp,
@@ -556,6 +673,7 @@ def main():
                 "max_abs_diff_per_query": float((lpd["mixed"] - lpd["fp32"]).abs().max()),
             },
         }
+        del lpd
 
     # log_pred_density throughput (queries resident in HBM)
     for _ in range(2):
@@ -571,9 +689,8 @@ def main():
     lpd_ms = e0.elapsed_time(e1) / lpd_reps
     lpd_pts = len(Xte) / (lpd_ms * 1e-3)
 
-    # end to end through the public API with host buffers: pinned X copied
-    # into the device buffer the model and its captured iteration read, one
-    # partial_step_, ELBO read back to the host
+    # end to end through the public API with host buffers: pinned X copied into
+    # the device buffer the model reads, one partial_step_, ELBO read back
     Xh = torch.tensor(Xtr).pin_memory()
     assert eng.X.data_ptr() == X.data_ptr()
     torch.cuda.synchronize()
@@ -591,61 +708,69 @@ def main():
     e2e_ms /= args.steps
     model.check_errors_()
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(Xtr, model.knn_graph.cpu().numpy(), k, thr)
+    # the host pattern and prior of a sample of rows for the CPU baseline
+    cpu_src = None
+    if not args.no_cpu_baseline:
+        p = eng.pattern
+        cpu_src = (p.rowptr.cpu().numpy(), p.col.cpu().numpy(), p.order.cpu().numpy())
+        n_keep = min(N, 40_000 if D > 32 else 400_000)
+        keep_rows = torch.as_tensor(cpu_src[2][:n_keep].astype(np.int64), device=dev)
+        cpu_prior = (eng.sigma_0[keep_rows].cpu().numpy(), eng.sigma_0_tril[keep_rows].cpu().numpy())
+        cpu_pos = {int(r_): i for i, r_ in enumerate(cpu_src[2][:n_keep])}
+    graph = model.knn_graph
+    precision = eng.precision
+    gpu_launches = (2 if (D <= 8 and precision == "fp32") else 4) * args.steps
+    del model, eng, snap, X, Y, lpd
+    torch.cuda.empty_cache()
 
-    if rank == 0:
-        line = {
-            "metric": METRIC,
-            "value": value,
-            "unit": "VI iters/s",
-            "n_gpus": world,
-            "steps": args.steps,
-            "warmup": args.warmup,
-            "ms_per_step": ms_per_step,
-            "higher_is_better": True,
-            "scaling": "weak",
-            "vs_baseline": None,
-            "dtype": "f32",
-            "data": "synthetic",
-            "precision": (f"{eng.precision} (FP64 factorisations)" if D > 8 else
-                          "fp32 (plain FP32 GPU kernels; FP64 factorisations)"),
-            "config": {
-                "workload": f"{args.workload}: {desc}",
-                "schedule": "fused batch VI (block_size=N) on the kNN candidate pattern",
-                "nnz_pairs": nnz,
-                "sparsity_threshold": thr,
-                "l2": "flushed (256 MB write) before every timed step",
-                "parallelism": "single GPU",
-                "init_s": round(t_init, 3),
-            },
-            "roofline": {
-                "kernel": dom,
-                "bound": "hbm",
-                "achieved": achieved,
-                "peak": peak,
-                "unit": "GB/s",
-                "frac": achieved / peak,
-                "traffic": traffic,
-                "peak_source": f"{peak_kind} hbm_gbs",
-                "alg_bytes_per_launch": ab[dom],
-                "kernel_ms": {k_: round(v, 5) for k_, v in durations.items()},
-                "kernel_alg_tflops": {k_: round(v, 3) for k_, v in tflops.items()},
-            },
-            "plain_fp32": plain,
-            "log_pred_density": {"value": lpd_pts, "unit": "pts/s", "ms": lpd_ms, "queries": len(Xte),
-                                 "kernels": N, "mean_log_density": float(lpd.mean())},
-            "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "VI iters/s", "h2d_bytes_per_step": X.numel() * 4,
-                    "d2h_bytes_per_step": 8, "elbo": elbo},
-            "gpu_launches": (2 if D <= 8 else 4) * args.steps,
-            "clocks": clocks.summary(),
-            "cpu_baseline": cpu,
-        }
-        print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    check = None
+    if not args.no_fp64_check:
+        check = fp64_check(Xtr, Xte, graph, thr, 10, dev)
+
+    cpu = None
+    if cpu_src is not None:
+        def sigma0_fn(rows):
+            idx = np.array([cpu_pos[int(r_)] for r_ in rows])
+            return cpu_prior[0][idx], cpu_prior[1][idx]
+
+        cpu = cpu_baseline(Xtr, pattern_rows_source(*cpu_src), sigma0_fn, N, nnz, k, thr, float(D))
+
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "VI iters/s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "precision": (f"{precision}: tensor-core tf32 hi / lo contractions, FP64 factorisations"
+                      if precision == "mixed" else "fp32: plain FP32 GPU kernels, FP64 factorisations"),
+        "config": {
+            "workload": f"{args.workload}: {desc}",
+            "schedule": "fused batch VI (block_size=N) on the kNN candidate pattern",
+            "nnz_pairs": nnz,
+            "sparsity_threshold": thr,
+            "l2": "flushed (256 MB write) before every timed step",
+            "parallelism": "single GPU",
+            "init_s": round(t_init, 3),
+        },
+        "roofline": roofline,
+        "plain_fp32": plain,
+        "fp64_check": check,
+        "log_pred_density": {"value": lpd_pts, "unit": "pts/s", "ms": lpd_ms, "queries": len(Xte),
+                             "kernels": N, "precision": precision},
+        "e2e": {"value": 1000.0 / e2e_ms, "unit": "VI iters/s", "h2d_bytes_per_step": int(Xtr.size * 4),
+                "d2h_bytes_per_step": 8, "elbo": elbo},
+        "gpu_launches": gpu_launches,
+        "clocks": clocks.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
 
 
 if __name__ == "__main__":

@@ -28,9 +28,15 @@ __global__ void __launch_bounds__(kElboThreads) knn_elbo_kernel(const T *__restr
                                                                 double a0, double b0, double nu0,
                                                                 double *__restrict__ partials) {
   const double LOG2 = 0.69314718055994530942, LOG2PI = 1.83787706640934548356;
-  // terms of the prior that do not depend on the kernel
-  const double lg_a0 = lgamma(a0), log_b0 = log(b0), log_nu0 = log(nu0);
-  const double mvlg_nu0 = mvlgamma_d(0.5 * nu0, D);
+  // terms of the prior that do not depend on the kernel (only with kernel
+  // terms to add: a points-only call may pass any hyper-parameters)
+  double lg_a0 = 0.0, log_b0 = 0.0, log_nu0 = 0.0, mvlg_nu0 = 0.0;
+  if (n_kernels > 0) {
+    lg_a0 = lgamma(a0);
+    log_b0 = log(b0);
+    log_nu0 = log(nu0);
+    mvlg_nu0 = mvlgamma_d(0.5 * nu0, D);
+  }
   double acc = 0.0;
   const int64_t N = n_kernels > n_points ? n_kernels : n_points;
   for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {

@@ -169,6 +169,45 @@ extern "C" size_t lakde_log_pred_density_workspace(int dtype, int64_t N, int64_t
   return (size_t)(2 * nchunks * Nq) * es;
 }
 
+// The partial and fold launches of the predictive density over the (max, sum)
+// scratch `ws` (lakde_log_pred_density_workspace bytes), shared by the
+// workspace and the allocation-free entry points.
+static int launch_pred(const char *what, int dtype, int64_t N, int64_t Nq, int64_t D, const void *X,
+                       const void *W_triu, const void *nu, const void *log_coeff, const void *Y, void *out, void *ws,
+                       void *stream) {
+  return dispatch_float(dtype, [&](auto t0) {
+    using T = decltype(t0);
+    return dispatch_dp(D, [&](auto dp) {
+      constexpr int DP = decltype(dp)::value;
+      using C = PredCfg<T, DP>;
+      const int64_t chunk = pred_chunk(N, Nq, C::KT);
+      const int64_t nchunks = (N + chunk - 1) / chunk;
+      const int64_t q_tiles = (Nq + C::QT - 1) / C::QT;
+      if (q_tiles * nchunks > 0x7fffffffLL) {
+        set_error("%s: grid too large", what);
+        return (int)LAKDE_EUNSUPPORTED;
+      }
+      auto kern = pred_partial_kernel<T, DP>;
+      if (C::smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
+        if (e != cudaSuccess) {
+          set_error("%s: %s", what, cudaGetErrorString(e));
+          return (int)LAKDE_ECUDA;
+        }
+      }
+      T *ws_m = static_cast<T *>(ws);
+      T *ws_s = ws_m + nchunks * Nq;
+      kern<<<(unsigned)(q_tiles * nchunks), C::QT, C::smem, as_stream(stream)>>>(
+          static_cast<const T *>(X), static_cast<const T *>(W_triu), static_cast<const T *>(nu),
+          static_cast<const T *>(log_coeff), static_cast<const T *>(Y), ws_m, ws_s, N, Nq, (int)D, chunk, q_tiles);
+      if (int st = check_launch(what)) return st;
+      pred_combine_kernel<T><<<(unsigned)((Nq + 255) / 256), 256, 0, as_stream(stream)>>>(
+          ws_m, ws_s, static_cast<T *>(out), Nq, nchunks, (T)log((double)N));
+      return check_launch(what);
+    });
+  });
+}
+
 extern "C" int lakde_log_pred_density(int dtype, int64_t N, int64_t Nq, int64_t D, const void *X, const void *W_triu,
                                       const void *nu, const void *log_coeff, const void *Y, void *out,
                                       void *workspace, size_t workspace_bytes, void *stream) {
@@ -193,38 +232,7 @@ extern "C" int lakde_log_pred_density(int dtype, int64_t N, int64_t Nq, int64_t 
     return LAKDE_EINVAL;
   }
   if (int st = bind_device("log_pred_density", {out, X, W_triu, nu, log_coeff, Y, workspace})) return st;
-  return dispatch_float(dtype, [&](auto t0) {
-    using T = decltype(t0);
-    return dispatch_dp(D, [&](auto dp) {
-      constexpr int DP = decltype(dp)::value;
-      using C = PredCfg<T, DP>;
-      const int64_t chunk = pred_chunk(N, Nq, C::KT);
-      const int64_t nchunks = (N + chunk - 1) / chunk;
-      const int64_t q_tiles = (Nq + C::QT - 1) / C::QT;
-      if (q_tiles * nchunks > 0x7fffffffLL) {
-        set_error("log_pred_density: grid too large");
-        return (int)LAKDE_EUNSUPPORTED;
-      }
-      auto kern = pred_partial_kernel<T, DP>;
-      if (C::smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
-        if (e != cudaSuccess) {
-          set_error("log_pred_density: %s", cudaGetErrorString(e));
-          return (int)LAKDE_ECUDA;
-        }
-      }
-      T *ws_m = static_cast<T *>(workspace);
-      T *ws_s = ws_m + nchunks * Nq;
-      kern<<<(unsigned)(q_tiles * nchunks), C::QT, C::smem, as_stream(stream)>>>(
-          static_cast<const T *>(X), static_cast<const T *>(W_triu), static_cast<const T *>(nu),
-          static_cast<const T *>(log_coeff), static_cast<const T *>(Y), ws_m, ws_s, N, Nq, (int)D, chunk, q_tiles);
-      int st = check_launch("log_pred_density");
-      if (st) return st;
-      pred_combine_kernel<T><<<(unsigned)((Nq + 255) / 256), 256, 0, as_stream(stream)>>>(
-          ws_m, ws_s, static_cast<T *>(out), Nq, nchunks, (T)log((double)N));
-      return check_launch("log_pred_density_combine");
-    });
-  });
+  return launch_pred("log_pred_density", dtype, N, Nq, D, X, W_triu, nu, log_coeff, Y, out, workspace, stream);
 }
 
 // ---------------------------------------------------------------------------
@@ -244,16 +252,24 @@ constexpr size_t kNoAllocScratchBytes = 16u << 20;
 static __device__ __align__(256) unsigned char g_pred_scratch[kNoAllocScratchBytes];
 
 // Device address of g_pred_scratch per device, resolved on the first call that
-// runs on that device (with the device current).
-static void *g_pred_scratch_ptr[128];
+// runs on that device (with the device current) and kept for the life of the
+// process.  A cudaDeviceReset destroys the array with the context, so the
+// address is not valid across one (nor is any other device pointer).
+constexpr int kMaxDevices = 128;
+static void *g_pred_scratch_ptr[kMaxDevices];
 static std::mutex g_pred_scratch_mu;
 
 static int pred_scratch_address(void **out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= 128) {
+  if (e != cudaSuccess) {
     set_error("log_pred_density_noalloc: cudaGetDevice failed: %s", cudaGetErrorString(e));
     return LAKDE_ECUDA;
+  }
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_error("log_pred_density_noalloc: device index %d is beyond the %d devices this entry point serves", dev,
+              kMaxDevices);
+    return LAKDE_EUNSUPPORTED;
   }
   std::lock_guard<std::mutex> lock(g_pred_scratch_mu);
   if (!g_pred_scratch_ptr[dev]) {
@@ -299,32 +315,5 @@ extern "C" int lakde_log_pred_density_noalloc(int dtype, int64_t N, int64_t Nq, 
   if (int st = bind_device("log_pred_density_noalloc", {out, X, W_triu, nu, log_coeff, Y})) return st;
   void *scratch = nullptr;
   if (int st = pred_scratch_address(&scratch)) return st;
-  return dispatch_float(dtype, [&](auto t0) {
-    using T = decltype(t0);
-    return dispatch_dp(D, [&](auto dp) {
-      constexpr int DP = decltype(dp)::value;
-      using C = PredCfg<T, DP>;
-      const int64_t chunk = pred_chunk(N, Nq, C::KT);
-      const int64_t nchunks = (N + chunk - 1) / chunk;
-      const int64_t q_tiles = (Nq + C::QT - 1) / C::QT;
-      auto kern = pred_partial_kernel<T, DP>;
-      if (C::smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
-        if (e != cudaSuccess) {
-          set_error("log_pred_density_noalloc: %s", cudaGetErrorString(e));
-          return (int)LAKDE_ECUDA;
-        }
-      }
-      T *ws_m = static_cast<T *>(scratch);
-      T *ws_s = ws_m + nchunks * Nq;
-      kern<<<(unsigned)(q_tiles * nchunks), C::QT, C::smem, as_stream(stream)>>>(
-          static_cast<const T *>(X), static_cast<const T *>(W_triu), static_cast<const T *>(nu),
-          static_cast<const T *>(log_coeff), static_cast<const T *>(Y), ws_m, ws_s, N, Nq, (int)D, chunk, q_tiles);
-      int st = check_launch("log_pred_density_noalloc");
-      if (st) return st;
-      pred_combine_kernel<T><<<(unsigned)((Nq + 255) / 256), 256, 0, as_stream(stream)>>>(
-          ws_m, ws_s, static_cast<T *>(out), Nq, nchunks, (T)log((double)N));
-      return check_launch("log_pred_density_noalloc_combine");
-    });
-  });
+  return launch_pred("log_pred_density_noalloc", dtype, N, Nq, D, X, W_triu, nu, log_coeff, Y, out, scratch, stream);
 }

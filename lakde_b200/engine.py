@@ -109,6 +109,25 @@ class FusedVI:
     def _tri(self):
         return self.pattern.rowptr, self.pattern.col
 
+    def restore_responsibilities(self, kern, point, values, point_sums=None):
+        """r from (kernel, point, value) triples (a checkpoint's COO blocks);
+        every pair must lie in the candidate pattern.  rsum = per-point sums of
+        r, from the checkpoint when it has them."""
+        p = self.pattern
+        keys = p.rows() * self.N + p.col.long()
+        want = kern.long() * self.N + point.long()
+        pos = torch.searchsorted(keys, want)
+        ok = (pos < keys.numel()) & (keys[pos.clamp(max=keys.numel() - 1)] == want)
+        if not bool(ok.all()):
+            raise ValueError(f"{int((~ok).sum())} responsibilities of the checkpoint lie outside the candidate "
+                             "pattern; resume with candidates='dense' or a pattern that contains them")
+        self.r.zero_()
+        self.r[pos] = values.to(self.dtype)
+        if point_sums is not None:
+            self.rsum.copy_(point_sums.to(self.dtype))
+        else:
+            self.rsum.zero_().scatter_add_(0, p.col.long(), self.r)
+
     @property
     def S(self):
         if self._S is None:

@@ -64,6 +64,10 @@ class VIModel(ABC):
     def data_log_likelihood(self, X):
         pass
 
+    def resume_(self, X, sparsity_threshold=None):
+        """Prepares a model restored by ``load_state_dict`` to continue fitting
+        (the models override it; nothing to do by default)."""
+
     def num_blocks(self, N):
         return (N - 1) // self.block_size + 1
 
@@ -84,6 +88,8 @@ class VIModel(ABC):
         if self.iter_steps == 0:
             self.init_parameters_(X, threshold)
             self.init_summaries_(X, threshold)
+        else:
+            self.resume_(X, threshold)
         blocks = self.num_blocks(X.size(0))
         try:
             for _ in range(iterations * blocks):

@@ -255,17 +255,49 @@ class LocallyAdaptiveKDE(VIModel, ABC):
                    "rnm_active_contribs", "W_inv_jitter")
 
     def state_dict(self):
+        """The reference's keys (lakde/local_adaptive_kde.py:287-305); the fused
+        path writes its responsibilities as one COO block and adds the per-point
+        sums of r (``rnm_point_sums``), so a resumed fit continues bit for bit."""
         d = super().state_dict()
         if self.fused and self.engine is not None:
             self.rnm_blocks = self.fused_rnm_blocks()
             self.rnm_active_contribs = torch.count_nonzero(self.engine.r)
+            d["rnm_point_sums"] = self.engine.rsum.clone()
         d.update({k: getattr(self, k) for k in self._STATE_KEYS})
         return d
 
     def load_state_dict(self, state_dict):
+        """Restores the reference's keys (lakde/local_adaptive_kde.py:272-285).
+        The next ``fit`` continues from this state (``resume_``): the block
+        schedule uses the COO blocks as they are; the fused schedule rebuilds
+        its engine and scatters the COO blocks (any block size, the reference's
+        included) into its candidate pattern."""
         super().load_state_dict(state_dict)
         for k in self._STATE_KEYS:
             setattr(self, k, state_dict[k])
+        self.engine = None
+        self._point_sums = state_dict.get("rnm_point_sums")
+
+    def _resume_tensors(self, X, keys):
+        dev = X.device
+        for k in keys:
+            v = getattr(self, k, None)
+            if torch.is_tensor(v):
+                setattr(self, k, v.to(dev))
+        self.rnm_blocks = [(ind.to(dev), val.to(device=dev, dtype=X.dtype)) for ind, val in self.rnm_blocks]
+
+    def _restore_engine_state(self, eng):
+        """Responsibilities and per-kernel / per-point state of a checkpoint into a
+        freshly built engine (whose prior is already computed)."""
+        kern, point, vals = [], [], []
+        for bi, (ind, val) in enumerate(self.rnm_blocks):
+            kern.append(ind[0].long() + bi * self.block_size)
+            point.append(ind[1].long())
+            vals.append(val)
+        eng.restore_responsibilities(torch.cat(kern), torch.cat(point), torch.cat(vals), self._point_sums)
+        for name, src in (("c", self.rnm_log_consts), ("a", self.a), ("b", self.b), ("nu", self.nu),
+                          ("logdet_W", self.logdet_W), ("W_inv_jitter", self.W_inv_jitter)):
+            getattr(eng, name).copy_(src.to(eng.dtype))
 
     def hparam_state_dict(self):
         d = super().hparam_state_dict()

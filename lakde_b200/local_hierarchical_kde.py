@@ -100,6 +100,39 @@ class LocalHierarchicalKDE(LocallyAdaptiveKDE):
         self.logdet_W = X.new_empty(N)
         self.expect_lambda_contribs = X.new_empty(self.num_blocks(N), D, D, dtype=torch.double)
 
+    def resume_(self, X, sparsity_threshold=None):
+        """Continues from a restored state dict.  The fused engine is rebuilt:
+        the candidate pattern from the kNN graph of ``k_or_knn_graph``
+        (recomputed from X when it is a count), then r, c, the per-kernel state
+        and the shared precision from the checkpoint."""
+        N, D = X.shape
+        self._resume_tensors(X, self._STATE_KEYS + self._HIER_KEYS)
+        if not self.fused or self.engine is not None:
+            return
+        self.a_0 = tensor_as(self.a_0, X)
+        self.b_0 = tensor_as(self.b_0, X)
+        self.nu_0 = tensor_as(self.nu_0, X)
+        g = self.k_or_knn_graph
+        if isinstance(g, int):
+            graph = compute_knn_graph(X, g, 1024, include_self=True, metric="l2", dtype=torch.int32)
+        else:
+            graph = (torch.from_numpy(g) if isinstance(g, np.ndarray) else g).to(X.device)
+        self.k = graph.size(-1)
+        init_k = min(math.floor(1 / sparsity_threshold), self.k) if sparsity_threshold else self.k
+        pattern = build_pattern(self.candidates, graph, N, X.device, self.candidate_counts)
+        eng = FusedHier(X, graph, pattern, self.nu_0, self.a_0, self.b_0, sparsity_threshold, init_k,
+                        tensor_as(self.nu_shared_0, X), self.precision)
+        self._restore_engine_state(eng)
+        eng.W_shared_triu.copy_(self.W_shared_triu.to(eng.W_shared_triu.dtype))
+        eng.expect_lambda_contribs[0] = self.expect_lambda_contribs.sum(0)
+        eng.W_shared_inv_jitter.copy_(self.W_shared_inv_jitter.reshape(-1)[:1].to(torch.float64))
+        eng._refresh_prior()
+        self.engine = eng
+        self._eager_steps = 0
+        self._sync_from_engine()
+        self._sync_shared()
+        self.block_size = N
+
     def _sync_shared(self):
         eng = self.engine
         self.lambda_0_triu = eng.lambda_0_triu

@@ -104,6 +104,35 @@ class LocalKNearestKDE(LocallyAdaptiveKDE):
         self.logdet_W = X.new_empty(N)
         self.sigma_0_lambda_mm_trace = X.new_empty(N)
 
+    def resume_(self, X, sparsity_threshold=None):
+        """Continues from a restored state dict (lakde/kdes.py:42-48 skips the
+        initialisation once iter_steps > 0).  The fused engine is rebuilt: the
+        candidate pattern from the saved kNN graph, the prior recomputed from X
+        (deterministic), then r, c and the per-kernel state from the checkpoint."""
+        N, D = X.shape
+        self._resume_tensors(X, self._STATE_KEYS + self._KNN_KEYS)
+        if not self.fused or self.engine is not None:
+            return
+        self.a_0 = tensor_as(self.a_0, X)
+        self.b_0 = tensor_as(self.b_0, X)
+        self.nu_0 = tensor_as(self.nu_0, X)
+        self.knn_graph = self.knn_graph.to(X.device)
+        self.k = self.knn_graph.size(-1)
+        init_k = min(math.floor(1 / sparsity_threshold), self.k) if sparsity_threshold else self.k
+        pattern = build_pattern(self.candidates, self.knn_graph, N, X.device, self.candidate_counts)
+        eng = FusedKNN(X, self.knn_graph, pattern, self.nu_0, self.a_0, self.b_0, sparsity_threshold, init_k,
+                       self.precision)
+        eng.init_prior()
+        self._restore_engine_state(eng)
+        eng.sigma_0_lambda_mm_trace.copy_(self.sigma_0_lambda_mm_trace.to(eng.dtype))
+        self.engine = eng
+        self._eager_steps = 0
+        self._sync_from_engine()
+        self.sigma_0_jitter = eng.sigma_0_jitter
+        self.logdet_sigma_0 = eng.logdet_sigma_0
+        self.sigma_0_lambda_mm_trace = eng.sigma_0_lambda_mm_trace
+        self.block_size = N
+
     def init_summaries_(self, X, sparsity_threshold=None):
         """lakde/local_knn_kde.py:140-193."""
         if self.fused:

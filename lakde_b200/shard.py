@@ -153,9 +153,9 @@ class CudaShardOps:
         return self.K.knn_elbo_parts(D, a_0, b_0, nu_0, a=a, b=b, nu=nu, logdet_W=logdet_W,
                                      logdet_sigma_0=logdet_sigma_0, mm=mm).reshape(1)
 
-    def elbo_point_terms(self, c, D, tail):
+    def elbo_point_terms(self, c, D, tail, a_0, b_0, nu_0):
         """float64 sum of the ELBO's per-point terms plus tail (0-dim)."""
-        return self.K.knn_elbo_parts(D, 0.0, 1.0, 1.0, c=c, tail=tail)
+        return self.K.knn_elbo_parts(D, a_0, b_0, nu_0, c=c, tail=tail)
 
     def vi_rows(self, pat, r, X, lo, nu_0, a, b, b_0, jitter, eps, nu, logdet, info, logrho, P, T, mm):
         """M-step, factorisation, b update and log rho of this shard's rows in
@@ -328,7 +328,7 @@ class ShardedKNN:
         kern = self.ops.elbo_kernel_terms(self.a, self.b, self.nu, self.logdet_W, self.logdet_sigma_0, self.mm, D,
                                           self.a_0, self.b_0, self.nu_0)
         self.comm.sum_(kern)
-        return kern[0] + self.ops.elbo_point_terms(self.c, D, -N * math.log(N - 1))
+        return kern[0] + self.ops.elbo_point_terms(self.c, D, -N * math.log(N - 1), self.a_0, self.b_0, self.nu_0)
 
     def log_pred_density(self, Y):
         """lakde/local_adaptive_kde.py:200-223 over the kernels of all ranks:

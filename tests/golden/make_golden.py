@@ -7,6 +7,8 @@ checkout; the tests read the .npz files.
 
     python tests/golden/make_golden.py path/to/lakde-checkout
     LAKDE_REFERENCE=path/to/lakde-checkout python tests/golden/make_golden.py
+
+GOLDEN_ONLY=ops|models|checkpoint regenerates one group of fixtures.
 """
 
 import os
@@ -192,6 +194,45 @@ def model_fixtures():
         print(name, res["elbo"][-1], res["ll"].mean(), int(res["nnz"]))
 
 
+def state_to_arrays(state, prefix="state_"):
+    """A reference state dict as flat npz arrays (rnm_blocks block by block)."""
+    out = {}
+    for key, v in state.items():
+        if key == "rnm_blocks":
+            out[prefix + "rnm_nblocks"] = np.array(len(v))
+            for bi, (ind, val) in enumerate(v):
+                out[f"{prefix}rnm_b{bi}_ind"] = t2n(ind)
+                out[f"{prefix}rnm_b{bi}_val"] = t2n(val)
+        elif torch.is_tensor(v):
+            out[prefix + key] = t2n(v)
+        else:
+            out[prefix + key] = np.array(v)
+    return out
+
+
+def checkpoint_fixtures():
+    """The reference's state dict after 5 iterations of the config-1 run
+    (block_size 512, float32), then the ELBO after every block update and the
+    held-out log density of 5 more iterations of the same model object."""
+    Xtr, Xte = circle_gmm(seed=0, n_train=2000, n_test=1000)
+    Xt, Yt = torch.tensor(Xtr), torch.tensor(Xte)
+    m = LocalKNearestKDE(block_size=512, k_or_knn_graph=20)
+    m.fit(Xt, iterations=5, sparsity_threshold=None)
+    res = state_to_arrays(m.state_dict())
+    res["elbo_at_state"] = np.array(float(m.compute_elbo(Xt)))
+    rec = Recorder()
+    m.fit(Xt, iterations=5, callbacks=rec, sparsity_threshold=None)
+    res.update(X=Xtr, Y=Xte, elbo_after=np.array(rec.elbo), ll_after=t2n(m.log_pred_density(Xt, Yt)),
+               c_after=t2n(m.rnm_log_consts))
+    np.savez_compressed(os.path.join(HERE, "knn_c1_f32_b512_resume.npz"), **res)
+    print("knn_c1_f32_b512_resume", res["elbo_after"][-1], res["ll_after"].mean())
+
+
 if __name__ == "__main__":
-    ops_fixtures()
-    model_fixtures()
+    only = os.environ.get("GOLDEN_ONLY")
+    if only in (None, "ops"):
+        ops_fixtures()
+    if only in (None, "models"):
+        model_fixtures()
+    if only in (None, "checkpoint"):
+        checkpoint_fixtures()

@@ -215,6 +215,139 @@ def test_hierarchical_uneven_neighbourhoods_match_restricted_oracle(dtype):
         np.testing.assert_allclose(m.rnm_log_consts.cpu().numpy(), ora.rnm_log_consts, atol=1e-5)
         np.testing.assert_allclose(ll, ll_o, atol=1e-5)
     else:
+        # float32 data runs the tensor-core path (tf32 hi / lo); its accuracy
+        # against FP64 on this data is asserted at full size below
         assert m.engine.precision == "mixed"
         assert np.isfinite(ll).all() and np.isfinite(rec.elbo).all()
         m.check_errors_()
+
+
+def test_embedded_mixture_full_size_mixed_vs_fp64():
+    """The near-singular hierarchical workload at its full size: d=43, 30,000
+    training and 3,000 held-out points from a 10-dim 6-component mixture
+    embedded in 43 dims with 1e-3 noise (local condition numbers near 1e6),
+    each point explained by its first c_m nearest kernels with c_m lognormal
+    (median 64, sigma 1, cap 4,096), LocalHierarchicalKDE fused and replayed as
+    a CUDA graph for 10 iterations in FP64, plain FP32 and mixed precision
+    (tensor-core tf32 hi / lo contractions, FP64 factorisations).
+
+    Bound: the mixed held-out mean log density lies within 1e-3 nats of FP64,
+    or, where plain FP32 itself drifts further on this data, no further from
+    FP64 than plain FP32 does plus 1e-3 nats."""
+    from lakde_b200 import LocalHierarchicalKDE
+    from lakde_b200.sparse_util import PairPattern
+    from lakde_b200.synthetic import embedded_mixture, lognormal_neighbourhood_sizes
+    from lakde_b200.utils import compute_knn_graph
+
+    Xn, Yn = embedded_mixture(seed=0, n_train=30_000, n_test=3_000)
+    N = len(Xn)
+    X64 = torch.tensor(Xn.astype(np.float64), device=DEV)
+    Y64 = torch.tensor(Yn.astype(np.float64), device=DEV)
+    k0 = 16
+    counts = np.clip(lognormal_neighbourhood_sizes(N, seed=0), k0, N - 1)
+    kmax = int(counts.max())
+    graph = compute_knn_graph(X64, kmax).long()
+    keep = torch.arange(kmax, device=DEV)[None, :] < torch.tensor(counts, device=DEV)[:, None]
+    kern = graph[keep]
+    point = torch.arange(N, device=DEV).repeat_interleave(torch.tensor(counts, device=DEV))
+    pattern = PairPattern.from_pairs(kern, point, N, N)
+    seed_graph = graph[:, :k0].to(torch.int32).contiguous()
+    res = {}
+    for name, dt, prec in (("fp64", torch.float64, "fp32"), ("fp32", torch.float32, "fp32"),
+                           ("mixed", torch.float32, "mixed")):
+        m = LocalHierarchicalKDE(k_or_knn_graph=seed_graph, fused=True, candidates=pattern, cuda_graph=True,
+                                 precision=prec)
+        m.fit(X64.to(dt), iterations=10)
+        m.check_errors_()
+        assert m.engine.precision == prec
+        ll = m.log_pred_density(X64.to(dt), Y64.to(dt)).double()
+        assert bool(torch.isfinite(ll).all()), name
+        res[name] = (float(ll.mean()), float(m.compute_elbo(X64.to(dt))))
+        del m
+        torch.cuda.empty_cache()
+    d_mixed = abs(res["mixed"][0] - res["fp64"][0])
+    d_fp32 = abs(res["fp32"][0] - res["fp64"][0])
+    print("held-out mean log density and ELBO:", res, "mixed-fp64", d_mixed, "fp32-fp64", d_fp32)
+    assert d_mixed <= max(1e-3, d_fp32 + 1e-3), res
+
+
+# ------------------------------------------------------------- checkpoints
+def _reference_state(g):
+    """The reference's state dict stored by tests/golden/make_golden.py
+    (checkpoint_fixtures), as device tensors."""
+    st = {"rnm_blocks": [(torch.tensor(g[f"state_rnm_b{i}_ind"], device=DEV),
+                          torch.tensor(g[f"state_rnm_b{i}_val"], device=DEV))
+                         for i in range(int(g["state_rnm_nblocks"]))]}
+    for key in g.files:
+        if not key.startswith("state_") or key.startswith("state_rnm_b") or key == "state_rnm_nblocks":
+            continue
+        name, v = key[len("state_"):], g[key]
+        st[name] = v.item() if name in ("block_size", "verbose", "iter_steps", "k") else torch.tensor(v, device=DEV)
+    return st
+
+
+def test_reference_checkpoint_resumes_on_the_block_schedule():
+    """A state dict the reference wrote after 5 iterations of the config-1 run
+    (block_size 512, float32) continues here exactly as it continued in the
+    reference: ELBO after every block update, normaliser and held-out log
+    density after 5 more iterations."""
+    from lakde_b200 import LocalKNearestKDE
+
+    g = load("knn_c1_f32_b512_resume")
+    X = torch.tensor(g["X"], device=DEV)
+    Y = torch.tensor(g["Y"], device=DEV)
+    m = LocalKNearestKDE(k_or_knn_graph=20, block_size=512)
+    m.load_state_dict(_reference_state(g))
+    rec = Rec()
+    m.fit(X, iterations=5, callbacks=rec)
+    assert m.iter_steps == 40
+    np.testing.assert_allclose(rec.elbo, g["elbo_after"], rtol=2e-6)
+    np.testing.assert_allclose(m.rnm_log_consts.cpu().numpy(), g["c_after"], atol=5e-4)
+    np.testing.assert_allclose(m.log_pred_density(X, Y).cpu().numpy(), g["ll_after"], atol=5e-4)
+
+
+def test_reference_checkpoint_loads_into_the_fused_schedule():
+    """The same reference state dict scattered into the fused engine (all-pairs
+    pattern): the ELBO of the restored state equals the reference's, and the
+    batch iterations continue from it."""
+    from lakde_b200 import LocalKNearestKDE
+
+    g = load("knn_c1_f32_b512_resume")
+    X = torch.tensor(g["X"], device=DEV)
+    m = LocalKNearestKDE(k_or_knn_graph=20, fused=True, candidates="dense", cuda_graph=False)
+    m.load_state_dict(_reference_state(g))
+    m.fit(X, iterations=0)
+    e0 = float(m.compute_elbo(X))
+    np.testing.assert_allclose(e0, float(g["elbo_at_state"]), rtol=2e-6)
+    rec = Rec()
+    m.fit(X, iterations=3, callbacks=rec)
+    assert np.isfinite(rec.elbo).all() and rec.elbo[-1] >= e0 - 1e-4 * abs(e0)
+    # and it saves again as one block of the whole kernel set
+    st = m.state_dict()
+    assert st["block_size"] == len(X) and len(st["rnm_blocks"]) == 1
+
+
+@pytest.mark.parametrize("d,precision", [(2, "fp32"), (13, "mixed"), (13, "fp32")])
+def test_fused_checkpoint_round_trip_is_bit_identical(d, precision):
+    """save -> load -> continue gives the uninterrupted fit bit for bit (the
+    fused engine rebuilt from the COO blocks, CUDA graph replay on both sides)."""
+    import io
+
+    from lakde_b200 import LocalKNearestKDE
+    from lakde_b200.synthetic import heavy_tail_mixture
+
+    Xn, _ = heavy_tail_mixture(seed=4, n_train=4000, n_test=10, d=d)
+    X = torch.tensor(Xn.astype(np.float32), device=DEV)
+    kw = dict(k_or_knn_graph=16, fused=True, cuda_graph=True, precision=precision)
+    whole = LocalKNearestKDE(**kw).fit(X, iterations=5, sparsity_threshold=5e-4)
+    first = LocalKNearestKDE(**kw).fit(X, iterations=3, sparsity_threshold=5e-4)
+    buf = io.BytesIO()
+    torch.save(first.state_dict(), buf)
+    buf.seek(0)
+    resumed = LocalKNearestKDE(**kw)
+    resumed.load_state_dict(torch.load(buf, weights_only=False))
+    resumed.fit(X, iterations=2, sparsity_threshold=5e-4)
+    assert resumed.iter_steps == whole.iter_steps == 5
+    torch.testing.assert_close(resumed.rnm_log_consts, whole.rnm_log_consts, rtol=0, atol=0)
+    torch.testing.assert_close(resumed.engine.r, whole.engine.r, rtol=0, atol=0)
+    assert float(resumed.compute_elbo(X)) == float(whole.compute_elbo(X))

@@ -147,8 +147,25 @@ class NumpyShardOps:
         q_lam = torch.sum(B_q + (nu - D - 1) * e_logdet / 2 - nu / 2 * D)
         return ((p_lam - q_lam) + (p_tau - q_tau)).reshape(1)
 
-    def elbo_point_terms(self, c, D, tail):
+    def elbo_point_terms(self, c, D, tail, a_0=None, b_0=None, nu_0=None):
         return torch.sum(-D / 2 * math.log(2 * math.pi) + c.double()) + tail
+
+
+class NumpyShardOpsFused(NumpyShardOps):
+    """Adds the fused per-row pass of D <= 8 (lakde_vi_rows), restated with
+    the oracle, so the sharded engine takes its one-pass branch."""
+
+    def vi_rows(self, pat, r, X, lo, nu_0, a, b, b_0, jitter, eps, nu, logdet, info, logrho, P, T, mm):
+        n, D = nu.shape[0], X.shape[1]
+        S = torch.empty(n, D, D, dtype=X.dtype)
+        U = torch.empty_like(S)
+        trace = torch.empty(n, dtype=X.dtype)
+        self.mstep(pat, r, X, lo, nu_0, S, nu, "fp32", None)
+        # the factorisation reads E[tau] = a / b before b is updated
+        self.factor(S, jitter, eps, P, torch.tensor([nu_0], dtype=X.dtype), a, b, T, U, logdet, trace, info)
+        mm.copy_(nu * trace)
+        b.copy_(b_0 + nu_0 * mm / 2)
+        self.estep(pat, X, lo, U, nu, logdet, logrho, "fp32", None)
 
 
 ITERS, THR = 4, 1e-4
@@ -170,7 +187,7 @@ def knn_pattern(graph):
     return PairPattern(t(rowptr), t(point.astype(np.int32)), t(cptr), t(pos.astype(np.int32)), N, N, t(rank))
 
 
-def _fit(world, rank, port, outdir):
+def _fit(world, rank, port, outdir, fused=False):
     torch.set_num_threads(1)
     comm = LocalComm()
     if world > 1:
@@ -186,7 +203,8 @@ def _fit(world, rank, port, outdir):
     D = X.shape[1]
     pattern = knn_pattern(g["knn_graph"])
     eng = ShardedKNN(X, graph, pattern, nu_0=D, a_0=1e-6, b_0=1e-6, threshold=THR, init_k=graph.shape[1],
-                     comm=comm, ops=NumpyShardOps())
+                     comm=comm, ops=NumpyShardOpsFused() if fused else NumpyShardOps())
+    assert D <= 8  # the fused per-row branch is the D <= 8 step
     eng.init_summaries()
     elbo = []
     for _ in range(ITERS):
@@ -195,7 +213,7 @@ def _fit(world, rank, port, outdir):
     eng.check_errors()
     lpd = eng.log_pred_density(Y)
     k, m, r = eng.responsibilities()
-    np.savez(os.path.join(outdir, f"w{world}_r{rank}.npz"), elbo=np.array(elbo), c=eng.c.numpy(),
+    np.savez(os.path.join(outdir, f"w{world}_r{rank}_f{int(fused)}.npz"), elbo=np.array(elbo), c=eng.c.numpy(),
              rsum=eng.rsum.numpy(), lpd=lpd.numpy(), k=k.numpy(), m=m.numpy(), r=r.numpy(), lo=eng.lo, hi=eng.hi)
     if world > 1:
         import torch.distributed as dist
@@ -203,8 +221,8 @@ def _fit(world, rank, port, outdir):
         dist.destroy_process_group()
 
 
-def _spawned(rank, world, port, outdir):
-    _fit(world, rank, port, outdir)
+def _spawned(rank, world, port, outdir, fused):
+    _fit(world, rank, port, outdir, fused)
 
 
 def _free_port():
@@ -213,14 +231,17 @@ def _free_port():
         return s.getsockname()[1]
 
 
-@pytest.fixture(scope="module")
-def runs():
+@pytest.fixture(scope="module", params=[False, True], ids=["four-pass", "fused-rows"])
+def runs(request):
+    """World 1 and a gloo world of 2, through the four-pass step or the fused
+    per-row step (NumpyShardOpsFused.vi_rows)."""
     import torch.multiprocessing as mp
 
+    fused = request.param
     outdir = tempfile.mkdtemp(prefix="lakde_shard_")
-    _fit(1, 0, 0, outdir)
-    mp.spawn(_spawned, args=(2, _free_port(), outdir), nprocs=2, join=True)
-    load = lambda w, r: dict(np.load(os.path.join(outdir, f"w{w}_r{r}.npz")))  # noqa: E731
+    _fit(1, 0, 0, outdir, fused)
+    mp.spawn(_spawned, args=(2, _free_port(), outdir, fused), nprocs=2, join=True)
+    load = lambda w, r: dict(np.load(os.path.join(outdir, f"w{w}_r{r}_f{int(fused)}.npz")))  # noqa: E731
     return load(1, 0), [load(2, 0), load(2, 1)]
 
 

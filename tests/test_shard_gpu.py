@@ -147,3 +147,32 @@ def test_world_of_one_matches_the_fused_engine(precision, d):
     torch.testing.assert_close(sh.r, ref.r, rtol=0, atol=0)
     assert abs(float(sh.compute_elbo()) - float(ref.compute_elbo())) <= 1e-9 * abs(float(ref.compute_elbo()))
     torch.testing.assert_close(sh.log_pred_density(Y), ref.log_pred_density(Y), rtol=0, atol=2e-5)
+
+
+def test_elbo_parts_over_two_kernel_ranges_sum_to_the_whole():
+    """The sharded ELBO: the kernel terms of two kernel ranges (two ranks) plus
+    the point terms once equal lakde_knn_elbo over all kernels and points."""
+    from lakde_b200 import kernels as K
+
+    rng = np.random.default_rng(7)
+    N, D = 1000, 13
+    a = t(rng.uniform(5, 9, N))
+    b = t(rng.uniform(0.5, 2, N))
+    nu = t(rng.uniform(D + 1, D + 40, N))
+    ldw = t(rng.normal(0, 3, N))
+    lds0 = t(rng.normal(-5, 2, N))
+    mm = t(rng.uniform(1, 50, N))
+    c = t(rng.normal(-2, 1, N))
+    a_0, b_0, nu_0 = 1e-6, 1e-6, float(D)
+    whole = float(K.knn_elbo(a, b, nu, ldw, lds0, mm, c, a_0, b_0, nu_0, D))
+    cut = 377
+    parts = 0.0
+    for lo, hi in ((0, cut), (cut, N)):
+        parts += float(K.knn_elbo_parts(D, a_0, b_0, nu_0, a=a[lo:hi], b=b[lo:hi], nu=nu[lo:hi],
+                                        logdet_W=ldw[lo:hi], logdet_sigma_0=lds0[lo:hi], mm=mm[lo:hi]))
+    parts += float(K.knn_elbo_parts(D, a_0, b_0, nu_0, c=c, tail=-N * np.log(N - 1)))
+    assert abs(parts - whole) <= 1e-12 * abs(whole)
+    # a points-only call does not depend on the kernel hyper-parameters
+    p1 = float(K.knn_elbo_parts(D, a_0, b_0, nu_0, c=c))
+    p2 = float(K.knn_elbo_parts(D, 0.0, 0.0, 0.0, c=c))
+    assert p1 == p2 and np.isfinite(p2)
