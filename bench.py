@@ -187,23 +187,8 @@ def timed_steps(eng, steps, flush, torch):
 
 def kernel_split(eng, reps, flush, torch):
     """Average duration of each library kernel of the iteration, timed one by one."""
-    from lakde_b200 import kernels as K
-
     stream = torch.cuda.current_stream()
-    p = eng.pattern
-    if eng.D <= 8 and eng.precision == "fp32":
-        launches = {
-            "vi_rows": lambda: K.vi_rows(p.rowptr, p.col, eng.r, eng.X, eng.nu_0, eng.a, eng.b, eng.b_0_f,
-                                         eng.W_inv_jitter, eng.eps, eng.nu, eng.logdet_W, eng.info, eng.logrho,
-                                         P=eng.sigma_0, T=eng.sigma_0_tril, order=p.order,
-                                         mm=eng.sigma_0_lambda_mm_trace),
-        }
-    else:
-        tcs = "_tc" if eng.precision == "mixed" else ""
-        launches = {"mstep" + tcs: eng.mstep, "posterior_factor": eng.factor,
-                    "estep" + (tcs or "_logrho"): eng.estep_numerators}
-    launches["estep_normalise"] = lambda: K.estep_normalise(p.cptr, p.pos, eng.logrho, eng.r, eng.c, eng.rsum, 1,
-                                                            eng.threshold)
+    launches = eng.kernel_launches()
     out = {k: 0.0 for k in launches}
     for _ in range(reps):
         for name, fn in launches.items():

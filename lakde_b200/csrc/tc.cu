@@ -180,6 +180,8 @@ struct Args {
   const float *logdet;   // E-step
   const float *lc;       // predictive density: log coefficient per kernel
   float *logrho;         // E-step output, CSR order
+  const float *rw;       // E-step, optional: r per pair (CSR order) ...
+  float *rq;             // ... and the output sum_p r_p Q_p per kernel
   float *S;              // M-step output [N, D, D] (dense) ...
   int lower_only;
   float *SPo;            // ... or the S halves of the interleaved S / P tiles
@@ -211,7 +213,8 @@ struct Smem {
   static constexpr uint32_t RV = CIDX + 3 * MT * 4;                     // 3 x 128 float
   static constexpr uint32_t META = RV + 3 * MT * 4;                     // 3 x Meta
   static constexpr uint32_t PM = META + 3 * 64;                         // predictive density (max, sum)
-  static constexpr uint32_t BAR = PM + 2 * PQ * 4;                      // mbarriers
+  static constexpr uint32_t RQ = PM + 2 * PQ * 4;                       // E-step: per-warp partials, row sum
+  static constexpr uint32_t BAR = RQ + 64;                              // mbarriers
   static constexpr uint32_t bytes = BAR + 64;
 };
 static_assert(Smem::RSTR * 128 * 4 <= 4 * Smem::B_BYTES, "accumulator copy fits the B stages");
@@ -338,6 +341,7 @@ struct Kern {
         } else {
           c = g.col[base + p];
           if (MODE == MSTEP) w = g.r[base + p];
+          if (MODE == ESTEP && g.rw) w = g.rw[base + p];
           if (c < 0 || c >= g.npts) {
             c = -1;
             w = 0.f;
@@ -349,6 +353,8 @@ struct Kern {
       if (MODE == MSTEP) {
         rv[p] = w;
         rs += w;
+      } else if (MODE == ESTEP) {
+        rv[p] = w;
       }
       if (c >= 0) {
         const float *src = (MODE == PRED) ? g.Y + (int64_t)c * g.ldy : g.X + (int64_t)c * g.ldx;
@@ -562,6 +568,22 @@ struct Kern {
       for (int k = 0; k < 16; ++k) q = fmaf(v[k], v[k], q);
     }
     const int p = tid;
+    if (MODE == ESTEP && g.rw) {
+      // sum_p r_p Q_p of the row: warp sums, then the four in warp order
+      // (deterministic), carried over the row's tiles in shared memory
+      const float *rv = reinterpret_cast<const float *>(sm + Smem::RV) + ms * MT;
+      float *rq = reinterpret_cast<float *>(sm + Smem::RQ);
+      float part = (p < meta.cnt && cidx[p] >= 0) ? rv[p] * q : 0.f;
+      part = warp_sum(part);
+      if ((tid & 31) == 0) rq[warp] = part;
+      asm volatile("bar.sync 2, 128;" ::: "memory");
+      if (tid == 0) {
+        const float prev = (meta.flags & 1) ? 0.f : rq[4];
+        const float acc = prev + ((rq[0] + rq[1]) + (rq[2] + rq[3]));
+        rq[4] = acc;
+        if (meta.flags & 2) g.rq[meta.n] = acc;
+      }
+    }
     if (p >= meta.cnt) return;
     if (MODE == ESTEP) {
       const int32_t c = cidx[p];
@@ -857,7 +879,7 @@ extern "C" int lakde_pack_w_cores(int dtype, int64_t N, int64_t D, const void *W
 extern "C" int lakde_estep_tc(int dtype, int64_t N, int64_t D, int64_t npts, const void *rowptr, const void *col,
                               const void *order, const void *X, int64_t ldx, int64_t kernel_offset,
                               const void *W_cores, const void *nu, const void *logdet_W, void *logrho,
-                              int32_t *queue, int32_t *err, void *stream) {
+                              const void *r, void *rq_sum, int32_t *queue, int32_t *err, void *stream) {
   clear_error();
   if (int st = tc_common_checks("estep_tc", dtype, N, D, npts, kernel_offset, X, ldx)) return st;
   if (N == 0) return LAKDE_OK;
@@ -869,7 +891,12 @@ extern "C" int lakde_estep_tc(int dtype, int64_t N, int64_t D, int64_t npts, con
     set_error("estep_tc: W_cores must be 16-byte aligned");
     return LAKDE_EINVAL;
   }
-  if (int st = bind_device("estep_tc", {logrho, rowptr, col, order, X, W_cores, nu, logdet_W, queue, err})) return st;
+  if ((r == nullptr) != (rq_sum == nullptr)) {
+    set_error("estep_tc: r and rq_sum go together");
+    return LAKDE_EINVAL;
+  }
+  if (int st = bind_device("estep_tc", {logrho, rowptr, col, order, X, W_cores, nu, logdet_W, r, rq_sum, queue, err}))
+    return st;
   tc::Args g{};
   g.rowptr = static_cast<const int64_t *>(rowptr);
   g.col = static_cast<const int32_t *>(col);
@@ -880,6 +907,8 @@ extern "C" int lakde_estep_tc(int dtype, int64_t N, int64_t D, int64_t npts, con
   g.nu = static_cast<const float *>(nu);
   g.logdet = static_cast<const float *>(logdet_W);
   g.logrho = static_cast<float *>(logrho);
+  g.rw = static_cast<const float *>(r);
+  g.rq = static_cast<float *>(rq_sum);
   g.npts = npts;
   g.N = N;
   g.koff = kernel_offset;
