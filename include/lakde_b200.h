@@ -217,6 +217,21 @@ LAKDE_API int lakde_vi_rows(int dtype, int64_t N, int64_t D, int64_t npts,
  */
 LAKDE_API size_t lakde_w_cores_floats(int64_t D);
 
+/*
+ * Test hook of the bounded completion waits (no counterpart in the reference):
+ * lakde_estep_tc's kernel on the given inputs (float32, no order, no queue)
+ * with the first staged tile of each CTA expecting 16 bytes more than its
+ * copies deliver.  Every issued copy lands, so nothing stays in flight; the
+ * wait gives up after its time limit (1.5 s), *err becomes 1 and the kernel
+ * frees its tensor memory and returns.
+ */
+LAKDE_API int lakde_tc_wait_timeout_probe(int64_t N, int64_t D, int64_t npts,
+                                          const void *rowptr, const void *col,
+                                          const void *X, int64_t ldx,
+                                          const void *W_cores, const void *nu,
+                                          const void *logdet_W, void *logrho,
+                                          int32_t *err, void *stream);
+
 /* W cores of N kernels from W_triu [N, D, D] (dense, upper; float32). */
 LAKDE_API int lakde_pack_w_cores(int dtype, int64_t N, int64_t D,
                                  const void *W_triu, void *W_cores,

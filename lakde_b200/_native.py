@@ -65,6 +65,10 @@ _SIGNATURES = {
         _c_int,
     ),
     "lakde_w_cores_floats": ([_c_i64], ctypes.c_size_t),
+    "lakde_tc_wait_timeout_probe": (
+        [_c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
+        _c_int,
+    ),
     "lakde_pack_w_cores": ([_c_int, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp], _c_int),
     "lakde_estep_normalise": (
         [_c_int, _c_i64, _c_vp, _c_vp, _c_int, _c_vp, _c_vp, _c_vp, _c_vp, _c_int, _c_dbl, _c_vp],

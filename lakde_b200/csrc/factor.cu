@@ -286,11 +286,13 @@ __device__ __forceinline__ void assemble_tiles(const FactorArgs<T> &g, int64_t n
 // ---- tiled inputs: one bulk copy per matrix, converted in place ----------
 __device__ __forceinline__ uint32_t sm_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-constexpr uint32_t kBulkSpinLimit = 1u << 24;
+constexpr uint32_t kBulkSpinLimit = 1u << 26;
 
-// Waits for the mbarrier phase; false after kBulkSpinLimit polls.
+// Waits for the mbarrier phase; false once 1.5 s have passed (checked every
+// 1024 polls) or after kBulkSpinLimit polls.
 __device__ __forceinline__ bool bulk_wait(uint64_t *mbar, uint32_t parity) {
   const uint32_t a = sm_u32(mbar);
+  uint64_t t0 = 0;
   for (uint32_t it = 0; it < kBulkSpinLimit; ++it) {
     uint32_t done;
     asm volatile(
@@ -300,6 +302,12 @@ __device__ __forceinline__ bool bulk_wait(uint64_t *mbar, uint32_t parity) {
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
+    if ((it & 1023u) == 0) {
+      uint64_t now;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+      if (it == 0) t0 = now;
+      else if (now - t0 > 1500000000ull) return false;
+    }
   }
   return false;
 }

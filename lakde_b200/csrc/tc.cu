@@ -51,7 +51,8 @@ namespace tc {
 constexpr int MT = 128;        // pairs (queries) per tile: the MMA M
 constexpr int NTHR = 256;      // 8 warps
 constexpr int RAW_STRIDE = 256;  // bytes per staged pair row (D <= 64 floats)
-constexpr uint32_t kSpinLimit = 1u << 24;
+constexpr uint32_t kSpinLimit = 1u << 26;
+constexpr uint64_t kWaitLimitNs = 1500000000ull;  // 1.5 s: far above any copy or MMA of one tile
 constexpr int PQ = 2048;       // queries per predictive-density launch
 
 enum Mode { ESTEP = 0, MSTEP = 1, PRED = 2 };
@@ -96,9 +97,17 @@ __device__ __forceinline__ void mbar_arrive_tx(uint64_t *mbar, uint32_t bytes) {
                : "memory");
 }
 
-// Waits for the phase with the given parity; false after kSpinLimit polls.
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits for the phase with the given parity; false once kWaitLimitNs have
+// passed (checked every 1024 polls) or after kSpinLimit polls.
 __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity) {
   const uint32_t addr = smem_u32(mbar);
+  uint64_t t0 = 0;
   for (uint32_t it = 0; it < kSpinLimit; ++it) {
     uint32_t done;
     asm volatile(
@@ -108,6 +117,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity) {
         : "r"(addr), "r"(parity)
         : "memory");
     if (done) return true;
+    if ((it & 1023u) == 0) {
+      const uint64_t now = global_ns();
+      if (it == 0) t0 = now;
+      else if (now - t0 > kWaitLimitNs) return false;
+    }
   }
   return false;
 }
@@ -197,6 +211,7 @@ struct Args {
   int ntile;             // nt (nt + 1) / 2
   int32_t *queue;        // row counter of the work queue (zero at launch), or null
   int32_t *err;
+  int stall;             // test hook: the first stage expects 16 bytes no copy delivers
 };
 
 // Shared memory of one CTA.  The B stages of the E-step / predictive density
@@ -397,6 +412,7 @@ struct Kern {
       meta->rsum = P.racc;
     }
     __syncwarp();
+    if (g.stall && P.rows == 1 && first) bytes += 16;  // never delivered: the wait must give up
     if (lane == 0) mbar_arrive_tx(raw_full, bytes);
     else mbar_arrive(raw_full);
   }
@@ -845,6 +861,42 @@ int launch_rows(const char *what, tc::Args &g, int64_t rows, void *stream) {
 }
 
 }  // namespace
+
+// Test hook for the bounded waits: the E-step of lakde_estep_tc on the given
+// inputs, with the first staged tile of each CTA expecting 16 bytes more than
+// its copies deliver.  Every copy that is issued lands, so nothing is left in
+// flight; the stage's wait gives up after its time limit, the kernel sets *err
+// to 1, frees its tensor memory and returns.
+extern "C" int lakde_tc_wait_timeout_probe(int64_t N, int64_t D, int64_t npts, const void *rowptr, const void *col,
+                                           const void *X, int64_t ldx, const void *W_cores, const void *nu,
+                                           const void *logdet_W, void *logrho, int32_t *err, void *stream) {
+  clear_error();
+  if (int st = tc_common_checks("tc_wait_timeout_probe", LAKDE_F32, N, D, npts, 0, X, ldx)) return st;
+  if (N < 1 || !rowptr || !col || !W_cores || !nu || !logdet_W || !logrho || !err) {
+    set_error("tc_wait_timeout_probe: null pointer or no rows");
+    return LAKDE_EINVAL;
+  }
+  if (int st = bind_device("tc_wait_timeout_probe", {logrho, rowptr, col, X, W_cores, nu, logdet_W, err})) return st;
+  tc::Args g{};
+  g.rowptr = static_cast<const int64_t *>(rowptr);
+  g.col = static_cast<const int32_t *>(col);
+  g.X = static_cast<const float *>(X);
+  g.ldx = ldx;
+  g.Wc = static_cast<const float *>(W_cores);
+  g.nu = static_cast<const float *>(nu);
+  g.logdet = static_cast<const float *>(logdet_W);
+  g.logrho = static_cast<float *>(logrho);
+  g.npts = npts;
+  g.N = N;
+  g.D = (int)D;
+  g.nt = tile_blocks(D);
+  g.ntile = tile_total(D);
+  g.err = err;
+  g.stall = 1;
+  return dispatch_tc(D, [&](auto dp) {
+    return launch_rows<tc::ESTEP, decltype(dp)::value>("tc_wait_timeout_probe", g, N, stream);
+  });
+}
 
 extern "C" size_t lakde_w_cores_floats(int64_t D) {
   if (D < 1 || D > 64) return 0;

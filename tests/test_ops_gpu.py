@@ -630,3 +630,43 @@ def test_estep_tc_kernel_offset(K, D):
     Xp = K.pad_rows(t(X))
     lr4 = K.estep_tc(t(rowptr), t(cols, torch.int32), Xp, Wc, t(nu), t(logdet), err)
     torch.testing.assert_close(lr4, lr, rtol=0, atol=0)
+
+
+def test_bounded_wait_times_out_sets_err_and_the_engine_raises(K):
+    """A tensor-core completion wait that runs out: the test hook makes the
+    first stage's mbarrier expect 16 bytes no copy delivers (every issued copy
+    lands, nothing stays in flight).  The kernel gives up after its time
+    limit, sets err, frees its tensor memory and returns; the engine's error
+    check then raises, and the context stays usable."""
+    from lakde_b200 import _native as nat
+    from lakde_b200.engine import FusedKNN
+    from lakde_b200.sparse_util import PairPattern
+
+    rng, X, rowptr, cols = tc_problem(21, N=64, k=8)
+    N, D = X.shape
+    W = (rand_upper(rng, N, D, np.float64) / np.sqrt(D)).astype(np.float32)
+    nu = t(rng.uniform(D + 1, D + 10, N).astype(np.float32))
+    logdet = t(O.chol_logdet(W).astype(np.float32))
+    Xp = K.pad_rows(t(X))
+    Wc = K.pack_w_cores(t(W))
+    out = torch.zeros(len(cols), device=DEV)
+    Xt = t(X)
+    graph = torch.tensor(O.knn_graph(X, 8).astype(np.int32), device=DEV)
+    eng = FusedKNN(Xt, graph, PairPattern.from_knn_graph(graph), float(D), 1e-6, 1e-6, 0.0, 8)
+    eng.check_errors()
+    st = nat.lib().lakde_tc_wait_timeout_probe(N, D, N, nat.ptr(t(rowptr)), nat.ptr(t(cols, torch.int32)),
+                                               nat.ptr(Xp), Xp.stride(0), nat.ptr(Wc), nat.ptr(nu), nat.ptr(logdet),
+                                               nat.ptr(out), nat.ptr(eng.err), nat.stream_of(out))
+    nat.check(st, "tc_wait_timeout_probe")
+    torch.cuda.synchronize()
+    assert int(eng.err) == 1
+    with pytest.raises(RuntimeError, match="timed out"):
+        eng.check_errors()
+    # the device still works: an ordinary launch afterwards gives correct values
+    err = torch.zeros(1, dtype=torch.int32, device=DEV)
+    lr = K.estep_tc(t(rowptr), t(cols, torch.int32), Xt, Wc, nu, logdet, err)
+    ref = O.sparse_log_rho(rowptr, cols, X.astype(np.float64), W.astype(np.float64),
+                           nu.cpu().numpy().astype(np.float64), logdet.cpu().numpy().astype(np.float64))
+    assert int(err) == 0
+    fin = np.isfinite(ref)
+    np.testing.assert_allclose(lr.cpu().numpy()[fin], ref[fin], rtol=1e-4, atol=1e-3)
