@@ -56,6 +56,22 @@ LAKDE_API int lakde_abi_version(void);
 /* Largest data dimensionality D the factorisation and sparse kernels accept. */
 LAKDE_API int lakde_max_dim(void);
 
+/*
+ * Launch choices of kernels that have more than one equivalent form; every
+ * choice gives the same results, only the speed differs.  An autotuner times
+ * them on the caller's data and keeps the fastest, per knob and class of D
+ * (D <= 16, <= 32, <= 48, <= 64; process-wide, read at each launch).  No
+ * counterpart in the reference.
+ *   LAKDE_TUNE_FACTOR: 0 = the FP64 factorisation with two warps per block;
+ *                      1 = one warp per block, 11 blocks per SM, for calls
+ *                          that stage no T and write no L (else 0 is used).
+ *   LAKDE_TUNE_ROWS:   0 = tensor-core rows from the caller's work queue;
+ *                      1 = a static stride over the grid (the queue ignored).
+ */
+typedef enum { LAKDE_TUNE_FACTOR = 0, LAKDE_TUNE_ROWS = 1, LAKDE_TUNE_KNOBS = 2 } lakde_tune_knob;
+LAKDE_API int lakde_tuning_set(int knob, int64_t D, int value);
+LAKDE_API int lakde_tuning_get(int knob, int64_t D);
+
 /* ------------------------------------------------------------------------- */
 /* The three ops of the reference extension (same argument meaning).         */
 /* ------------------------------------------------------------------------- */

@@ -25,6 +25,8 @@ _SIGNATURES = {
     "lakde_last_error": ([], ctypes.c_char_p),
     "lakde_abi_version": ([], _c_int),
     "lakde_max_dim": ([], _c_int),
+    "lakde_tuning_set": ([_c_int, _c_i64, _c_int], _c_int),
+    "lakde_tuning_get": ([_c_int, _c_i64], _c_int),
     "lakde_ind2ptr": ([_c_vp, _c_int, _c_i64, _c_i64, _c_vp, _c_int, _c_vp], _c_int),
     "lakde_chol_quad_form": (
         [_c_int, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64, _c_i64, _c_i64, _c_vp],

@@ -61,7 +61,30 @@ int bind_device(const char *what, std::initializer_list<const void *> ptrs) {
   return LAKDE_OK;
 }
 
+// Launch choices set by an autotuner, per knob and class of D (D <= 16, 32,
+// 48, 64); process-wide, read at every launch.
+static int g_tuning[LAKDE_TUNE_KNOBS][4] = {};
+
+static int d_class(int64_t D) { return D <= 16 ? 0 : D <= 32 ? 1 : D <= 48 ? 2 : 3; }
+
+int tuning(int knob, int64_t D) {
+  return (knob >= 0 && knob < LAKDE_TUNE_KNOBS && D >= 1 && D <= kMaxDim) ? g_tuning[knob][d_class(D)] : 0;
+}
+
 }  // namespace lakde
+
+extern "C" int lakde_tuning_set(int knob, int64_t D, int value) {
+  lakde::clear_error();
+  static const int kChoices[LAKDE_TUNE_KNOBS] = {2, 2};
+  if (knob < 0 || knob >= LAKDE_TUNE_KNOBS || D < 1 || D > lakde::kMaxDim || value < 0 || value >= kChoices[knob]) {
+    lakde::set_error("tuning_set: knob %d at D=%lld has no choice %d", knob, (long long)D, value);
+    return LAKDE_EINVAL;
+  }
+  lakde::g_tuning[knob][lakde::d_class(D)] = value;
+  return LAKDE_OK;
+}
+
+extern "C" int lakde_tuning_get(int knob, int64_t D) { return lakde::tuning(knob, D); }
 
 extern "C" const char *lakde_last_error(void) { return lakde::g_last_error; }
 

@@ -29,6 +29,9 @@ int bind_device(const char *what, std::initializer_list<const void *> ptrs);
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Current value of a launch-choice knob for dimension D (lakde_tuning_set).
+int tuning(int knob, int64_t D);
+
 // Largest D handled by the register / shared-memory kernels.
 constexpr int kMaxDim = 64;
 

@@ -179,11 +179,15 @@ __global__ void __launch_bounds__(128) factor_thread_kernel(FactorArgs<T> g) {
 }
 
 // ------------------------- warp per matrix, FP64 tensor cores --------------
-template <int DP>
+template <int DP, bool LEAN = false>
 struct DmmaCfg {
   static constexpr int NT = DP / 8;
   static constexpr int NTILE = NT * (NT + 1) / 2;
-  static constexpr int WPB = 2;
+  // LEAN: no per-matrix T_n staged and no L output (the tiled path with its
+  // trace from the E-step): ~19 KB per warp at DP = 64, one warp per block,
+  // 11 blocks per SM (registers capped to fit)
+  static constexpr int WPB = LEAN ? 1 : 2;
+  static constexpr int BLOCKS_PER_SM = LEAN ? 11 : 1;
   // per warp: FP64 tiles, 1 / L_ii, then the lower triangle of a per-matrix
   // FP32 T_n (packed rows or tiles, in doubles rounded up to 16 bytes), which
   // doubles as the scratch tile of the L output (T_n is then not staged)
@@ -192,7 +196,7 @@ struct DmmaCfg {
   static constexpr int off_scratch = off_tstage;
   // T_n as packed rows, or as NTILE tiles of 64 floats (tiled inputs)
   static constexpr int tstage_rows = ((DP * (DP + 1) / 2 + 3) / 4) * 2;
-  static constexpr int tstage = tstage_rows > NTILE * 32 ? tstage_rows : NTILE * 32;
+  static constexpr int tstage = LEAN ? 0 : (tstage_rows > NTILE * 32 ? tstage_rows : NTILE * 32);
   static constexpr int off_mbar = off_tstage + tstage;  // one mbarrier (two doubles keep 16-byte alignment)
   static constexpr int per_warp = off_mbar + 2;
   static constexpr size_t smem = (size_t)WPB * per_warp * sizeof(double);
@@ -315,11 +319,11 @@ __device__ __forceinline__ bool bulk_wait(uint64_t *mbar, uint32_t parity) {
 // Lane 0 issues the copies of SP_n (into the tile area) and T_n (into the T
 // stage) on the warp's mbarrier; every lane first orders its earlier shared
 // memory accesses before the asynchronous writes.
-template <int DP>
+template <int DP, bool LEAN>
 __device__ __forceinline__ void bulk_issue(const FactorArgs<float> &g, int64_t n, double *M, uint64_t *mbar, int lane) {
-  using C = DmmaCfg<DP>;
+  using C = DmmaCfg<DP, LEAN>;
   constexpr uint32_t sp_bytes = C::NTILE * 512u, t_bytes = C::NTILE * 256u;
-  const uint32_t total = sp_bytes + (g.Tt ? t_bytes : 0u);
+  const uint32_t total = sp_bytes + ((!LEAN && g.Tt) ? t_bytes : 0u);
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   __syncwarp();
   if (lane == 0) {
@@ -329,7 +333,7 @@ __device__ __forceinline__ void bulk_issue(const FactorArgs<float> &g, int64_t n
                      sm_u32(M)),
                  "l"(g.SP + n * (int64_t)(C::NTILE * 128)), "r"(sp_bytes), "r"(sm_u32(mbar))
                  : "memory");
-    if (g.Tt)
+    if (!LEAN && g.Tt)
       asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                        sm_u32(M + C::off_tstage)),
                    "l"(g.Tt + n * (int64_t)(C::NTILE * 64)), "r"(t_bytes), "r"(sm_u32(mbar))
@@ -407,10 +411,10 @@ __device__ __forceinline__ void load_tcol(const T *Tn, int D, int lower, int Ac,
     }
 }
 
-template <typename T, int DP>
+template <typename T, int DP, bool LEAN>
 __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, double *M, int lane, uint32_t *phase,
                                            bool *halt) {
-  using C = DmmaCfg<DP>;
+  using C = DmmaCfg<DP, LEAN>;
   constexpr int NT = C::NT;
   double *scratch = M + C::off_scratch;
   double *rdiag = M + C::off_rdiag;
@@ -432,7 +436,7 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
     if constexpr (sizeof(T) == 4) {
       if (tiled) {
         uint64_t *mbar = reinterpret_cast<uint64_t *>(M + C::off_mbar);
-        bulk_issue<DP>(g, n, M, mbar, lane);
+        bulk_issue<DP, LEAN>(g, n, M, mbar, lane);
         const bool arrived = bulk_wait(mbar, *phase);
         *phase ^= 1u;
         if (!arrived) {
@@ -640,9 +644,10 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
 
 // Persistent: each warp walks matrices n, n + stride, ... (a grid of exactly
 // the resident blocks).
-template <typename T, int DP>
-__global__ void __launch_bounds__(32 * DmmaCfg<DP>::WPB) factor_dmma_kernel(FactorArgs<T> g) {
-  using C = DmmaCfg<DP>;
+template <typename T, int DP, bool LEAN>
+__global__ void __launch_bounds__(32 * DmmaCfg<DP, LEAN>::WPB, DmmaCfg<DP, LEAN>::BLOCKS_PER_SM)
+    factor_dmma_kernel(FactorArgs<T> g) {
+  using C = DmmaCfg<DP, LEAN>;
   extern __shared__ double smem_d[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double *M = smem_d + warp * C::per_warp;
@@ -656,7 +661,7 @@ __global__ void __launch_bounds__(32 * DmmaCfg<DP>::WPB) factor_dmma_kernel(Fact
   }
   __syncwarp();
   for (int64_t n = (int64_t)blockIdx.x * C::WPB + warp; n < g.N && !halt; n += stride) {
-    factor_one<T, DP>(g, n, M, lane, &phase, &halt);
+    factor_one<T, DP, LEAN>(g, n, M, lane, &phase, &halt);
     __syncwarp();
   }
 }
@@ -667,10 +672,10 @@ using namespace lakde;
 
 // Persistent DMMA launch: exactly the blocks that are resident at once
 // (registers and shared memory), so every block starts immediately.
-template <typename TT, int DP>
-static int launch_factor_dmma(const FactorArgs<TT> &g, int64_t N, void *stream) {
-  using C = DmmaCfg<DP>;
-  auto kern = factor_dmma_kernel<TT, DP>;
+template <typename TT, int DP, bool LEAN>
+static int launch_factor_dmma_v(const FactorArgs<TT> &g, int64_t N, void *stream) {
+  using C = DmmaCfg<DP, LEAN>;
+  auto kern = factor_dmma_kernel<TT, DP, LEAN>;
   if (C::smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
     if (e != cudaSuccess) {
@@ -691,6 +696,15 @@ static int launch_factor_dmma(const FactorArgs<TT> &g, int64_t N, void *stream) 
   if (blocks > (int64_t)sms * per_sm) blocks = (int64_t)sms * per_sm;
   kern<<<(unsigned)blocks, 32 * C::WPB, C::smem, as_stream(stream)>>>(g);
   return check_launch("posterior_factor");
+}
+
+// The lean variant when the call stages no T_n and writes no L and the
+// tuning table selects it (lakde_tuning_set, knob LAKDE_TUNE_FACTOR).
+template <typename TT, int DP>
+static int launch_factor_dmma(const FactorArgs<TT> &g, int64_t N, void *stream) {
+  const bool lean_ok = !g.L && !g.Tm && !g.Tt;
+  if (lean_ok && tuning(LAKDE_TUNE_FACTOR, g.D) == 1) return launch_factor_dmma_v<TT, DP, true>(g, N, stream);
+  return launch_factor_dmma_v<TT, DP, false>(g, N, stream);
 }
 
 extern "C" int lakde_posterior_factor(int dtype, int64_t N, int64_t D, const void *S, const void *P,

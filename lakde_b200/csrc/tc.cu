@@ -838,7 +838,7 @@ int sm_count() {
 
 // One persistent CTA per SM (the shared memory of the pipeline allows one).
 template <int MODE, int DP>
-int launch_rows(const char *what, tc::Args &g, int64_t rows, void *stream) {
+int launch_rows(const char *what, tc::Args g, int64_t rows, void *stream) {
   auto kern = tc::tc_kernel<MODE, DP>;
   const size_t smem = tc::Smem::bytes;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -846,6 +846,7 @@ int launch_rows(const char *what, tc::Args &g, int64_t rows, void *stream) {
     set_error("%s: %s", what, cudaGetErrorString(e));
     return LAKDE_ECUDA;
   }
+  if (tuning(LAKDE_TUNE_ROWS, g.D) == 1) g.queue = nullptr;
   if (g.queue) {
     e = cudaMemsetAsync(g.queue, 0, sizeof(int32_t), as_stream(stream));
     if (e != cudaSuccess) {

@@ -65,6 +65,7 @@ class FusedVI:
         self.a = (a_0 + nu_0 * D / 2).expand(N).contiguous()
         self.b = self.a.clone()
         self.graph = None
+        self.tuning = None  # launch choices picked by lakde_b200.tuning.tune_engine
         self.err = torch.zeros(1, dtype=torch.int32, device=self.device)
         # "mixed": the E- and M-step contractions on the tensor cores (tcgen05
         # kind::tf32, hi + lo split of the centred differences and of W_triu,

@@ -164,6 +164,12 @@ class LocallyAdaptiveKDE(VIModel, ABC):
 
     def _fused_step(self):
         eng = self.engine
+        if (getattr(self, "autotune", False) and self._eager_steps >= 1 and getattr(eng, "tuning", None) is None
+                and hasattr(eng, "kernel_launches")):
+            # after one eager iteration (every buffer allocated), before the capture
+            from .tuning import tune_engine
+
+            eng.tuning = tune_engine(eng)
         if self.cuda_graph and eng.graph is None and self._eager_steps >= 1:
             eng.capture()
         if eng.graph is not None:

@@ -28,8 +28,9 @@ class LocalHierarchicalKDE(LocallyAdaptiveKDE):
                  block_size: int = 512, nu_shared_0: Union[torch.Tensor, float] = None,
                  a_0: Union[torch.Tensor, float] = 1e-6, b_0: Union[torch.Tensor, float] = 1e-6, verbose=False,
                  logs=False, fused=False, candidates="knn", cuda_graph=True, candidate_counts=None,
-                 precision="auto"):
+                 precision="auto", autotune=True):
         super().__init__(nu_0, a_0, b_0, block_size, verbose, logs, fused, candidates, cuda_graph)
+        self.autotune = autotune
         self.k_or_knn_graph = k_or_knn_graph
         self.candidate_counts = candidate_counts
         self.precision = precision

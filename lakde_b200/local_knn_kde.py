@@ -40,15 +40,18 @@ class LocalKNearestKDE(LocallyAdaptiveKDE):
     Extra keyword arguments: ``fused`` (batch VI on a fixed pair pattern,
     default False = the reference's block schedule), ``candidates`` (the pair
     pattern of the fused path: "knn", "dense", "lists" + ``candidate_counts``,
-    or a PairPattern) and ``cuda_graph`` (replay fused iterations as a CUDA
-    graph).
+    or a PairPattern), ``cuda_graph`` (replay fused iterations as a CUDA
+    graph), ``precision`` ("auto", "mixed" or "fp32") and ``autotune`` (time
+    the library's launch choices on the first fused iteration and keep the
+    fastest; lakde_b200.tuning).
     """
 
     def __init__(self, nu_0: Union[torch.Tensor, float] = None, k_or_knn_graph: Union[torch.Tensor, int] = None,
                  block_size: int = 512, a_0: Union[torch.Tensor, float] = 1e-6, b_0: Union[torch.Tensor, float] = 1e-6,
                  verbose=False, logs=False, fused=False, candidates="knn", cuda_graph=True, candidate_counts=None,
-                 precision="auto"):
+                 precision="auto", autotune=True):
         super().__init__(nu_0, a_0, b_0, block_size, verbose, logs, fused, candidates, cuda_graph)
+        self.autotune = autotune
         self.k_or_knn_graph = k_or_knn_graph
         self.candidate_counts = candidate_counts
         self.precision = precision

@@ -298,8 +298,7 @@ def test_log_pred_density(K, D, dtype):
 
 # ------------------------------------------------------- fused per-row pass
 @pytest.mark.parametrize("D,dtype", [(2, np.float32), (5, np.float32), (8, np.float32), (2, np.float64),
-                                     (5, np.float64), (8, np.float64), (13, np.float32), (21, np.float32),
-                                     (43, np.float32), (63, np.float32)])
+                                     (5, np.float64), (8, np.float64)])
 def test_vi_rows_matches_unfused_composition(K, D, dtype):
     rng = np.random.default_rng(10 + D)
     N = 400
