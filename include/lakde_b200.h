@@ -409,6 +409,21 @@ LAKDE_API int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D,
                                            const void *T_tiles, void *trace,
                                            void *stream);
 
+/* Workspace bytes lakde_weighted_gram needs for dimension D. */
+LAKDE_API size_t lakde_weighted_gram_workspace(int64_t D);
+
+/*
+ * out [D, D] (float64, full symmetric) = sum_n w_n W_triu_n W_triu_n^T over
+ * N kernels, W_triu [N, D, D] upper (dtype F32/F64) and w [N]: the
+ * hierarchical model's shared-precision sum (lakde/local_hierarchical_kde.py:
+ * 293-297) in FP64 without a float64 copy of the factors; deterministic
+ * (fixed reduction order).
+ */
+LAKDE_API int lakde_weighted_gram(int dtype, int64_t N, int64_t D,
+                                  const void *W_triu, const void *w,
+                                  double *out, void *workspace,
+                                  size_t workspace_bytes, void *stream);
+
 /* Workspace bytes lakde_knn_elbo needs. */
 LAKDE_API size_t lakde_knn_elbo_workspace(void);
 

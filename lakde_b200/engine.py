@@ -453,10 +453,13 @@ class FusedHier(FusedVI):
         return self._sigma_bar, self._sigma_bar
 
     def _lambda_contrib(self, weights):
-        """sum_n w_n W_triu_n W_triu_n^T in float64 (lakde/local_hierarchical_kde.py:293-297)."""
-        N, D = self.N, self.D
-        A = (self.U.double() * weights.double().sqrt()[:, None, None]).permute(1, 0, 2).reshape(D, N * D)
-        return A @ A.T
+        """sum_n w_n W_triu_n W_triu_n^T in float64 (lakde/local_hierarchical_kde.py:293-297), one
+        library kernel over the model-dtype factors (fixed buffers: the step can be captured)."""
+        if getattr(self, "_gram_ws", None) is None:
+            self._gram_ws = torch.empty(int(K.nat.lib().lakde_weighted_gram_workspace(self.D)), dtype=torch.uint8,
+                                        device=self.device)
+            self._gram_out = torch.empty(self.D, self.D, dtype=torch.float64, device=self.device)
+        return K.weighted_gram(self.U, weights, out=self._gram_out, workspace=self._gram_ws)
 
     def init_summaries(self):
         """lakde/local_hierarchical_kde.py:198-258 at block_size = N."""

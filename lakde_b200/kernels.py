@@ -426,6 +426,22 @@ def posterior_factor_tiled(SP, D, jitter, eps, nu_0, a, b, out, logdet, info, T_
     )
 
 
+def weighted_gram(W_triu, w, out=None, workspace=None):
+    """sum_n w_n W_triu_n W_triu_n^T in float64, [D, D] (see include/lakde_b200.h)."""
+    nat.require_cuda(W_triu, w, out, op="weighted_gram")
+    N, D, _ = W_triu.shape
+    W_triu = W_triu.contiguous()
+    w = w.to(W_triu.dtype).contiguous()
+    out = torch.empty(D, D, dtype=torch.float64, device=W_triu.device) if out is None else out
+    need = int(nat.lib().lakde_weighted_gram_workspace(D))
+    if workspace is None or workspace.numel() < need:
+        workspace = torch.empty(need, dtype=torch.uint8, device=W_triu.device)
+    nat.check(nat.lib().lakde_weighted_gram(nat.dtype_code(W_triu), N, D, nat.ptr(W_triu), nat.ptr(w), nat.ptr(out),
+                                            nat.ptr(workspace), workspace.numel(), nat.stream_of(W_triu)),
+              "weighted_gram")
+    return out
+
+
 def knn_elbo(a, b, nu, logdet_W, logdet_sigma_0, mm, c, a_0, b_0, nu_0, D, out=None, workspace=None):
     """ELBO of LocalKNearestKDE in float64 as a 0-dim device tensor (see include/lakde_b200.h)."""
     nat.require_cuda(a, b, nu, logdet_W, logdet_sigma_0, mm, c, op="knn_elbo")

@@ -669,3 +669,17 @@ def test_bounded_wait_times_out_sets_err_and_the_engine_raises(K):
     assert int(err) == 0
     fin = np.isfinite(ref)
     np.testing.assert_allclose(lr.cpu().numpy()[fin], ref[fin], rtol=1e-4, atol=1e-3)
+
+
+@pytest.mark.parametrize("D,N,dtype", [(3, 500, np.float64), (21, 3000, np.float32), (43, 1000, np.float32),
+                                       (64, 777, np.float64), (43, 0, np.float32)])
+def test_weighted_gram_matches_fp64(K, D, N, dtype):
+    """sum_n w_n W_triu_n W_triu_n^T of the hierarchical shared precision
+    (lakde/local_hierarchical_kde.py:293-297) against a float64 einsum."""
+    rng = np.random.default_rng(D + N)
+    W = np.triu(rng.standard_normal((N, D, D))).astype(dtype)
+    w = rng.uniform(0.5, 30, N).astype(dtype)
+    out = K.weighted_gram(t(W), t(w)).cpu().numpy()
+    ref = np.einsum("n,nij,nkj->ik", w.astype(np.float64), W.astype(np.float64), W.astype(np.float64))
+    np.testing.assert_allclose(out, ref, rtol=1e-12, atol=1e-10 * max(1.0, np.abs(ref).max()))
+    np.testing.assert_array_equal(out, out.T)
