@@ -35,11 +35,16 @@
 //
 // Shared-memory operand layout (canonical, no swizzle; a core matrix is 8 rows
 // x 16 bytes = 8 x 4 tf32):
-//   tile   16 pair groups x 32 cores: core c < 16 holds dims 4c..4c+3 of the
-//          8 pairs' hi parts, core 16 + c the lo parts.  As the E-step A
-//          operand (K-major, M = pairs) LBO = 128 (next 4 dims), SBO = 4096
-//          (next 8 pairs); as the M-step A = [G_hi; G_lo]^T and B = G_hi
-//          (MN-major, K = pairs) SBO = 128 (next 4 dims), LBO = 4096.
+//   tile   E-step / predictive density: 16 pair groups x 32 cores: core
+//          c < 16 holds dims 4c..4c+3 of the 8 pairs' hi parts, core 16 + c
+//          the lo parts; the A operand (K-major, M = pairs): LBO = 128 (next
+//          4 dims), SBO = 4096 (next 8 pairs).
+//          M-step: G^T, rows = [hi dims 0..63; lo dims 0..63], K = pairs:
+//          core (row group r / 8, pair quad p / 4) at (r / 8) GT_SBO +
+//          (p / 4) 128; A = [G_hi; G_lo]^T (M = 128) and B = G_hi (its first
+//          N rows) are both K-major with LBO = 128 (next 4 pairs) and SBO =
+//          GT_SBO (next 8 rows); GT_SBO = 4112 rather than 4096 keeps the
+//          converters' 16-byte stores on distinct bank groups.
 //   B      W cores (K-major, N = output dim i, K = input dim j, element (i, j)
 //          = W_triu[j][i] = X[i][j] with X = L^-1 lower): per K step J the row
 //          groups I = 0..NT-1 of 2 cores each, LBO = 128, SBO = 256.
@@ -54,6 +59,7 @@ constexpr int RAW_STRIDE = 256;  // bytes per staged pair row (D <= 64 floats)
 constexpr uint32_t kSpinLimit = 1u << 26;
 constexpr uint64_t kWaitLimitNs = 1500000000ull;  // 1.5 s: far above any copy or MMA of one tile
 constexpr int PQ = 2048;       // queries per predictive-density launch
+constexpr uint32_t GT_SBO = 4112;  // M-step tile: bytes between 8-row groups of G^T
 
 enum Mode { ESTEP = 0, MSTEP = 1, PRED = 2 };
 
@@ -217,8 +223,8 @@ struct Args {
 // Shared memory of one CTA.  The B stages of the E-step / predictive density
 // double as the accumulator copy of the M-step's epilogue.
 struct Smem {
-  static constexpr uint32_t TILE = 0;                                   // 64 KB
-  static constexpr uint32_t RAW = TILE + 16 * 4096;                     // 2 x 32 KB
+  static constexpr uint32_t TILE = 0;                                   // 64 KB (M-step: 16 x GT_SBO)
+  static constexpr uint32_t RAW = TILE + 16 * GT_SBO;                   // 2 x 32 KB
   static constexpr uint32_t BST = RAW + 2 * MT * RAW_STRIDE;            // 2 x (hi 16 KB + lo 16 KB)
   static constexpr uint32_t B_BYTES = 16384;
   static constexpr uint32_t RSTR = 68;                                  // M-step accumulator copy row stride
@@ -425,15 +431,54 @@ struct Kern {
     const unsigned char *raw = sm + Smem::RAW + (uint32_t)s * MT * RAW_STRIDE;
     const float4 *xn = reinterpret_cast<const float4 *>(sm + Smem::XN + ms * 256);
     unsigned char *tile = sm + Smem::TILE;
-    const int p = tid & (MT - 1), h = tid >> 7;
     const int D = g.D;
-    const int cvalid = (p < meta.cnt) ? cidx[p] : -1;
     const int rch = (D + 3) / 4;  // chunks present in a staged row
-    float w = 1.f;
     if (MODE == MSTEP) {
-      const float rr = cvalid >= 0 ? rv[p] : 0.f;
-      w = sqrtf(rr > 0.f ? rr : 0.f);
+      // G^T: unit (pair quad q, dim chunk k) reads the chunk of its 4 pairs
+      // (consecutive units: consecutive chunks, distinct bank groups), forms
+      // sqrt(r) (x_m - x_n), and writes per dim the 4 pairs as one 16-byte
+      // row of a core, hi at row d, lo at row 64 + d
+#pragma unroll
+      for (int s2 = 0; s2 < 2; ++s2) {
+        const int u = tid + NTHR * s2;
+        const int q = u >> 4, k = u & 15;
+        float4 dq[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int p = 4 * q + i;
+          const int c = (p < meta.cnt) ? cidx[p] : -1;
+          float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (c >= 0 && k < rch) {
+            const float rr = rv[p];
+            const float w = sqrtf(rr > 0.f ? rr : 0.f);
+            const float4 x = *reinterpret_cast<const float4 *>(raw + p * RAW_STRIDE + k * 16);
+            const float4 cc = xn[k];
+            const int d0 = 4 * k;
+            d.x = (x.x - cc.x) * w;
+            d.y = (d0 + 1 < D) ? (x.y - cc.y) * w : 0.f;
+            d.z = (d0 + 2 < D) ? (x.z - cc.z) * w : 0.f;
+            d.w = (d0 + 3 < D) ? (x.w - cc.w) * w : 0.f;
+          }
+          dq[i] = d;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const float4 v = j == 0   ? make_float4(dq[0].x, dq[1].x, dq[2].x, dq[3].x)
+                           : j == 1 ? make_float4(dq[0].y, dq[1].y, dq[2].y, dq[3].y)
+                           : j == 2 ? make_float4(dq[0].z, dq[1].z, dq[2].z, dq[3].z)
+                                    : make_float4(dq[0].w, dq[1].w, dq[2].w, dq[3].w);
+          float4 hi, lo;
+          split4(v, hi, lo);
+          const int r = 4 * k + j;
+          unsigned char *o = tile + (uint32_t)(r >> 3) * GT_SBO + (uint32_t)q * 128u + (uint32_t)(r & 7) * 16u;
+          *reinterpret_cast<float4 *>(o) = hi;
+          *reinterpret_cast<float4 *>(o + 8 * GT_SBO) = lo;
+        }
+      }
+      return;
     }
+    const int p = tid & (MT - 1), h = tid >> 7;
+    const int cvalid = (p < meta.cnt) ? cidx[p] : -1;
     unsigned char *dst = tile + (uint32_t)(p >> 3) * 4096u + (uint32_t)(p & 7) * 16u;
 #pragma unroll
     for (int i = 0; i < HCH; ++i) {
@@ -447,12 +492,6 @@ struct Kern {
         d.y = (d0 + 1 < D) ? x.y - c.y : 0.f;
         d.z = (d0 + 2 < D) ? x.z - c.z : 0.f;
         d.w = (d0 + 3 < D) ? x.w - c.w : 0.f;
-        if (MODE == MSTEP) {
-          d.x *= w;
-          d.y *= w;
-          d.z *= w;
-          d.w *= w;
-        }
       }
       float4 hi, lo;
       split4(d, hi, lo);
@@ -488,14 +527,14 @@ struct Kern {
                                                    uint32_t acc_sel, uint64_t *mma_done) {
     const uint32_t tile = smem_u32(sm + Smem::TILE);
     if (MODE == MSTEP) {
-      // [H; B] (+)= [G_hi; G_lo]^T G_hi over the tile's pair groups
-      const uint32_t idesc = idesc_tf32(128, DP, 1, 1);
+      // [H; B] (+)= [G_hi; G_lo]^T G_hi over the tile's pairs, 8 per MMA
+      const uint32_t idesc = idesc_tf32(128, DP, 0, 0);
       const uint32_t td = tmem + acc_sel * 64u;
       const int ng = (meta.cnt + 7) / 8;
       for (int gi = 0; gi < ng; ++gi) {
-        const uint32_t a = tile + (uint32_t)gi * 4096u;
+        const uint32_t a = tile + (uint32_t)gi * 256u;
         const uint32_t acc = ((meta.flags & 1) && gi == 0) ? 0u : 1u;
-        mma_tf32(td, desc(a, 4096, 128), desc(a, 4096, 128), idesc, acc);
+        mma_tf32(td, desc(a, 128, GT_SBO), desc(a, 128, GT_SBO), idesc, acc);
       }
     } else {
       const uint32_t idesc = idesc_tf32(128, DP, 0, 0);

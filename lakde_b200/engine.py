@@ -226,10 +226,10 @@ class FusedVI:
     # ------------------------------------------------------------ prediction
     def log_pred_density(self, Y):
         """lakde/local_adaptive_kde.py:200-223: posterior from the current r, then
-        the fused Student-t mixture kernel.  The mixed path recomputes S and the
-        factorisation into the buffers the next iteration overwrites first (the
-        S halves of SP, or S, and the W cores), so it allocates no per-kernel
-        matrices; nu and logdet_W of the model are left as they are."""
+        the fused Student-t mixture kernel.  S and the factorisation are
+        recomputed into buffers the next iteration overwrites first (the S
+        halves of SP or S, and the W cores or W_triu), so no per-kernel matrices
+        are allocated; nu and logdet_W of the model are left as they are."""
         nu = torch.empty_like(self.nu)
         logdet = torch.empty_like(self.logdet_W)
         info = torch.empty_like(self.info)
@@ -250,15 +250,14 @@ class FusedVI:
             torch.minimum(self.failed, info.min(), out=self.failed)
             lc = K.pred_coeff(nu, logdet, self.D)
             return K.log_pred_density_tc(self.Xp, self.Wc, nu, lc, Y.to(self.dtype), self.err)
-        S = torch.empty_like(self.S)
-        K.mstep(rowptr, col, self.r, self.X, self.nu_0, S=S, nu=nu)
+        # S and W_triu into the engine's own buffers (the next step rewrites them first)
+        K.mstep(rowptr, col, self.r, self.X, self.nu_0, S=self.S, nu=nu)
         P, _ = self._prior()
-        W, logdet, info, _, _ = K.posterior_factor(S, self.W_inv_jitter, self.eps, P=P, nu_0=self.nu_0_t, a=self.a,
-                                                   b=self.b, logdet=logdet, info=info)
-        del S
+        K.posterior_factor(self.S, self.W_inv_jitter, self.eps, P=P, nu_0=self.nu_0_t, a=self.a, b=self.b,
+                           logdet=logdet, info=info, out=self.U)
         torch.minimum(self.failed, info.min(), out=self.failed)
         lc = K.pred_coeff(nu, logdet, self.D)
-        return K.log_pred_density(self.X, W, nu, lc, Y.to(self.dtype))
+        return K.log_pred_density(self.X, self.U, nu, lc, Y.to(self.dtype))
 
     def posterior_factors(self):
         """(W_triu, nu, logdet_W) as log_pred_density recomputes them."""

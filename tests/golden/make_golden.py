@@ -195,16 +195,18 @@ def model_fixtures():
 
 
 def state_to_arrays(state, prefix="state_"):
-    """A reference state dict as flat npz arrays (rnm_blocks block by block)."""
+    """A reference state dict as flat npz arrays (rnm_blocks block by block),
+    copied: the reference's state dict holds its live tensors, which a
+    continued fit updates in place."""
     out = {}
     for key, v in state.items():
         if key == "rnm_blocks":
             out[prefix + "rnm_nblocks"] = np.array(len(v))
             for bi, (ind, val) in enumerate(v):
-                out[f"{prefix}rnm_b{bi}_ind"] = t2n(ind)
-                out[f"{prefix}rnm_b{bi}_val"] = t2n(val)
+                out[f"{prefix}rnm_b{bi}_ind"] = t2n(ind).copy()
+                out[f"{prefix}rnm_b{bi}_val"] = t2n(val).copy()
         elif torch.is_tensor(v):
-            out[prefix + key] = t2n(v)
+            out[prefix + key] = t2n(v).copy()
         else:
             out[prefix + key] = np.array(v)
     return out

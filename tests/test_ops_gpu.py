@@ -651,7 +651,8 @@ def test_bounded_wait_times_out_sets_err_and_the_engine_raises(K):
     out = torch.zeros(len(cols), device=DEV)
     Xt = t(X)
     graph = torch.tensor(O.knn_graph(X, 8).astype(np.int32), device=DEV)
-    eng = FusedKNN(Xt, graph, PairPattern.from_knn_graph(graph), float(D), 1e-6, 1e-6, 0.0, 8)
+    tiny = torch.tensor(1e-6, device=DEV)
+    eng = FusedKNN(Xt, graph, PairPattern.from_knn_graph(graph), float(D), tiny, tiny, 0.0, 8)
     eng.check_errors()
     st = nat.lib().lakde_tc_wait_timeout_probe(N, D, N, nat.ptr(t(rowptr)), nat.ptr(t(cols, torch.int32)),
                                                nat.ptr(Xp), Xp.stride(0), nat.ptr(Wc), nat.ptr(nu), nat.ptr(logdet),
