@@ -67,8 +67,15 @@ LAKDE_API int lakde_max_dim(void);
  *                          that stage no T and write no L (else 0 is used).
  *   LAKDE_TUNE_ROWS:   0 = tensor-core rows from the caller's work queue;
  *                      1 = a static stride over the grid (the queue ignored).
+ *   LAKDE_TUNE_VI_ROWS: 0 = lakde_vi_rows with 8 lanes per kernel row;
+ *                      1 = one thread per kernel row.
  */
-typedef enum { LAKDE_TUNE_FACTOR = 0, LAKDE_TUNE_ROWS = 1, LAKDE_TUNE_KNOBS = 2 } lakde_tune_knob;
+typedef enum {
+  LAKDE_TUNE_FACTOR = 0,
+  LAKDE_TUNE_ROWS = 1,
+  LAKDE_TUNE_VI_ROWS = 2,
+  LAKDE_TUNE_KNOBS = 3
+} lakde_tune_knob;
 LAKDE_API int lakde_tuning_set(int knob, int64_t D, int value);
 LAKDE_API int lakde_tuning_get(int knob, int64_t D);
 

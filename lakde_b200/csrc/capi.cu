@@ -75,7 +75,7 @@ int tuning(int knob, int64_t D) {
 
 extern "C" int lakde_tuning_set(int knob, int64_t D, int value) {
   lakde::clear_error();
-  static const int kChoices[LAKDE_TUNE_KNOBS] = {2, 2};
+  static const int kChoices[LAKDE_TUNE_KNOBS] = {2, 2, 2};
   if (knob < 0 || knob >= LAKDE_TUNE_KNOBS || D < 1 || D > lakde::kMaxDim || value < 0 || value >= kChoices[knob]) {
     lakde::set_error("tuning_set: knob %d at D=%lld has no choice %d", knob, (long long)D, value);
     return LAKDE_EINVAL;

@@ -133,6 +133,84 @@ __device__ __forceinline__ bool chol_rows(const T (&S)[DP * (DP + 1) / 2], const
   return ok;
 }
 
+// The per-kernel part of the pass, from the row's scatter S and nu: the
+// posterior A = nu_0 a_n / b_n P_n + S + jitter I in FP64 with the jitter
+// ladder, logdet_W = -2 sum log L_ii, the trace ||L^-1 T_n||_F^2 by forward
+// substitution, mm = nu trace and the b update; writes the per-kernel
+// outputs (NaN when the ladder failed or the row had an invalid index) and
+// returns whether L holds a factor.
+template <typename T, int DP>
+__device__ __forceinline__ bool row_posterior(const RowArgs<T> &g, int64_t n, const T (&S)[DP * (DP + 1) / 2], T nu,
+                                              bool bad, double (&L)[DP * (DP + 1) / 2], T &logdet) {
+  constexpr int TT = DP * (DP + 1) / 2;
+  const int D = g.D;
+  const T b_old = g.b[n];
+  const T scale = f_mul(g.nu0, f_div(g.a[n], b_old));
+  // the lower triangle of P_n, row by row (vector loads for D == DP)
+  T Pv[TT];
+  const bool has_p = g.P != nullptr;
+  if (has_p) {
+    const T *P = g.P + n * g.Pbs;
+#pragma unroll
+    for (int i = 0; i < DP; ++i) {
+      T row[DP];
+      load_row<T, DP>(P, i, D, row);
+#pragma unroll
+      for (int j = 0; j <= i; ++j) Pv[tix<DP>(i, j)] = i < D ? row[j] : T(0);
+    }
+  }
+  T jit = g.jitter[n];
+  bool ok = chol_rows<T, DP>(S, Pv, has_p, scale, jit, D, L);
+  if (!ok) {
+    T jt = T(0);
+    for (int k = 0; k < 32 && !ok; ++k) {
+      jt = f_add(jt, (T)(g.eps * ldexp(1.0, k)));
+      ok = chol_rows<T, DP>(S, Pv, has_p, scale, jt, D, L);
+      if (ok) jit = jt;
+    }
+  }
+  ok = ok && !bad;
+
+  // logdet of W = 2 sum log W_triu_ii, W_triu_ii = 1 / L_ii (in the model dtype)
+  double ld = 0.0;
+#pragma unroll
+  for (int i = 0; i < DP; ++i)
+    if (i < D) ld += log((double)(T)(1.0 / L[tix<DP>(i, i)]));
+  logdet = (T)(2.0 * ld);
+
+  // trace ||L^-1 T_n||_F^2 by forward substitution of each column of T_n
+  // (a column at a time: the whole T_n would not stay in registers)
+  double tr = 0.0;
+  if (g.Tm) {
+    const T *Tn = g.Tm + n * g.Tbs;
+#pragma unroll
+    for (int a = 0; a < DP; ++a) {
+      if (a >= D) continue;
+      T tc[DP];
+#pragma unroll
+      for (int i = 0; i < DP; ++i) tc[i] = i < D ? Tn[i * D + a] : T(0);
+      double z[DP];
+#pragma unroll
+      for (int i = 0; i < DP; ++i) {
+        double s = (double)tc[i];
+#pragma unroll
+        for (int j = 0; j < i; ++j) s -= L[tix<DP>(i, j)] * z[j];
+        z[i] = s / L[tix<DP>(i, i)];
+        tr += z[i] * z[i];
+      }
+    }
+  }
+  const T mm = nu * (T)tr;
+  const T nanv = T(NAN);
+  g.jitter[n] = jit;
+  g.info[n] = ok ? 0 : -1;
+  g.nu_out[n] = ok ? nu : nanv;
+  g.logdet_out[n] = ok ? logdet : nanv;
+  if (g.mm_out) g.mm_out[n] = ok ? mm : nanv;
+  if (g.Tm) g.b[n] = ok ? g.b0 + g.nu0 * mm / T(2) : nanv;
+  return ok;
+}
+
 // float32 with D <= 8: three blocks per SM (168 registers, a few spills to
 // L1) hide the pair gathers better than two (0.372 -> 0.329 ms per launch on
 // 200,000 rows, K = 50; four blocks spill too much)
@@ -194,72 +272,10 @@ __global__ void __launch_bounds__(128, (sizeof(T) == 4 && DP == 8) ? 3 : 1) vi_r
     }
   }
   const T nu = g.nu0 + vsum;
-
-  // ------------------------------------------------------------- posterior
-  const T b_old = g.b[n];
-  const T scale = f_mul(g.nu0, f_div(g.a[n], b_old));
-  // the lower triangle of P_n, row by row (vector loads for D == DP)
-  T Pv[TT];
-  const bool has_p = g.P != nullptr;
-  if (has_p) {
-    const T *P = g.P + n * g.Pbs;
-#pragma unroll
-    for (int i = 0; i < DP; ++i) {
-      T row[DP];
-      load_row<T, DP>(P, i, D, row);
-#pragma unroll
-      for (int j = 0; j <= i; ++j) Pv[tix<DP>(i, j)] = i < D ? row[j] : T(0);
-    }
-  }
-  T jit = g.jitter[n];
   double L[TT];
-  bool ok = chol_rows<T, DP>(S, Pv, has_p, scale, jit, D, L);
-  if (!ok) {
-    T jt = T(0);
-    for (int k = 0; k < 32 && !ok; ++k) {
-      jt = f_add(jt, (T)(g.eps * ldexp(1.0, k)));
-      ok = chol_rows<T, DP>(S, Pv, has_p, scale, jt, D, L);
-      if (ok) jit = jt;
-    }
-  }
-  ok = ok && !bad;
-
-  // logdet of W = 2 sum log W_triu_ii, W_triu_ii = 1 / L_ii (in the model dtype)
-  double ld = 0.0;
-#pragma unroll
-  for (int i = 0; i < DP; ++i)
-    if (i < D) ld += log((double)(T)(1.0 / L[tix<DP>(i, i)]));
-  const T logdet = (T)(2.0 * ld);
-
-  // trace ||L^-1 T_n||_F^2 by forward substitution of each column of T_n
-  double tr = 0.0;
-  if (g.Tm) {
-    const T *Tn = g.Tm + n * g.Tbs;
-    T Tv[DP][DP];
-#pragma unroll
-    for (int i = 0; i < DP; ++i) load_row<T, DP>(Tn, i, D, Tv[i]);
-#pragma unroll
-    for (int a = 0; a < DP; ++a) {
-      if (a >= D) continue;
-      double z[DP];
-#pragma unroll
-      for (int i = 0; i < DP; ++i) {
-        double s = i < D ? (double)Tv[i][a] : 0.0;
-#pragma unroll
-        for (int j = 0; j < i; ++j) s -= L[tix<DP>(i, j)] * z[j];
-        z[i] = s / L[tix<DP>(i, i)];
-        tr += z[i] * z[i];
-      }
-    }
-  }
-  const T mm = nu * (T)tr;
+  T logdet;
+  const bool ok = row_posterior<T, DP>(g, n, S, nu, bad, L, logdet);
   const T nanv = T(NAN);
-  g.jitter[n] = jit;
-  g.info[n] = ok ? 0 : -1;
-  g.nu_out[n] = ok ? nu : nanv;
-  g.logdet_out[n] = ok ? logdet : nanv;
-  if (g.mm_out) g.mm_out[n] = ok ? mm : nanv;
-  if (g.Tm) g.b[n] = ok ? g.b0 + g.nu0 * mm / T(2) : nanv;
 
   // ---------------------------------------------------------------- E-step
   T Lf[TT], rinv[DP];
@@ -309,6 +325,161 @@ __global__ void __launch_bounds__(128, (sizeof(T) == 4 && DP == 8) ? 3 : 1) vi_r
       T lr = f_add(f_mul(q, expo), cst);
       if (c[u] == n + g.koff) lr = neg_inf<T>();
       g.logrho[p0 + u] = lr;
+    }
+  }
+}
+
+// The same pass with a kernel row per group of LPR lanes (4 rows per warp):
+// the row's pairs are dealt to the lanes (pair start + l + LPR k to lane l),
+// so a lane gathers a few point rows instead of the whole row's, in batches of
+// B whose gathers are all in flight together.  Each lane accumulates its share
+// of S_n and of sum r; an xor butterfly over the group sums them (every lane
+// ends with the same bits, in a fixed order).  Lane 0 of the group factorises
+// and writes the per-kernel outputs, then broadcasts the factor's pieces;
+// every lane then gathers its pairs again (mostly L2 hits by then) and
+// computes their log rho.  Only S is live across the factorisation.
+template <typename T, int DP, int LPR, int B>
+__global__ void __launch_bounds__(128, 3) vi_rows_lanes_kernel(RowArgs<T> g) {
+  constexpr int TT = DP * (DP + 1) / 2;
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31, sub = lane & (LPR - 1), leader = lane & ~(LPR - 1);
+  const int64_t it = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / LPR;
+  const bool live = it < g.N;
+  const int64_t n = live ? (g.order ? (int64_t)g.order[it] : it) : 0;
+  const int D = g.D;
+  int64_t start = 0, end = 0;
+  if (live) {
+    start = g.rowptr[n];
+    end = g.rowptr[n + 1];
+  }
+  int bad = end < start;
+  if (bad) end = start;
+
+  T xn[DP];
+  load_row<T, DP>(g.X, n + g.koff, D, xn);
+
+  // ---------------------------------------------------------------- M-step
+  T S[TT];
+#pragma unroll
+  for (int e = 0; e < TT; ++e) S[e] = T(0);
+  T vsum = T(0);
+  for (int64_t p0 = start + sub; p0 < end; p0 += (int64_t)LPR * B) {
+    int32_t c[B];
+    T v[B];
+#pragma unroll
+    for (int k = 0; k < B; ++k) {
+      const int64_t p = p0 + (int64_t)LPR * k;
+      c[k] = -1;
+      v[k] = T(0);
+      if (p < end) {
+        c[k] = g.col[p];
+        v[k] = g.r[p];
+        if (c[k] < 0 || c[k] >= g.npts) {
+          bad = 1;
+          c[k] = -1;
+        }
+      }
+    }
+    T dl[B][DP];
+#pragma unroll
+    for (int k = 0; k < B; ++k) {
+      load_row<T, DP>(g.X, c[k] < 0 ? 0 : c[k], D, dl[k]);
+#pragma unroll
+      for (int d = 0; d < DP; ++d) dl[k][d] = (c[k] >= 0 && d < D) ? dl[k][d] - xn[d] : T(0);
+    }
+#pragma unroll
+    for (int k = 0; k < B; ++k) {
+      if (c[k] < 0) continue;
+#pragma unroll
+      for (int i = 0; i < DP; ++i) {
+        const T vi = v[k] * dl[k][i];
+#pragma unroll
+        for (int j = 0; j <= i; ++j) S[tix<DP>(i, j)] = fma(vi, dl[k][j], S[tix<DP>(i, j)]);
+      }
+      vsum += v[k];
+    }
+  }
+  // group sums (xor butterfly: the same bits in every lane of the group)
+#pragma unroll
+  for (int off = LPR / 2; off >= 1; off >>= 1) {
+#pragma unroll
+    for (int e = 0; e < TT; ++e) S[e] += __shfl_xor_sync(FULL, S[e], off, LPR);
+    vsum += __shfl_xor_sync(FULL, vsum, off, LPR);
+    bad |= __shfl_xor_sync(FULL, bad, off, LPR);
+  }
+
+  // ------------------------------------------------------- posterior, lane 0
+  T Lf[TT], rinv[DP];
+  T cst = T(0), expo = T(0);
+  int ok = 0;
+  const T nu = g.nu0 + vsum;
+  if (sub == 0 && live) {
+    double L[TT];
+    T logdet;
+    ok = row_posterior<T, DP>(g, n, S, nu, bad != 0, L, logdet) ? 1 : 0;
+#pragma unroll
+    for (int i = 0; i < DP; ++i) {
+#pragma unroll
+      for (int j = 0; j < i; ++j) Lf[tix<DP>(i, j)] = (T)L[tix<DP>(i, j)];
+      rinv[i] = (T)(1.0 / L[tix<DP>(i, i)]);
+    }
+    const double e = mvdigamma_d(0.5 * (double)nu, D) + D * 0.69314718055994530942 + (double)logdet;
+    cst = (T)(0.5 * e);
+    expo = T(-0.5) * nu;
+  }
+  // broadcast from the group's lane 0
+  ok = __shfl_sync(FULL, ok, leader);
+  cst = __shfl_sync(FULL, cst, leader);
+  expo = __shfl_sync(FULL, expo, leader);
+#pragma unroll
+  for (int i = 0; i < DP; ++i) {
+#pragma unroll
+    for (int j = 0; j < i; ++j) Lf[tix<DP>(i, j)] = __shfl_sync(FULL, Lf[tix<DP>(i, j)], leader);
+    rinv[i] = __shfl_sync(FULL, rinv[i], leader);
+  }
+  if (!live) return;
+
+  // ---------------------------------------------------------------- E-step
+  const T nanv = T(NAN);
+  for (int64_t p0 = start + sub; p0 < end; p0 += (int64_t)LPR * B) {
+    int32_t c[B];
+#pragma unroll
+    for (int k = 0; k < B; ++k) {
+      const int64_t p = p0 + (int64_t)LPR * k;
+      c[k] = -1;
+      if (p < end) {
+        c[k] = g.col[p];
+        if (!ok || c[k] < 0 || c[k] >= g.npts) c[k] = -2;
+      }
+    }
+    T dl[B][DP];
+#pragma unroll
+    for (int k = 0; k < B; ++k) {
+      load_row<T, DP>(g.X, c[k] < 0 ? 0 : c[k], D, dl[k]);
+#pragma unroll
+      for (int d = 0; d < DP; ++d) dl[k][d] = (c[k] >= 0 && d < D) ? dl[k][d] - xn[d] : T(0);
+    }
+#pragma unroll
+    for (int k = 0; k < B; ++k) {
+      const int64_t p = p0 + (int64_t)LPR * k;
+      if (c[k] == -1) continue;  // past the end of the row
+      if (c[k] == -2) {
+        g.logrho[p] = nanv;
+        continue;
+      }
+      T y[DP];
+      T q = T(0);
+#pragma unroll
+      for (int i = 0; i < DP; ++i) {
+        T s2 = dl[k][i];
+#pragma unroll
+        for (int j = 0; j < i; ++j) s2 = fma(-Lf[tix<DP>(i, j)], y[j], s2);
+        y[i] = s2 * rinv[i];
+        q = fma(y[i], y[i], q);
+      }
+      T lr = f_add(f_mul(q, expo), cst);
+      if (c[k] == n + g.koff) lr = neg_inf<T>();
+      g.logrho[p] = lr;
     }
   }
 }
@@ -367,13 +538,30 @@ extern "C" int lakde_vi_rows(int dtype, int64_t N, int64_t D, int64_t npts, cons
     g.N = N;
     g.koff = kernel_offset;
     g.D = (int)D;
-    const unsigned blocks = (unsigned)((N + 127) / 128);
+    if (tuning(LAKDE_TUNE_VI_ROWS, D) == 1) {
+      // a thread per row
+      const unsigned blocks = (unsigned)((N + 127) / 128);
+      if (D <= 2)
+        vi_rows_kernel<TT, 2><<<blocks, 128, 0, as_stream(stream)>>>(g);
+      else if (D <= 4)
+        vi_rows_kernel<TT, 4><<<blocks, 128, 0, as_stream(stream)>>>(g);
+      else
+        vi_rows_kernel<TT, 8><<<blocks, 128, 0, as_stream(stream)>>>(g);
+      return check_launch("vi_rows");
+    }
+    // 8 lanes per row (16 rows per 128-thread block)
+    constexpr int LPR = 8, B = sizeof(TT) == 4 ? 4 : 2;
+    const int64_t blocks = (N * LPR + 127) / 128;
+    if (blocks > 0x7fffffffLL) {
+      set_error("vi_rows: too many rows");
+      return (int)LAKDE_EUNSUPPORTED;
+    }
     if (D <= 2)
-      vi_rows_kernel<TT, 2><<<blocks, 128, 0, as_stream(stream)>>>(g);
+      vi_rows_lanes_kernel<TT, 2, LPR, B><<<(unsigned)blocks, 128, 0, as_stream(stream)>>>(g);
     else if (D <= 4)
-      vi_rows_kernel<TT, 4><<<blocks, 128, 0, as_stream(stream)>>>(g);
+      vi_rows_lanes_kernel<TT, 4, LPR, B><<<(unsigned)blocks, 128, 0, as_stream(stream)>>>(g);
     else
-      vi_rows_kernel<TT, 8><<<blocks, 128, 0, as_stream(stream)>>>(g);
+      vi_rows_lanes_kernel<TT, 8, LPR, B><<<(unsigned)blocks, 128, 0, as_stream(stream)>>>(g);
     return check_launch("vi_rows");
   });
 }
