@@ -264,19 +264,14 @@ LAKDE_API int lakde_pack_w_cores(int dtype, int64_t N, int64_t D,
  * Tensor-core E-step: the logrho of lakde_estep_logrho for rows n = 0..N-1,
  * row n being kernel n + kernel_offset of X [npts, ldx], W_triu given as W
  * cores (16-byte aligned).  Restates lakde/local_adaptive_kde.py:36-44 on a
- * pair pattern.  With r [nnz] and rq_sum [N] (both or neither) it also writes
- * rq_sum_n = sum_p r_p Q_p over row n, Q_p the quad form of pair p: with
- * A_n = c_n P_n + S_n + j_n I factorised (S_n from the same r) this is
- * tr(S_n W_n), so tr(P_n W_n) = (D - rq_sum_n - j_n tr(W_n)) / c_n without a
- * further product of the factors.
+ * pair pattern.
  */
 LAKDE_API int lakde_estep_tc(int dtype, int64_t N, int64_t D, int64_t npts,
                              const void *rowptr, const void *col,
                              const void *order, const void *X, int64_t ldx,
                              int64_t kernel_offset, const void *W_cores,
                              const void *nu, const void *logdet_W, void *logrho,
-                             const void *r, void *rq_sum, int32_t *queue,
-                             int32_t *err, void *stream);
+                             int32_t *queue, int32_t *err, void *stream);
 
 /*
  * Tensor-core M-step: S_n and nu_n of lakde_mstep for rows n = 0..N-1, row n
@@ -402,8 +397,7 @@ LAKDE_API int lakde_mstep_tc_tiled(int dtype, int64_t N, int64_t D, int64_t npts
  * lakde_posterior_factor (no L), W_triu dense [N, D, D], X_tiles:
  * X_n = L_n^-1 = W_triu_n^T as lower tiles (64 * tiles floats per kernel)
  * and / or W_cores (16-byte aligned, lakde_w_cores_floats(D) floats per
- * kernel; NaN for a failed matrix); any two may be NULL.  X_norm2 [N]
- * (optional, with W_cores): ||X_n||_F^2 = tr(W_n) from the FP64 factor.  info_n = -2 marks a matrix whose
+ * kernel; NaN for a failed matrix); any two may be NULL.  info_n = -2 marks a matrix whose
  * input copy did not complete within the wait limit.
  */
 LAKDE_API int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D,
@@ -411,10 +405,9 @@ LAKDE_API int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D,
                                            const void *a, const void *b,
                                            void *jitter, double eps,
                                            void *W_triu, void *X_tiles,
-                                           void *W_cores, void *X_norm2,
-                                           void *logdet_W, int32_t *info,
-                                           const void *T_tiles, void *trace,
-                                           void *stream);
+                                           void *W_cores, void *logdet_W,
+                                           int32_t *info, const void *T_tiles,
+                                           void *trace, void *stream);
 
 /* Workspace bytes lakde_weighted_gram needs for dimension D. */
 LAKDE_API size_t lakde_weighted_gram_workspace(int64_t D);

@@ -58,7 +58,7 @@ _SIGNATURES = {
     ),
     "lakde_estep_tc": (
         [_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp,
-         _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
+         _c_vp, _c_vp, _c_vp],
         _c_int,
     ),
     "lakde_mstep_tc": (
@@ -110,7 +110,7 @@ _SIGNATURES = {
     ),
     "lakde_posterior_factor_tiled": (
         [_c_int, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
-         _c_vp, _c_vp, _c_vp, _c_vp],
+         _c_vp, _c_vp, _c_vp],
         _c_int,
     ),
     "lakde_knn_elbo": (

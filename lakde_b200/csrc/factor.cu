@@ -40,7 +40,6 @@ struct FactorArgs {
   // optional output: X = L^-1 (= W_triu^T) as the W cores of the tensor-core
   // E-step's B operand, 64 floats per tile (layout at lakde_pack_w_cores)
   float *Wc;
-  float *xnorm2;  // optional with Wc: ||X_n||_F^2 = tr(W_n), from the FP64 tiles
   int64_t N;
   int D;
 };
@@ -475,7 +474,6 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
       for (int e = lane; e < C::NTILE * 64; e += 32) Xt[e] = NAN;
     if (Wc)
       for (int e = lane; e < C::NTILE * 64; e += 32) Wc[e] = NAN;
-    if (g.xnorm2 && lane == 0) g.xnorm2[n] = NAN;
     if (lane == 0) {
       g.logdet[n] = nanv;
       if (g.Tm || g.Tt) g.trace[n] = nanv;
@@ -515,7 +513,6 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
     // writes row l / 4, column l % 4 of a core, so a warp store is one
     // contiguous 128-byte core.  Rows i >= D (the identity padding) are zero.
     const int rr = lane >> 2, cc = lane & 3;
-    double x2 = 0.0;
 #pragma unroll
     for (int J = 0; J < NT; ++J) {
       float *seg = Wc + 64 * (J * NT - J * (J - 1) / 2);
@@ -525,16 +522,10 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const int j = 8 * J + 4 * h + cc;
-          double v = M[dmma::tix(I, J) + rr * 8 + 4 * h + cc];
-          v = (i < D && j <= i) ? v : 0.0;
-          x2 = fma(v, v, x2);
-          seg[(I - J) * 64 + h * 32 + lane] = (float)v;
+          const double v = M[dmma::tix(I, J) + rr * 8 + 4 * h + cc];
+          seg[(I - J) * 64 + h * 32 + lane] = (i < D && j <= i) ? (float)v : 0.f;
         }
       }
-    }
-    if (g.xnorm2) {
-      x2 = warp_sum(x2);
-      if (lane == 0) g.xnorm2[n] = (float)x2;
     }
   }
   // W_triu = X^T: W tile (J, I) = X_IJ^T for I >= J, zero below; lanes write
@@ -832,8 +823,8 @@ extern "C" int lakde_pack_tiles(int dtype, int64_t N, int64_t D, const void *src
 
 extern "C" int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D, const void *SP, const void *nu_0,
                                             const void *a, const void *b, void *jitter, double eps, void *W_triu,
-                                            void *X_tiles, void *W_cores, void *X_norm2, void *logdet_W,
-                                            int32_t *info, const void *T_tiles, void *trace, void *stream) {
+                                            void *X_tiles, void *W_cores, void *logdet_W, int32_t *info,
+                                            const void *T_tiles, void *trace, void *stream) {
   clear_error();
   if (dtype != LAKDE_F32) {
     set_error("posterior_factor_tiled: float32 values only");
@@ -845,7 +836,7 @@ extern "C" int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D, con
   }
   if (N == 0) return LAKDE_OK;
   if (!SP || !nu_0 || !a || !b || !jitter || (!W_triu && !X_tiles && !W_cores) || !logdet_W || !info ||
-      (T_tiles && !trace) || (X_norm2 && !W_cores)) {
+      (T_tiles && !trace)) {
     set_error("posterior_factor_tiled: missing buffer");
     return LAKDE_EINVAL;
   }
@@ -859,8 +850,7 @@ extern "C" int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D, con
     return LAKDE_EINVAL;
   }
   if (int st = bind_device("posterior_factor_tiled",
-                           {SP, W_triu, X_tiles, W_cores, X_norm2, nu_0, a, b, jitter, logdet_W, info, T_tiles,
-                            trace}))
+                           {SP, W_triu, X_tiles, W_cores, nu_0, a, b, jitter, logdet_W, info, T_tiles, trace}))
     return st;
   FactorArgs<float> g{};
   g.SP = static_cast<const float *>(SP);
@@ -873,7 +863,6 @@ extern "C" int lakde_posterior_factor_tiled(int dtype, int64_t N, int64_t D, con
   g.W = static_cast<float *>(W_triu);
   g.Xt = static_cast<float *>(X_tiles);
   g.Wc = static_cast<float *>(W_cores);
-  g.xnorm2 = static_cast<float *>(X_norm2);
   g.logdet = static_cast<float *>(logdet_W);
   g.info = info;
   g.T_lower = 1;

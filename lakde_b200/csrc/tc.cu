@@ -18,11 +18,14 @@
 // One persistent CTA per SM, 256 threads, software-pipelined over 128-pair
 // tiles:
 //   * warp 0 (producer) pops kernel rows from an atomic row queue (rows in
-//     the caller's longest-first order: a pair-count-balanced schedule), and
-//     for tile t + 1 stages its column indices / weights in shared memory and
-//     issues one cp.async.bulk per pair row (rows of X padded to a multiple of
-//     16 bytes), plus the kernel centre and, for the E-step, the kernel's W
-//     cores; the stage's mbarrier completes on the bytes;
+//     the caller's longest-first order: a pair-count-balanced schedule) and
+//     stages tile t + 2: its column indices / weights in shared memory and a
+//     bulk copy of the kernel centre (on that stage's mbarrier); for the
+//     first tile of a row, one tile ahead, it bulk-copies the row's W cores
+//     into one of two B stages;
+//   * all threads gather tile t + 1's pair rows (rows of X padded to a
+//     multiple of 16 bytes) with 16-byte cp.async copies, a whole iteration
+//     ahead of their use;
 //   * all 8 warps convert tile t: centre, (M-step: scale by sqrt r), split
 //     into the hi / lo core-matrix tile, and for the first tile of a row split
 //     the row's W cores in place;
@@ -55,7 +58,7 @@ namespace tc {
 
 constexpr int MT = 128;        // pairs (queries) per tile: the MMA M
 constexpr int NTHR = 256;      // 8 warps
-constexpr int RAW_STRIDE = 256;  // bytes per staged pair row (D <= 64 floats)
+constexpr int RAW_STRIDE = 272;  // bytes per staged pair row: 64 floats + 16 bytes against bank conflicts
 constexpr uint32_t kSpinLimit = 1u << 26;
 constexpr uint64_t kWaitLimitNs = 1500000000ull;  // 1.5 s: far above any copy or MMA of one tile
 constexpr int PQ = 2048;       // queries per predictive-density launch
@@ -200,8 +203,6 @@ struct Args {
   const float *logdet;   // E-step
   const float *lc;       // predictive density: log coefficient per kernel
   float *logrho;         // E-step output, CSR order
-  const float *rw;       // E-step, optional: r per pair (CSR order) ...
-  float *rq;             // ... and the output sum_p r_p Q_p per kernel
   float *S;              // M-step output [N, D, D] (dense) ...
   int lower_only;
   float *SPo;            // ... or the S halves of the interleaved S / P tiles
@@ -224,18 +225,17 @@ struct Args {
 // double as the accumulator copy of the M-step's epilogue.
 struct Smem {
   static constexpr uint32_t TILE = 0;                                   // 64 KB (M-step: 16 x GT_SBO)
-  static constexpr uint32_t RAW = TILE + 16 * GT_SBO;                   // 2 x 32 KB
+  static constexpr uint32_t RAW = TILE + 16 * GT_SBO;                   // 2 x 34 KB
   static constexpr uint32_t BST = RAW + 2 * MT * RAW_STRIDE;            // 2 x (hi 16 KB + lo 16 KB)
   static constexpr uint32_t B_BYTES = 16384;
   static constexpr uint32_t RSTR = 68;                                  // M-step accumulator copy row stride
   static constexpr uint32_t RED = BST;
-  static constexpr uint32_t XN = BST + 4 * B_BYTES;                     // 3 x 256 B kernel centres
-  static constexpr uint32_t CIDX = XN + 3 * 256;                        // 3 x 128 int
-  static constexpr uint32_t RV = CIDX + 3 * MT * 4;                     // 3 x 128 float
-  static constexpr uint32_t META = RV + 3 * MT * 4;                     // 3 x Meta
-  static constexpr uint32_t PM = META + 3 * 64;                         // predictive density (max, sum)
-  static constexpr uint32_t RQ = PM + 2 * PQ * 4;                       // E-step: per-warp partials, row sum
-  static constexpr uint32_t BAR = RQ + 64;                              // mbarriers
+  static constexpr uint32_t XN = BST + 4 * B_BYTES;                     // 4 x 256 B kernel centres
+  static constexpr uint32_t CIDX = XN + 4 * 256;                        // 4 x 128 int
+  static constexpr uint32_t RV = CIDX + 4 * MT * 4;                     // 4 x 128 float
+  static constexpr uint32_t META = RV + 4 * MT * 4;                     // 4 x Meta
+  static constexpr uint32_t PM = META + 4 * 64;                         // predictive density (max, sum)
+  static constexpr uint32_t BAR = PM + 2 * PQ * 4;                      // mbarriers
   static constexpr uint32_t bytes = BAR + 64;
 };
 static_assert(Smem::RSTR * 128 * 4 <= 4 * Smem::B_BYTES, "accumulator copy fits the B stages");
@@ -246,6 +246,7 @@ struct Meta {
   int cnt;        // pairs in the tile
   int flags;      // 1: first tile of its row, 2: last tile of its row, 4: row has an invalid index
   int bs;         // B stage / accumulator of the row (row counter parity)
+  int bph;        // parity of this row's use of B stage bs (its W-copy mbarrier phase)
   float c0, c1;   // E-step: 0.5 E[log|Lambda|], -nu / 2;  predictive density: log coefficient, (nu + 1) / 2
   float rsum;     // M-step: sum of r over the row (last tile)
 };
@@ -263,6 +264,7 @@ struct Kern {
     int64_t end;      // end of the current row
     int64_t popped;   // rows taken by this CTA
     int rows;         // rows started by this CTA (their parity selects the B stage / accumulator)
+    int bpar;         // bit b: parity of the next use of B stage b (its W-copy mbarrier phase)
     float racc;       // M-step: running sum of r over the row
     int bad;          // M-step: invalid index seen in the row
     float c0, c1;     // row constants of the E-step / predictive density
@@ -289,15 +291,15 @@ struct Kern {
     return (MODE != PRED && g.order) ? (int64_t)g.order[it] : it;
   }
 
-  // Stages the next tile into raw slot s / meta slot ms (or a stop marker
-  // when the CTA has no work left).  All 32 lanes arrive on the stage's
-  // mbarrier after writing their part of the metadata; lane 0's arrival
-  // carries the byte count of the bulk copies.
-  static __device__ void produce(const Args &g, Prod &P, unsigned char *sm, int s, int ms, int lane) {
+  // Stages the next tile into meta slot ms (or a stop marker when the CTA has
+  // no work left): metadata, column indices / weights and the bulk copy of
+  // the kernel centre, which completes on mbarrier xfull.  All 32 lanes
+  // arrive on it; lane 0's arrival carries the byte count.
+  static __device__ void produce(const Args &g, Prod &P, unsigned char *sm, uint64_t *xfull, int ms, int lane) {
     Meta *meta = reinterpret_cast<Meta *>(sm + Smem::META) + ms;
     int32_t *cidx = reinterpret_cast<int32_t *>(sm + Smem::CIDX) + ms * MT;
     float *rv = reinterpret_cast<float *>(sm + Smem::RV) + ms * MT;
-    uint64_t *raw_full = reinterpret_cast<uint64_t *>(sm + Smem::BAR) + s;
+    uint64_t *raw_full = xfull;
     const uint32_t rb = (uint32_t)(((g.D + 3) / 4) * 16);  // bytes copied per row
     bool first = false;
     if (!P.done && P.next >= P.end) {
@@ -346,8 +348,8 @@ struct Kern {
     const int cnt = (int)((P.end - base) < MT ? (P.end - base) : MT);
     P.next = base + cnt;
     const bool last = P.next >= P.end;
-    unsigned char *raw = sm + Smem::RAW + (uint32_t)s * MT * RAW_STRIDE;
-    // column indices and weights, 4 per lane; one bulk copy per valid pair row
+    // column indices and weights, 4 per lane (the rows are gathered by all
+    // threads, see gather_rows)
     uint32_t bytes = 0;
     unsigned bad = 0;
     float rs = 0.f;
@@ -362,7 +364,6 @@ struct Kern {
         } else {
           c = g.col[base + p];
           if (MODE == MSTEP) w = g.r[base + p];
-          if (MODE == ESTEP && g.rw) w = g.rw[base + p];
           if (c < 0 || c >= g.npts) {
             c = -1;
             w = 0.f;
@@ -374,16 +375,8 @@ struct Kern {
       if (MODE == MSTEP) {
         rv[p] = w;
         rs += w;
-      } else if (MODE == ESTEP) {
-        rv[p] = w;
-      }
-      if (c >= 0) {
-        const float *src = (MODE == PRED) ? g.Y + (int64_t)c * g.ldy : g.X + (int64_t)c * g.ldx;
-        bulk_g2s(smem_u32(raw + p * RAW_STRIDE), src, rb, raw_full);
-        bytes += rb;
       }
     }
-    bytes = __reduce_add_sync(0xffffffffu, bytes);
     if (MODE == MSTEP) {
       bad = __reduce_or_sync(0xffffffffu, bad);
       rs = warp_sum(rs);
@@ -391,28 +384,23 @@ struct Kern {
       P.bad |= (int)bad;
     }
     const int bs = (P.rows - 1) & 1;
-    // the kernel centre, once per tile (its meta slot), and the row's W cores
-    // into B stage bs with the first tile
+    int bph = 0;
+    if (first) {
+      bph = (P.bpar >> bs) & 1;
+      P.bpar ^= 1 << bs;
+    }
+    // the kernel centre, once per tile (its meta slot)
     unsigned char *xn = sm + Smem::XN + ms * 256;
     const float *xsrc = g.X + (n + (MODE == PRED ? 0 : g.koff)) * g.ldx;
     if (lane == 0) bulk_g2s(smem_u32(xn), xsrc, rb, raw_full);
     bytes += rb;
-    if (MODE != MSTEP && first) {
-      constexpr int NG = DP / 8;  // row groups of a K step in the B stage
-      const float *wsrc = g.Wc + n * (int64_t)(g.ntile * 64);
-      unsigned char *bhi = sm + Smem::BST + (uint32_t)bs * 2 * Smem::B_BYTES;
-      for (int J = lane; J < g.nt; J += 32) {
-        const uint32_t seg_bytes = (uint32_t)(g.nt - J) * 256u;
-        bulk_g2s(smem_u32(bhi + J * NG * 256 + J * 256), wsrc + wseg(J, g.nt), seg_bytes, raw_full);
-      }
-      bytes += (uint32_t)g.ntile * 256u;
-    }
     if (lane == 0) {
       meta->n = n;
       meta->base = base;
       meta->cnt = cnt;
       meta->flags = (first ? 1 : 0) | (last ? 2 : 0) | (P.bad ? 4 : 0);
       meta->bs = bs;
+      meta->bph = bph;
       meta->c0 = P.c0;
       meta->c1 = P.c1;
       meta->rsum = P.racc;
@@ -421,6 +409,46 @@ struct Kern {
     if (g.stall && P.rows == 1 && first) bytes += 16;  // never delivered: the wait must give up
     if (lane == 0) mbar_arrive_tx(raw_full, bytes);
     else mbar_arrive(raw_full);
+  }
+
+  // The W cores of the row that starts at the tile in meta slot ms, into its
+  // B stage (warp 0; the E-step and the predictive density).  The stage's
+  // previous row has finished its MMAs (the caller has waited for them).
+  static __device__ void copy_w(const Args &g, unsigned char *sm, uint64_t *bfull, int ms, int lane) {
+    const Meta &meta = reinterpret_cast<const Meta *>(sm + Smem::META)[ms];
+    if (MODE == MSTEP || meta.n < 0 || !(meta.flags & 1)) return;
+    constexpr int NG = DP / 8;  // row groups of a K step in the B stage
+    const float *wsrc = g.Wc + meta.n * (int64_t)(g.ntile * 64);
+    unsigned char *bhi = sm + Smem::BST + (uint32_t)meta.bs * 2 * Smem::B_BYTES;
+    uint64_t *bar = bfull + meta.bs;
+    if (lane == 0) mbar_arrive_tx(bar, (uint32_t)g.ntile * 256u);
+    __syncwarp();
+    for (int J = lane; J < g.nt; J += 32) {
+      const uint32_t seg_bytes = (uint32_t)(g.nt - J) * 256u;
+      bulk_g2s(smem_u32(bhi + J * NG * 256 + J * 256), wsrc + wseg(J, g.nt), seg_bytes, bar);
+    }
+  }
+
+  // The pair (query) rows of the tile in meta slot ms into raw stage s:
+  // thread (pair p = tid % 128, half h) copies the 16-byte chunks 8 h .. 8 h
+  // + 7 of its row with cp.async and commits them as one group.
+  static __device__ __forceinline__ void gather_rows(const Args &g, unsigned char *sm, int s, int ms, int tid) {
+    const Meta &meta = reinterpret_cast<const Meta *>(sm + Smem::META)[ms];
+    const int p = tid & (MT - 1), h = tid >> 7;
+    const int32_t c = (meta.n >= 0 && p < meta.cnt) ? reinterpret_cast<const int32_t *>(sm + Smem::CIDX)[ms * MT + p]
+                                                    : -1;
+    if (c >= 0) {
+      const float *src = (MODE == PRED) ? g.Y + (int64_t)c * g.ldy : g.X + (int64_t)c * g.ldx;
+      const uint32_t dst = smem_u32(sm + Smem::RAW + (uint32_t)s * MT * RAW_STRIDE + (uint32_t)p * RAW_STRIDE);
+      const int rch = (g.D + 3) / 4;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int k = 8 * h + i;
+        if (k < rch)
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + 16u * k), "l"(src + 4 * k) : "memory");
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
   }
 
   // --------------------------------------------------------------- converter
@@ -482,7 +510,7 @@ struct Kern {
     unsigned char *dst = tile + (uint32_t)(p >> 3) * 4096u + (uint32_t)(p & 7) * 16u;
 #pragma unroll
     for (int i = 0; i < HCH; ++i) {
-      const int k = h * HCH + ((i + p) % HCH);
+      const int k = h * HCH + i;
       float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
       if (cvalid >= 0 && k < rch) {
         const float4 x = *reinterpret_cast<const float4 *>(raw + p * RAW_STRIDE + k * 16);
@@ -623,22 +651,6 @@ struct Kern {
       for (int k = 0; k < 16; ++k) q = fmaf(v[k], v[k], q);
     }
     const int p = tid;
-    if (MODE == ESTEP && g.rw) {
-      // sum_p r_p Q_p of the row: warp sums, then the four in warp order
-      // (deterministic), carried over the row's tiles in shared memory
-      const float *rv = reinterpret_cast<const float *>(sm + Smem::RV) + ms * MT;
-      float *rq = reinterpret_cast<float *>(sm + Smem::RQ);
-      float part = (p < meta.cnt && cidx[p] >= 0) ? rv[p] * q : 0.f;
-      part = warp_sum(part);
-      if ((tid & 31) == 0) rq[warp] = part;
-      asm volatile("bar.sync 2, 128;" ::: "memory");
-      if (tid == 0) {
-        const float prev = (meta.flags & 1) ? 0.f : rq[4];
-        const float acc = prev + ((rq[0] + rq[1]) + (rq[2] + rq[3]));
-        rq[4] = acc;
-        if (meta.flags & 2) g.rq[meta.n] = acc;
-      }
-    }
     if (p >= meta.cnt) return;
     if (MODE == ESTEP) {
       const int32_t c = cidx[p];
@@ -672,8 +684,9 @@ __global__ void __launch_bounds__(NTHR, 1) tc_kernel(Args g) {
   __shared__ uint32_t s_tmem;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   uint64_t *bars = reinterpret_cast<uint64_t *>(sm + Smem::BAR);
-  uint64_t *raw_full = bars;     // [2]
-  uint64_t *mma_done = bars + 2;
+  uint64_t *xfull = bars;         // [2] metadata + kernel centre of tile t (t & 1)
+  uint64_t *mma_done = bars + 2;  // MMAs of tile t committed
+  uint64_t *bfull = bars + 3;     // [2] W cores of a B stage
 
   // zero the operand tile (cores past DP stay zero) and the B stages (cores above the block diagonal)
   for (uint32_t o = tid * 16; o < Smem::RAW; o += NTHR * 16) *reinterpret_cast<uint4 *>(sm + o) = make_uint4(0, 0, 0, 0);
@@ -689,9 +702,11 @@ __global__ void __launch_bounds__(NTHR, 1) tc_kernel(Args g) {
   }
   if (warp == 0) tmem_alloc(&s_tmem, 128);
   if (tid == 0) {
-    mbar_init(raw_full, 32);
-    mbar_init(raw_full + 1, 32);
+    mbar_init(xfull, 32);
+    mbar_init(xfull + 1, 32);
     mbar_init(mma_done, 1);
+    mbar_init(bfull, 1);
+    mbar_init(bfull + 1, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   fence_async_smem();
@@ -699,37 +714,43 @@ __global__ void __launch_bounds__(NTHR, 1) tc_kernel(Args g) {
   __syncthreads();
   fence_after();
   const uint32_t tmem = s_tmem;
+  const Meta *metas = reinterpret_cast<const Meta *>(sm + Smem::META);
 
+  // prologue: tiles 0 and 1 staged, tile 0's W cores and pair rows in flight
   typename K::Prod P{};
   P.n = -1;
   P.next = 0;
   P.end = 0;
   P.done = false;
-  if (warp == 0) K::produce(g, P, sm, 0, 0, lane);
+  if (warp == 0) {
+    K::produce(g, P, sm, xfull, 0, lane);
+    K::produce(g, P, sm, xfull + 1, 1, lane);
+  }
+  __syncthreads();
+  if (warp == 0) K::copy_w(g, sm, bfull, 0, lane);
+  K::gather_rows(g, sm, 0, 0, tid);
 
   bool ok = true;
   int t = 0;
-  int pending_raw = 0;  // the stage whose copies were issued last and not yet waited on (+1), or 0
-  bool mma_pending = false;
-  int row_acc = 0;      // M-step: accumulator of the current row
+  int row_acc = 0;  // M-step: accumulator of the current row
   int prev_acc = 0;
   for (;;) {
-    const int s = t & 1, ms = t % 3;
-    bool w = mbar_wait(raw_full + s, (uint32_t)((t >> 1) & 1));
+    const int s = t & 1, ms = t & 3;
+    const Meta &meta = metas[ms];
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    bool w = mbar_wait(xfull + s, (uint32_t)((t >> 1) & 1));
+    if (MODE != MSTEP && meta.n >= 0 && (meta.flags & 1)) w = mbar_wait(bfull + meta.bs, (uint32_t)meta.bph) && w;
     if (t > 0) w = mbar_wait(mma_done, (uint32_t)((t - 1) & 1)) && w;
     ok = __syncthreads_and(w ? 1 : 0) != 0;
-    if (!ok) {
-      pending_raw = s + 1;
-      mma_pending = t > 0;
-      break;
-    }
+    if (!ok) break;
     fence_after();
-    mma_pending = false;
-    const Meta &meta = reinterpret_cast<const Meta *>(sm + Smem::META)[ms];
     const bool stop = meta.n < 0;
-    if (!stop && warp == 0) K::produce(g, P, sm, s ^ 1, (t + 1) % 3, lane);
     uint32_t acc_sel = (uint32_t)s;
     if (!stop) {
+      // tile t + 1: W cores (first tile of a row) and pair rows; tile t + 2: metadata
+      if (warp == 0) K::copy_w(g, sm, bfull, (t + 1) & 3, lane);
+      K::gather_rows(g, sm, s ^ 1, (t + 1) & 3, tid);
+      if (warp == 0) K::produce(g, P, sm, xfull + s, (t + 2) & 3, lane);
       if (MODE == MSTEP) {
         if (meta.flags & 1) row_acc ^= 1;
         acc_sel = (uint32_t)row_acc;
@@ -742,11 +763,10 @@ __global__ void __launch_bounds__(NTHR, 1) tc_kernel(Args g) {
         fence_after();
         K::issue_mma(g, sm, meta, tmem, acc_sel, mma_done);
       }
-      mma_pending = true;
     }
     if (t > 0) {
       fence_after();
-      K::epilogue(g, sm, (t + 2) % 3, tmem, (uint32_t)prev_acc, tid);
+      K::epilogue(g, sm, (t - 1) & 3, tmem, (uint32_t)prev_acc, tid);
       fence_before();
     }
     prev_acc = (int)acc_sel;
@@ -754,10 +774,16 @@ __global__ void __launch_bounds__(NTHR, 1) tc_kernel(Args g) {
     ++t;
   }
   if (!ok) {
-    // wait (bounded) for this CTA's copies and MMAs still in flight before leaving
-    if (tid == 0) atomicExch(g.err, 1);
-    if (pending_raw) mbar_wait(raw_full + (pending_raw - 1), (uint32_t)((t >> 1) & 1));
-    if (mma_pending) mbar_wait(mma_done, (uint32_t)((t - 1) & 1));
+    // Wait (bounded) for this CTA's copies and MMAs still in flight before
+    // leaving: the staging of tiles t and t + 1, tile t's W cores, tile t - 1's MMAs.
+    if (tid == 0) {
+      atomicExch(g.err, 1);
+      mbar_wait(xfull + (t & 1), (uint32_t)((t >> 1) & 1));
+      mbar_wait(xfull + ((t + 1) & 1), (uint32_t)(((t + 1) >> 1) & 1));
+      const Meta &meta = metas[t & 3];
+      if (MODE != MSTEP && meta.n >= 0 && (meta.flags & 1)) mbar_wait(bfull + meta.bs, (uint32_t)meta.bph);
+      if (t > 0) mbar_wait(mma_done, (uint32_t)((t - 1) & 1));
+    }
   }
   if (MODE == PRED) {
     __syncthreads();
@@ -971,7 +997,7 @@ extern "C" int lakde_pack_w_cores(int dtype, int64_t N, int64_t D, const void *W
 extern "C" int lakde_estep_tc(int dtype, int64_t N, int64_t D, int64_t npts, const void *rowptr, const void *col,
                               const void *order, const void *X, int64_t ldx, int64_t kernel_offset,
                               const void *W_cores, const void *nu, const void *logdet_W, void *logrho,
-                              const void *r, void *rq_sum, int32_t *queue, int32_t *err, void *stream) {
+                              int32_t *queue, int32_t *err, void *stream) {
   clear_error();
   if (int st = tc_common_checks("estep_tc", dtype, N, D, npts, kernel_offset, X, ldx)) return st;
   if (N == 0) return LAKDE_OK;
@@ -983,12 +1009,7 @@ extern "C" int lakde_estep_tc(int dtype, int64_t N, int64_t D, int64_t npts, con
     set_error("estep_tc: W_cores must be 16-byte aligned");
     return LAKDE_EINVAL;
   }
-  if ((r == nullptr) != (rq_sum == nullptr)) {
-    set_error("estep_tc: r and rq_sum go together");
-    return LAKDE_EINVAL;
-  }
-  if (int st = bind_device("estep_tc", {logrho, rowptr, col, order, X, W_cores, nu, logdet_W, r, rq_sum, queue, err}))
-    return st;
+  if (int st = bind_device("estep_tc", {logrho, rowptr, col, order, X, W_cores, nu, logdet_W, queue, err})) return st;
   tc::Args g{};
   g.rowptr = static_cast<const int64_t *>(rowptr);
   g.col = static_cast<const int32_t *>(col);
@@ -999,8 +1020,6 @@ extern "C" int lakde_estep_tc(int dtype, int64_t N, int64_t D, int64_t npts, con
   g.nu = static_cast<const float *>(nu);
   g.logdet = static_cast<const float *>(logdet_W);
   g.logrho = static_cast<float *>(logrho);
-  g.rw = static_cast<const float *>(r);
-  g.rq = static_cast<float *>(rq_sum);
   g.npts = npts;
   g.N = N;
   g.koff = kernel_offset;

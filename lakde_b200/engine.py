@@ -174,13 +174,13 @@ class FusedVI:
         else:
             K.mstep(rowptr, col, self.r, self.X, self.nu_0, S=self.S, nu=self.nu)
 
-    def factor(self, with_trace=True, xnorm2=None):
+    def factor(self, with_trace=True):
         mixed = self.precision == "mixed"
         if mixed and self.SP is not None:
             Tt = self.trace_tiles() if with_trace else None
             K.posterior_factor_tiled(self.SP, self.D, self.W_inv_jitter, self.eps, self.nu_0_t, self.a, self.b,
                                      None, self.logdet_W, self.info, T_tiles=Tt,
-                                     trace=self.trace if with_trace else None, W_cores=self.Wc, X_norm2=xnorm2)
+                                     trace=self.trace if with_trace else None, W_cores=self.Wc)
             torch.minimum(self.failed, self.info.min(), out=self.failed)
             return
         P, T = self._prior()
@@ -191,18 +191,17 @@ class FusedVI:
         )
         torch.minimum(self.failed, self.info.min(), out=self.failed)
 
-    def estep_numerators(self, rq_sum=None):
-        """log rho of every pair of the pattern (the E-step before the normaliser);
-        with rq_sum (mixed precision), also sum_p r_p Q_p per kernel."""
+    def estep_numerators(self):
+        """log rho of every pair of the pattern (the E-step before the normaliser)."""
         rowptr, col = self._tri()
         if self.precision == "mixed":
             K.estep_tc(rowptr, col, self.Xp, self.Wc, self.nu, self.logdet_W, self.err, order=self.pattern.order,
-                       out=self.logrho, queue=self.queue, r=self.r if rq_sum is not None else None, rq_sum=rq_sum)
+                       out=self.logrho, queue=self.queue)
         else:
             K.estep_logrho(rowptr, col, self.X, self.U, self.nu, self.logdet_W, out=self.logrho)
 
-    def estep(self, mode, rq_sum=None):
-        self.estep_numerators(rq_sum)
+    def estep(self, mode):
+        self.estep_numerators()
         K.estep_normalise(self.pattern.cptr, self.pattern.pos, self.logrho, self.r, self.c, self.rsum, mode,
                           self.threshold)
 
@@ -315,18 +314,10 @@ class FusedKNN(FusedVI):
         self.sigma_0_tril = L0
         if self.precision == "mixed" and 8 < self.D <= 64:
             # the tensor-core path reads S and P as interleaved tiles (P halves
-            # fixed here); the trace factor as tiles only if a product trace is asked for
+            # fixed here) and the trace factor as tiles (packed on first use)
             nt = K.tile_count(self.D)
             self.SP = torch.zeros(self.N, nt * 128, dtype=self.dtype, device=self.device)
             K.pack_tiles(sigma_0, self.SP, 128, 64)
-            self.rq = torch.empty(self.N, dtype=self.dtype, device=self.device)
-            self.xn2 = torch.empty(self.N, dtype=self.dtype, device=self.device)
-
-    # "identity": on the tiled mixed path the trace tr(Sigma0 W) comes from the
-    # E-step, tr(A W) = D with A = c Sigma0 + S + j I (c = nu_0 a / b) giving
-    # tr(Sigma0 W) = (D - sum_p r_p Q_p - j tr(W)) / c; "product": the FP64
-    # product ||L0^T W_triu||_F^2 inside the factorisation (lakde/linalg_util.py:35-37)
-    trace_mode = "identity"
 
     def trace_tiles(self):
         if self.Tt is None:
@@ -334,14 +325,6 @@ class FusedKNN(FusedVI):
             self.Tt = torch.zeros(self.N, nt * 64, dtype=self.dtype, device=self.device)
             K.pack_tiles(self.sigma_0_tril, self.Tt, 64, 0)
         return self.Tt
-
-    def _by_identity(self):
-        return self.precision == "mixed" and self.SP is not None and self.trace_mode == "identity"
-
-    def _trace_from_identity(self):
-        c = self.nu_0_t * (self.a / self.b)
-        tr = torch.addcmul(self.rq, self.W_inv_jitter, self.xn2).neg_().add_(self.D)
-        torch.div(tr, c, out=self.trace)
 
     def kernel_launches(self):
         """The library launches of one iteration as callables by kernel name
@@ -354,40 +337,20 @@ class FusedKNN(FusedVI):
                 mm=self.sigma_0_lambda_mm_trace)}
         else:
             mixed = self.precision == "mixed"
-            out = {("mstep_tc" if mixed else "mstep"): self.mstep}
-            if self._by_identity():
-                out["posterior_factor"] = lambda: self.factor(with_trace=False, xnorm2=self.xn2)
-                out["estep_tc"] = lambda: self.estep_numerators(self.rq)
-            else:
-                out["posterior_factor"] = self.factor
-                out["estep_tc" if mixed else "estep_logrho"] = self.estep_numerators
+            out = {("mstep_tc" if mixed else "mstep"): self.mstep, "posterior_factor": self.factor,
+                   ("estep_tc" if mixed else "estep_logrho"): self.estep_numerators}
         out["estep_normalise"] = lambda: K.estep_normalise(p.cptr, p.pos, self.logrho, self.r, self.c, self.rsum, 1,
                                                            self.threshold)
         return out
-
-    def _factor_and_numerators(self, mode):
-        """Factorisation, E-step (normaliser with `mode`) and the trace of the
-        b update, by the identity or by the product."""
-        if self._by_identity():
-            self.factor(with_trace=False, xnorm2=self.xn2)
-            self.estep(mode, rq_sum=self.rq)
-            self._trace_from_identity()
-        else:
-            self.factor()
-            self.estep(mode)
-
-    _T_lower = True  # the Cholesky factor of Sigma0
-
-    def _prior(self):
-        return self.sigma_0, self.sigma_0_tril
 
     def init_summaries(self):
         """lakde/local_knn_kde.py:140-193 at block_size = N."""
         self.init_prior()
         self.refresh_points()
         self.mstep()
-        self._factor_and_numerators(mode=0)
+        self.factor()
         torch.mul(self.nu, self.trace, out=self.sigma_0_lambda_mm_trace)
+        self.estep(mode=0)
 
     def step(self):
         """lakde/local_knn_kde.py:209-254 at block_size = N."""
@@ -402,7 +365,8 @@ class FusedKNN(FusedVI):
             return
         self.refresh_points()
         self.mstep()
-        self._factor_and_numerators(mode=1)
+        self.factor()
+        self.estep(mode=1)
         torch.mul(self.nu, self.trace, out=self.sigma_0_lambda_mm_trace)
         torch.add(self.sigma_0_lambda_mm_trace * (self.nu_0 / 2), self.b_0, out=self.b)
 

@@ -406,11 +406,11 @@ def mstep_tc_tiled(rowptr, col, r, X, nu_0, err, SP, nu, order=None, kernel_offs
 
 
 def posterior_factor_tiled(SP, D, jitter, eps, nu_0, a, b, out, logdet, info, T_tiles=None, trace=None,
-                           X_tiles=None, W_cores=None, X_norm2=None):
+                           X_tiles=None, W_cores=None):
     """posterior_factor from the tiled SP (and T) layout (see include/lakde_b200.h); writes W_triu to
     ``out``, X = W_triu^T as tiles to ``X_tiles`` and / or the W cores to ``W_cores``
     (any two may be None)."""
-    nat.require_cuda(SP, jitter, nu_0, a, b, out, X_tiles, W_cores, X_norm2, logdet, info, T_tiles, trace,
+    nat.require_cuda(SP, jitter, nu_0, a, b, out, X_tiles, W_cores, logdet, info, T_tiles, trace,
                      op="posterior_factor_tiled")
     N = jitter.numel()
     if W_cores is not None:
@@ -419,8 +419,8 @@ def posterior_factor_tiled(SP, D, jitter, eps, nu_0, a, b, out, logdet, info, T_
     nat.check(
         nat.lib().lakde_posterior_factor_tiled(
             nat.dtype_code(SP), N, int(D), nat.ptr(SP), nat.ptr(nu_0), nat.ptr(a), nat.ptr(b), nat.ptr(jitter),
-            float(eps), nat.ptr(out), nat.ptr(X_tiles), nat.ptr(W_cores), nat.ptr(X_norm2), nat.ptr(logdet),
-            nat.ptr(info), nat.ptr(T_tiles), nat.ptr(trace), nat.stream_of(SP),
+            float(eps), nat.ptr(out), nat.ptr(X_tiles), nat.ptr(W_cores), nat.ptr(logdet), nat.ptr(info),
+            nat.ptr(T_tiles), nat.ptr(trace), nat.stream_of(SP),
         ),
         "posterior_factor_tiled",
     )
@@ -539,12 +539,10 @@ def log_pred_density_bwd(X, W_triu, nu, log_coeff, Y, out, grad_out):
     return gY, sw, S_c
 
 
-def estep_tc(rowptr, col, X, W_cores, nu, logdet_W, err, order=None, out=None, kernel_offset=0, queue=None,
-             r=None, rq_sum=None):
+def estep_tc(rowptr, col, X, W_cores, nu, logdet_W, err, order=None, out=None, kernel_offset=0, queue=None):
     """Tensor-core (tf32 hi / lo) E-step numerators, D <= 64, W_triu given as W
-    cores (see include/lakde_b200.h).  Row n of rowptr is kernel n + kernel_offset
-    of X.  With r and rq_sum, also rq_sum[n] = sum over row n of r_p Q_p."""
-    nat.require_cuda(rowptr, col, X, W_cores, nu, logdet_W, err, order, queue, r, rq_sum, op="estep_tc")
+    cores (see include/lakde_b200.h).  Row n of rowptr is kernel n + kernel_offset of X."""
+    nat.require_cuda(rowptr, col, X, W_cores, nu, logdet_W, err, order, queue, op="estep_tc")
     assert rowptr.dtype == torch.int64 and col.dtype == torch.int32 and err.dtype == torch.int32
     assert W_cores.dtype == torch.float32 and W_cores.is_contiguous()
     N = rowptr.numel() - 1
@@ -554,7 +552,7 @@ def estep_tc(rowptr, col, X, W_cores, nu, logdet_W, err, order=None, out=None, k
         nat.lib().lakde_estep_tc(
             nat.dtype_code(X), N, X.size(1), X.size(0), nat.ptr(rowptr), nat.ptr(col), nat.ptr(order), nat.ptr(Xr),
             ldx, int(kernel_offset), nat.ptr(W_cores), nat.ptr(nu), nat.ptr(logdet_W), nat.ptr(out),
-            nat.ptr(r), nat.ptr(rq_sum), nat.ptr(queue), nat.ptr(err), nat.stream_of(X),
+            nat.ptr(queue), nat.ptr(err), nat.stream_of(X),
         ),
         "estep_tc",
     )

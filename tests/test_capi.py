@@ -57,12 +57,12 @@ def test_invalid_arguments_are_rejected_on_the_host(nat):
                                       ctypes.c_void_p(8), None, 0, 0, None, None, None) in (1, 2)
     # tensor-core entry points: rows of X must be 16-byte aligned (checked before any device work)
     p = ctypes.c_void_p(256)
-    st = lib.lakde_estep_tc(0, 10, 63, 10, p, p, None, p, 63, 0, p, p, p, p, None, None, None, p, None)
+    st = lib.lakde_estep_tc(0, 10, 63, 10, p, p, None, p, 63, 0, p, p, p, p, None, p, None)
     assert st == 1 and b"16-byte aligned rows" in lib.lakde_last_error()
     st = lib.lakde_mstep_tc(0, 10, 13, 10, p, p, None, p, ctypes.c_void_p(260), 16, 0, 14.0, p, p, 0, None, p, None)
     assert st == 1
-    assert lib.lakde_estep_tc(1, 10, 8, 10, p, p, None, p, 8, 0, p, p, p, p, None, None, None, p, None) == 2
-    assert lib.lakde_estep_tc(0, 10, 65, 10, p, p, None, p, 68, 0, p, p, p, p, None, None, None, p, None) == 4
+    assert lib.lakde_estep_tc(1, 10, 8, 10, p, p, None, p, 8, 0, p, p, p, p, None, p, None) == 2
+    assert lib.lakde_estep_tc(0, 10, 65, 10, p, p, None, p, 68, 0, p, p, p, p, None, p, None) == 4
     assert lib.lakde_w_cores_floats(63) == 36 * 64
     assert lib.lakde_w_cores_floats(21) == 6 * 64
     assert lib.lakde_w_cores_floats(3) == 64
