@@ -326,6 +326,11 @@ class FusedKNN(FusedVI):
             K.pack_tiles(self.sigma_0_tril, self.Tt, 64, 0)
         return self.Tt
 
+    _T_lower = True  # the Cholesky factor of Sigma0
+
+    def _prior(self):
+        return self.sigma_0, self.sigma_0_tril
+
     def kernel_launches(self):
         """The library launches of one iteration as callables by kernel name
         (to time them one by one; the step runs them in this order)."""
