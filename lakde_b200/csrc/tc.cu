@@ -10,10 +10,12 @@
 //
 // Precision: the differences are centred on the kernel in fp32 and split as
 // x = hi + lo with hi = tf32(x) and lo = tf32(x - hi) (round to nearest; 11 +
-// 11 significant bits, |lo| <= 2^-12 |x|).  Each product is formed as
-// hi*hi + lo*hi + hi*lo with fp32 accumulation in tensor memory: the dropped
-// lo*lo term and the rounding of lo are below 2^-22 relative, close to plain
-// fp32 arithmetic, which is what near-singular local covariances need.
+// 11 significant bits, |lo| <= 2^-11 |x|), with fp32 accumulation in tensor
+// memory.  The M-step forms all four blocks of (G_hi + G_lo)^T (G_hi + G_lo):
+// dropping lo*lo there would take a positive semi-definite 2^-24-relative
+// term off S, which shrinks exactly the small eigenvalues of a near-singular
+// neighbourhood.  The E-step forms hi*hi + lo*hi + hi*lo: its dropped lo*lo
+// and the rounding of lo are below 2^-22 relative with random sign.
 //
 // One persistent CTA per SM, 256 threads, software-pipelined over 128-pair
 // tiles:
@@ -57,7 +59,8 @@ namespace lakde {
 namespace tc {
 
 constexpr int MT = 128;        // pairs (queries) per tile: the MMA M
-constexpr int NTHR = 256;      // 8 warps
+constexpr int NTHR = 256;      // 8 consumer warps (two more produce)
+constexpr int NS = 8;          // metadata slots
 constexpr int RAW_STRIDE = 272;  // bytes per staged pair row: 64 floats + 16 bytes against bank conflicts
 constexpr uint32_t kSpinLimit = 1u << 26;
 constexpr uint64_t kWaitLimitNs = 1500000000ull;  // 1.5 s: far above any copy or MMA of one tile
@@ -230,34 +233,67 @@ struct Smem {
   static constexpr uint32_t B_BYTES = 16384;
   static constexpr uint32_t RSTR = 68;                                  // M-step accumulator copy row stride
   static constexpr uint32_t RED = BST;
-  static constexpr uint32_t XN = BST + 4 * B_BYTES;                     // 4 x 256 B kernel centres
-  static constexpr uint32_t CIDX = XN + 4 * 256;                        // 4 x 128 int
-  static constexpr uint32_t RV = CIDX + 4 * MT * 4;                     // 4 x 128 float
-  static constexpr uint32_t META = RV + 4 * MT * 4;                     // 4 x Meta
-  static constexpr uint32_t PM = META + 4 * 64;                         // predictive density (max, sum)
+  static constexpr uint32_t XN = BST + 4 * B_BYTES;                     // NS x 256 B kernel centres
+  static constexpr uint32_t CIDX = XN + NS * 256;                       // NS x 128 int
+  static constexpr uint32_t RV = CIDX + NS * MT * 4;                    // NS x 128 float
+  static constexpr uint32_t META = RV + NS * MT * 4;                    // NS x Meta
+  static constexpr uint32_t PM = META + NS * 64;                        // predictive density (max, sum)
   static constexpr uint32_t BAR = PM + 2 * PQ * 4;                      // mbarriers
-  static constexpr uint32_t bytes = BAR + 64;
+  static constexpr uint32_t bytes = BAR + 256;
 };
 static_assert(Smem::RSTR * 128 * 4 <= 4 * Smem::B_BYTES, "accumulator copy fits the B stages");
+static_assert(Smem::bytes + 1024 <= 232448, "shared memory of one CTA");
+
+// mbarriers (8 bytes each from Smem::BAR)
+struct Bars {
+  static constexpr int MFULL = 0;          // [NS] metadata of a slot written (32 producer lanes)
+  static constexpr int MEMPTY = NS;        // [NS] slot free again (consumer thread 0)
+  static constexpr int RFULL = 2 * NS;     // [2] pair rows and kernel centre landed (32 gatherer lanes + 1)
+  static constexpr int REMPTY = RFULL + 2; // [2] raw stage converted (consumer thread 0)
+  static constexpr int BFULL = REMPTY + 2; // [2] W cores of a B stage landed
+  static constexpr int BEMPTY = BFULL + 2; // [2] MMAs of the stage's last row done (tcgen05.commit)
+  static constexpr int MMA = BEMPTY + 2;   // MMAs of a tile done (tcgen05.commit)
+  static constexpr int COUNT = MMA + 1;
+};
+static_assert(Bars::COUNT * 8 <= 256, "mbarrier area");
 
 struct Meta {
   int64_t n;      // kernel row (< 0: no more tiles)
   int64_t base;   // first pair of the tile (CSR position; predictive density: query offset in the block)
   int cnt;        // pairs in the tile
-  int flags;      // 1: first tile of its row, 2: last tile of its row, 4: row has an invalid index
+  int flags;      // 1: first tile of its row, 2: last tile, 4: row has an invalid index, 8: B stage used before
   int bs;         // B stage / accumulator of the row (row counter parity)
   int bph;        // parity of this row's use of B stage bs (its W-copy mbarrier phase)
   float c0, c1;   // E-step: 0.5 E[log|Lambda|], -nu / 2;  predictive density: log coefficient, (nu + 1) / 2
   float rsum;     // M-step: sum of r over the row (last tile)
 };
 
+// All 32 lanes of a warp AND-reduce v over the n threads of named barrier id.
+__device__ __forceinline__ bool bar_and(int id, int n, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(id), "r"(n)
+      : "memory");
+  return r != 0;
+}
+
+__device__ __forceinline__ void bar_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+
 template <int MODE, int DP>
 struct Kern {
   static constexpr int NCH = DP / 4;     // 4-dim chunks of a row
   static constexpr int HCH = NCH / 2;    // chunks per converter thread
+  // M-step accumulator columns: the hi rows 0..63 of G^T, then its lo rows
+  // 64..64 + DP (rounded up to 16, the MMA's N granule)
+  static constexpr int MN = 64 + ((DP + 15) / 16) * 16;
+  // TMEM columns of one accumulator (two are allocated)
+  static constexpr uint32_t ACC_COLS = MODE == MSTEP ? 128u : 64u;
 
-  // ---------------------------------------------------------------- producer
-  // Producer state (warp 0, uniform over its lanes).
+  // ------------------------------------------------------- metadata warp
+  // Row state of the metadata warp (uniform over its lanes).
   struct Prod {
     int64_t n;        // current row
     int64_t next;     // first pair of the current row's next tile
@@ -265,6 +301,7 @@ struct Kern {
     int64_t popped;   // rows taken by this CTA
     int rows;         // rows started by this CTA (their parity selects the B stage / accumulator)
     int bpar;         // bit b: parity of the next use of B stage b (its W-copy mbarrier phase)
+    int bused;        // bit b: B stage b has been used
     float racc;       // M-step: running sum of r over the row
     int bad;          // M-step: invalid index seen in the row
     float c0, c1;     // row constants of the E-step / predictive density
@@ -291,16 +328,14 @@ struct Kern {
     return (MODE != PRED && g.order) ? (int64_t)g.order[it] : it;
   }
 
-  // Stages the next tile into meta slot ms (or a stop marker when the CTA has
-  // no work left): metadata, column indices / weights and the bulk copy of
-  // the kernel centre, which completes on mbarrier xfull.  All 32 lanes
-  // arrive on it; lane 0's arrival carries the byte count.
-  static __device__ void produce(const Args &g, Prod &P, unsigned char *sm, uint64_t *xfull, int ms, int lane) {
+  // Writes the next tile's metadata into slot ms (or a stop marker when the
+  // CTA has no work left): row, pair range, column indices (validated) and
+  // weights, row constants.  Every lane arrives on mfull afterwards.
+  // Returns false for the stop marker.
+  static __device__ bool produce(const Args &g, Prod &P, unsigned char *sm, uint64_t *mfull, int ms, int lane) {
     Meta *meta = reinterpret_cast<Meta *>(sm + Smem::META) + ms;
     int32_t *cidx = reinterpret_cast<int32_t *>(sm + Smem::CIDX) + ms * MT;
     float *rv = reinterpret_cast<float *>(sm + Smem::RV) + ms * MT;
-    uint64_t *raw_full = xfull;
-    const uint32_t rb = (uint32_t)(((g.D + 3) / 4) * 16);  // bytes copied per row
     bool first = false;
     if (!P.done && P.next >= P.end) {
       for (;;) {
@@ -339,18 +374,13 @@ struct Kern {
     }
     if (P.done) {
       if (lane == 0) meta->n = -1;
-      __syncwarp();
-      if (lane == 0) mbar_arrive_tx(raw_full, 0);
-      else mbar_arrive(raw_full);
-      return;
+      mbar_arrive(mfull);
+      return false;
     }
     const int64_t n = P.n, base = P.next;
     const int cnt = (int)((P.end - base) < MT ? (P.end - base) : MT);
     P.next = base + cnt;
     const bool last = P.next >= P.end;
-    // column indices and weights, 4 per lane (the rows are gathered by all
-    // threads, see gather_rows)
-    uint32_t bytes = 0;
     unsigned bad = 0;
     float rs = 0.f;
 #pragma unroll
@@ -384,71 +414,71 @@ struct Kern {
       P.bad |= (int)bad;
     }
     const int bs = (P.rows - 1) & 1;
-    int bph = 0;
+    int bph = 0, reused = 0;
     if (first) {
       bph = (P.bpar >> bs) & 1;
+      reused = (P.bused >> bs) & 1;
       P.bpar ^= 1 << bs;
+      P.bused |= 1 << bs;
     }
-    // the kernel centre, once per tile (its meta slot)
-    unsigned char *xn = sm + Smem::XN + ms * 256;
-    const float *xsrc = g.X + (n + (MODE == PRED ? 0 : g.koff)) * g.ldx;
-    if (lane == 0) bulk_g2s(smem_u32(xn), xsrc, rb, raw_full);
-    bytes += rb;
     if (lane == 0) {
       meta->n = n;
       meta->base = base;
       meta->cnt = cnt;
-      meta->flags = (first ? 1 : 0) | (last ? 2 : 0) | (P.bad ? 4 : 0);
+      meta->flags = (first ? 1 : 0) | (last ? 2 : 0) | (P.bad ? 4 : 0) | (reused ? 8 : 0);
       meta->bs = bs;
       meta->bph = bph;
       meta->c0 = P.c0;
       meta->c1 = P.c1;
       meta->rsum = P.racc;
     }
-    __syncwarp();
-    if (g.stall && P.rows == 1 && first) bytes += 16;  // never delivered: the wait must give up
-    if (lane == 0) mbar_arrive_tx(raw_full, bytes);
-    else mbar_arrive(raw_full);
+    mbar_arrive(mfull);
+    return true;
   }
 
-  // The W cores of the row that starts at the tile in meta slot ms, into its
-  // B stage (warp 0; the E-step and the predictive density).  The stage's
-  // previous row has finished its MMAs (the caller has waited for them).
-  static __device__ void copy_w(const Args &g, unsigned char *sm, uint64_t *bfull, int ms, int lane) {
-    const Meta &meta = reinterpret_cast<const Meta *>(sm + Smem::META)[ms];
-    if (MODE == MSTEP || meta.n < 0 || !(meta.flags & 1)) return;
+  // --------------------------------------------------------- gather warp
+  // The W cores of the row starting at the tile in slot ms into its B stage
+  // (the E-step and the predictive density), on mbarrier bfull.
+  static __device__ void copy_w(const Args &g, unsigned char *sm, const Meta &meta, uint64_t *bfull, int lane) {
     constexpr int NG = DP / 8;  // row groups of a K step in the B stage
     const float *wsrc = g.Wc + meta.n * (int64_t)(g.ntile * 64);
     unsigned char *bhi = sm + Smem::BST + (uint32_t)meta.bs * 2 * Smem::B_BYTES;
-    uint64_t *bar = bfull + meta.bs;
-    if (lane == 0) mbar_arrive_tx(bar, (uint32_t)g.ntile * 256u);
+    if (lane == 0) mbar_arrive_tx(bfull, (uint32_t)g.ntile * 256u);
     __syncwarp();
     for (int J = lane; J < g.nt; J += 32) {
       const uint32_t seg_bytes = (uint32_t)(g.nt - J) * 256u;
-      bulk_g2s(smem_u32(bhi + J * NG * 256 + J * 256), wsrc + wseg(J, g.nt), seg_bytes, bar);
+      bulk_g2s(smem_u32(bhi + J * NG * 256 + J * 256), wsrc + wseg(J, g.nt), seg_bytes, bfull);
     }
   }
 
-  // The pair (query) rows of the tile in meta slot ms into raw stage s:
-  // thread (pair p = tid % 128, half h) copies the 16-byte chunks 8 h .. 8 h
-  // + 7 of its row with cp.async and commits them as one group.
-  static __device__ __forceinline__ void gather_rows(const Args &g, unsigned char *sm, int s, int ms, int tid) {
-    const Meta &meta = reinterpret_cast<const Meta *>(sm + Smem::META)[ms];
-    const int p = tid & (MT - 1), h = tid >> 7;
-    const int32_t c = (meta.n >= 0 && p < meta.cnt) ? reinterpret_cast<const int32_t *>(sm + Smem::CIDX)[ms * MT + p]
-                                                    : -1;
-    if (c >= 0) {
-      const float *src = (MODE == PRED) ? g.Y + (int64_t)c * g.ldy : g.X + (int64_t)c * g.ldx;
-      const uint32_t dst = smem_u32(sm + Smem::RAW + (uint32_t)s * MT * RAW_STRIDE + (uint32_t)p * RAW_STRIDE);
-      const int rch = (g.D + 3) / 4;
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int k = 8 * h + i;
-        if (k < rch)
-          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + 16u * k), "l"(src + 4 * k) : "memory");
+  // The pair (query) rows of the tile in slot ms into raw stage s, and its
+  // kernel centre into the slot's centre buffer, completing on mbarrier
+  // rfull (33 arrivals: lane 0's byte count for the bulk copy, then one per
+  // lane when its cp.async copies have landed).  Half-warp h copies row
+  // 2 j + h, lane k % 16 its 16-byte chunk k: two 256-byte rows per
+  // instruction.
+  static __device__ __forceinline__ void gather(const Args &g, unsigned char *sm, const Meta &meta, int s, int ms,
+                                                uint64_t *rfull, bool stall, int lane) {
+    const uint32_t rb = (uint32_t)(((g.D + 3) / 4) * 16);  // bytes per row
+    if (lane == 0) {
+      mbar_arrive_tx(rfull, rb + (stall ? 16u : 0u));  // a stalled stage expects 16 bytes no copy delivers
+      const float *xsrc = g.X + (meta.n + (MODE == PRED ? 0 : g.koff)) * g.ldx;
+      bulk_g2s(smem_u32(sm + Smem::XN + ms * 256), xsrc, rb, rfull);
+    }
+    const int32_t *cidx = reinterpret_cast<const int32_t *>(sm + Smem::CIDX) + ms * MT;
+    const int h = lane >> 4, k = lane & 15;
+    const bool kin = 16 * k < (int)rb;
+    const uint32_t dst0 = smem_u32(sm + Smem::RAW + (uint32_t)s * MT * RAW_STRIDE) + 16u * k;
+    const int cnt = meta.cnt;
+    for (int p = h; p < cnt; p += 2) {
+      const int32_t c = cidx[p];
+      if (kin && c >= 0) {
+        const float *src = ((MODE == PRED) ? g.Y + (int64_t)c * g.ldy : g.X + (int64_t)c * g.ldx) + 4 * k;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst0 + (uint32_t)p * RAW_STRIDE), "l"(src)
+                     : "memory");
       }
     }
-    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(rfull)) : "memory");
   }
 
   // --------------------------------------------------------------- converter
@@ -555,9 +585,10 @@ struct Kern {
                                                    uint32_t acc_sel, uint64_t *mma_done) {
     const uint32_t tile = smem_u32(sm + Smem::TILE);
     if (MODE == MSTEP) {
-      // [H; B] (+)= [G_hi; G_lo]^T G_hi over the tile's pairs, 8 per MMA
-      const uint32_t idesc = idesc_tf32(128, DP, 0, 0);
-      const uint32_t td = tmem + acc_sel * 64u;
+      // [G_hi; G_lo]^T [G_hi, G_lo] over the tile's pairs, 8 per MMA: the
+      // four blocks hh, hl, lh, ll of (G_hi + G_lo)^T (G_hi + G_lo)
+      const uint32_t idesc = idesc_tf32(128, MN, 0, 0);
+      const uint32_t td = tmem + acc_sel * ACC_COLS;
       const int ng = (meta.cnt + 7) / 8;
       for (int gi = 0; gi < ng; ++gi) {
         const uint32_t a = tile + (uint32_t)gi * 256u;
@@ -566,7 +597,7 @@ struct Kern {
       }
     } else {
       const uint32_t idesc = idesc_tf32(128, DP, 0, 0);
-      const uint32_t td = tmem + acc_sel * 64u;
+      const uint32_t td = tmem + acc_sel * ACC_COLS;
       const uint32_t bhi = smem_u32(sm + Smem::BST + (uint32_t)meta.bs * 2 * Smem::B_BYTES);
       const uint32_t blo = bhi + Smem::B_BYTES;
       const int nt = g.nt;
@@ -588,24 +619,28 @@ struct Kern {
     const int warp = tid >> 5;
     if (MODE == MSTEP) {
       if (!(meta.flags & 2)) return;
-      // every accumulator row to shared memory (H rows 0-63, B rows 64-127),
-      // then S_ij = H_ij + B_ij + B_ji, lower triangle
+      // accumulator row i < 64 holds (hh_ij, hl_ij) in columns (j, 64 + j),
+      // row 64 + i holds (lh_ij, ll_ij): each thread adds its row's two
+      // halves into shared memory, then S_ij = red_ij + red_(64+i)j over the
+      // lower triangle
       float *red = reinterpret_cast<float *>(sm + Smem::RED);
       const bool empty = (meta.cnt == 0) && (meta.flags & 1);
       if (tid < 128) {
-        const uint32_t taddr = tmem + acc_sel * 64u + ((uint32_t)(warp * 32) << 16);
+        const uint32_t taddr = tmem + acc_sel * ACC_COLS + ((uint32_t)(warp * 32) << 16);
 #pragma unroll
         for (int c0 = 0; c0 < DP; c0 += 16) {
-          float v[16];
+          float v[16], u[16];
           if (!empty) {
             tmem_ld16(taddr + c0, v);
+            tmem_ld16(taddr + 64 + c0, u);
           } else {
 #pragma unroll
-            for (int k = 0; k < 16; ++k) v[k] = 0.f;
+            for (int k = 0; k < 16; ++k) v[k] = u[k] = 0.f;
           }
 #pragma unroll
           for (int k = 0; k < 16; k += 4)
-            *reinterpret_cast<float4 *>(red + tid * Smem::RSTR + c0 + k) = make_float4(v[k], v[k + 1], v[k + 2], v[k + 3]);
+            *reinterpret_cast<float4 *>(red + tid * Smem::RSTR + c0 + k) =
+                make_float4(v[k] + u[k], v[k + 1] + u[k + 1], v[k + 2] + u[k + 2], v[k + 3] + u[k + 3]);
         }
       }
       fence_before();
@@ -613,7 +648,7 @@ struct Kern {
       const int64_t n = meta.n;
       const bool bad = (meta.flags & 4) != 0;
       const int D = g.D;
-      const float *H = red, *Bm = red + 64 * Smem::RSTR;
+      const float *Uh = red, *Vl = red + 64 * Smem::RSTR;
       if (tid == 0) g.nu_out[n] = bad ? NAN : g.nu0 + meta.rsum;
       if (g.SPo) {
         float *dst = g.SPo + n * (int64_t)(g.ntile * 128);
@@ -624,7 +659,7 @@ struct Kern {
           const int J = t - I * (I + 1) / 2;
           const int i = 8 * I + (e >> 3), j = 8 * J + (e & 7);
           float v = 0.f;
-          if (i < D && j <= i) v = (H[i * Smem::RSTR + j] + Bm[i * Smem::RSTR + j]) + Bm[j * Smem::RSTR + i];
+          if (i < D && j <= i) v = Vl[i * Smem::RSTR + j] + Uh[i * Smem::RSTR + j];
           dst[t * 128 + e] = bad ? NAN : v;
         }
       } else {
@@ -633,7 +668,7 @@ struct Kern {
           const int i = q / D, j = q % D;
           if (g.lower_only && j > i) continue;
           const int a = i > j ? i : j, b = i > j ? j : i;  // symmetric: from the lower triangle
-          Sn[q] = bad ? NAN : (H[a * Smem::RSTR + b] + Bm[a * Smem::RSTR + b]) + Bm[b * Smem::RSTR + a];
+          Sn[q] = bad ? NAN : Vl[a * Smem::RSTR + b] + Uh[a * Smem::RSTR + b];
         }
       }
       asm volatile("bar.sync 1, %0;" ::"n"(NTHR) : "memory");
@@ -641,7 +676,7 @@ struct Kern {
     }
     if (tid >= 128) return;
     // lane = pair (query) row
-    const uint32_t taddr = tmem + acc_sel * 64u + ((uint32_t)(warp * 32) << 16);
+    const uint32_t taddr = tmem + acc_sel * ACC_COLS + ((uint32_t)(warp * 32) << 16);
     float q = 0.f;
 #pragma unroll
     for (int c0 = 0; c0 < DP; c0 += 16) {
@@ -677,36 +712,50 @@ struct Kern {
   }
 };
 
+// Warps 0-7 convert, issue the MMAs (thread 0) and run the epilogue; warp 8
+// writes the tile metadata up to NS - 2 tiles ahead; warp 9 gathers the pair
+// rows, kernel centres and W cores one tile ahead.
+constexpr int NWARPS = NTHR / 32 + 2;
+
 template <int MODE, int DP>
-__global__ void __launch_bounds__(NTHR, 1) tc_kernel(Args g) {
+__global__ void __launch_bounds__(NTHR + 64, 1) tc_kernel(Args g) {
   using K = Kern<MODE, DP>;
   extern __shared__ __align__(1024) unsigned char sm[];
   __shared__ uint32_t s_tmem;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   uint64_t *bars = reinterpret_cast<uint64_t *>(sm + Smem::BAR);
-  uint64_t *xfull = bars;         // [2] metadata + kernel centre of tile t (t & 1)
-  uint64_t *mma_done = bars + 2;  // MMAs of tile t committed
-  uint64_t *bfull = bars + 3;     // [2] W cores of a B stage
+  uint64_t *mfull = bars + Bars::MFULL, *mempty = bars + Bars::MEMPTY;
+  uint64_t *rfull = bars + Bars::RFULL, *rempty = bars + Bars::REMPTY;
+  uint64_t *bfull = bars + Bars::BFULL, *bempty = bars + Bars::BEMPTY;
+  uint64_t *mma_done = bars + Bars::MMA;
+  const Meta *metas = reinterpret_cast<const Meta *>(sm + Smem::META);
 
   // zero the operand tile (cores past DP stay zero) and the B stages (cores above the block diagonal)
-  for (uint32_t o = tid * 16; o < Smem::RAW; o += NTHR * 16) *reinterpret_cast<uint4 *>(sm + o) = make_uint4(0, 0, 0, 0);
+  for (uint32_t o = tid * 16; o < Smem::RAW; o += NWARPS * 32 * 16)
+    *reinterpret_cast<uint4 *>(sm + o) = make_uint4(0, 0, 0, 0);
   if (MODE != MSTEP)
-    for (uint32_t o = tid * 16; o < 4 * Smem::B_BYTES; o += NTHR * 16)
+    for (uint32_t o = tid * 16; o < 4 * Smem::B_BYTES; o += NWARPS * 32 * 16)
       *reinterpret_cast<uint4 *>(sm + Smem::BST + o) = make_uint4(0, 0, 0, 0);
   if (MODE == PRED) {
     float *pm = reinterpret_cast<float *>(sm + Smem::PM);
-    for (int i = tid; i < PQ; i += NTHR) {
+    for (int i = tid; i < PQ; i += NWARPS * 32) {
       pm[i] = -INFINITY;
       pm[PQ + i] = 0.f;
     }
   }
-  if (warp == 0) tmem_alloc(&s_tmem, 128);
+  if (warp == 0) tmem_alloc(&s_tmem, 2 * K::ACC_COLS);
   if (tid == 0) {
-    mbar_init(xfull, 32);
-    mbar_init(xfull + 1, 32);
+    for (int i = 0; i < NS; ++i) {
+      mbar_init(mfull + i, 32);
+      mbar_init(mempty + i, 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(rfull + i, 33);
+      mbar_init(rempty + i, 1);
+      mbar_init(bfull + i, 1);
+      mbar_init(bempty + i, 1);
+    }
     mbar_init(mma_done, 1);
-    mbar_init(bfull, 1);
-    mbar_init(bfull + 1, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   fence_async_smem();
@@ -714,89 +763,122 @@ __global__ void __launch_bounds__(NTHR, 1) tc_kernel(Args g) {
   __syncthreads();
   fence_after();
   const uint32_t tmem = s_tmem;
-  const Meta *metas = reinterpret_cast<const Meta *>(sm + Smem::META);
 
-  // prologue: tiles 0 and 1 staged, tile 0's W cores and pair rows in flight
-  typename K::Prod P{};
-  P.n = -1;
-  P.next = 0;
-  P.end = 0;
-  P.done = false;
-  if (warp == 0) {
-    K::produce(g, P, sm, xfull, 0, lane);
-    K::produce(g, P, sm, xfull + 1, 1, lane);
-  }
-  __syncthreads();
-  if (warp == 0) K::copy_w(g, sm, bfull, 0, lane);
-  K::gather_rows(g, sm, 0, 0, tid);
-
-  bool ok = true;
-  int t = 0;
-  int row_acc = 0;  // M-step: accumulator of the current row
-  int prev_acc = 0;
-  for (;;) {
-    const int s = t & 1, ms = t & 3;
-    const Meta &meta = metas[ms];
+  if (warp == NWARPS - 2) {
+    // ---------------------------------------------------- metadata warp
+    typename K::Prod P{};
+    P.n = -1;
+    for (int i = 0;; ++i) {
+      const int ms = i % NS;
+      if (i >= NS && !mbar_wait(mempty + ms, (uint32_t)((i / NS - 1) & 1))) {
+        if (lane == 0) atomicExch(g.err, 1);
+        break;
+      }
+      if (!K::produce(g, P, sm, mfull + ms, ms, lane)) break;
+    }
+  } else if (warp == NWARPS - 1) {
+    // ------------------------------------------------------ gather warp
+    int issued = 0;        // tiles whose copies this warp issued
+    int wlast0 = -1, wlast1 = -1;  // parity of the last W copy into B stage 0 / 1
+    bool first_tile = true;
+    for (int i = 0;; ++i) {
+      const int ms = i % NS, s = i & 1;
+      if (!mbar_wait(mfull + ms, (uint32_t)((i / NS) & 1))) {
+        if (lane == 0) atomicExch(g.err, 1);
+        break;
+      }
+      const Meta &meta = metas[ms];
+      if (meta.n < 0) break;
+      if (i >= 2 && !mbar_wait(rempty + s, (uint32_t)((i / 2 - 1) & 1))) {
+        if (lane == 0) atomicExch(g.err, 1);
+        break;
+      }
+      if (MODE != MSTEP && (meta.flags & 1)) {
+        if ((meta.flags & 8) && !mbar_wait(bempty + meta.bs, (uint32_t)(meta.bph ^ 1))) {
+          if (lane == 0) atomicExch(g.err, 1);
+          break;
+        }
+        K::copy_w(g, sm, meta, bfull + meta.bs, lane);
+        if (meta.bs) wlast1 = meta.bph;
+        else wlast0 = meta.bph;
+      }
+      K::gather(g, sm, meta, s, ms, rfull + s, g.stall && first_tile, lane);
+      first_tile = false;
+      issued = i + 1;
+    }
+    // nothing of this warp's stays in flight: its row copies, then (bounded)
+    // the last phases of the stages it filled
     asm volatile("cp.async.wait_all;" ::: "memory");
-    bool w = mbar_wait(xfull + s, (uint32_t)((t >> 1) & 1));
-    if (MODE != MSTEP && meta.n >= 0 && (meta.flags & 1)) w = mbar_wait(bfull + meta.bs, (uint32_t)meta.bph) && w;
-    if (t > 0) w = mbar_wait(mma_done, (uint32_t)((t - 1) & 1)) && w;
-    ok = __syncthreads_and(w ? 1 : 0) != 0;
-    if (!ok) break;
-    fence_after();
-    const bool stop = meta.n < 0;
-    uint32_t acc_sel = (uint32_t)s;
-    if (!stop) {
-      // tile t + 1: W cores (first tile of a row) and pair rows; tile t + 2: metadata
-      if (warp == 0) K::copy_w(g, sm, bfull, (t + 1) & 3, lane);
-      K::gather_rows(g, sm, s ^ 1, (t + 1) & 3, tid);
-      if (warp == 0) K::produce(g, P, sm, xfull + s, (t + 2) & 3, lane);
-      if (MODE == MSTEP) {
-        if (meta.flags & 1) row_acc ^= 1;
-        acc_sel = (uint32_t)row_acc;
+    for (int i = issued - 2; i < issued; ++i)
+      if (i >= 0) mbar_wait(rfull + (i & 1), (uint32_t)((i / 2) & 1));
+    if (wlast0 >= 0) mbar_wait(bfull, (uint32_t)wlast0);
+    if (wlast1 >= 0) mbar_wait(bfull + 1, (uint32_t)wlast1);
+  } else {
+    // -------------------------------------------------- consumer warps
+    bool ok = true;
+    int t = 0;
+    int row_acc = 0;  // M-step: accumulator of the current row
+    int prev_acc = 0;
+    for (;; ++t) {
+      const int ms = t % NS, s = t & 1;
+      bool w = mbar_wait(mfull + ms, (uint32_t)((t / NS) & 1));
+      const Meta &meta = metas[ms];
+      const bool stop = w && meta.n < 0;
+      if (w && !stop) {
+        w = mbar_wait(rfull + s, (uint32_t)((t / 2) & 1));
+        if (w && MODE != MSTEP && (meta.flags & 1)) w = mbar_wait(bfull + meta.bs, (uint32_t)meta.bph);
       }
-      K::convert(g, sm, s, ms, tid);
-      fence_async_smem();
-      fence_before();
-      __syncthreads();
-      if (tid == 0) {
-        fence_after();
-        K::issue_mma(g, sm, meta, tmem, acc_sel, mma_done);
-      }
-    }
-    if (t > 0) {
+      if (t > 0) w = mbar_wait(mma_done, (uint32_t)((t - 1) & 1)) && w;
+      ok = bar_and(2, NTHR, w);
+      if (!ok) break;
       fence_after();
-      K::epilogue(g, sm, (t - 1) & 3, tmem, (uint32_t)prev_acc, tid);
-      fence_before();
+      // tile t - 2's epilogue ran in the last iteration: its slot is free
+      if (tid == 0 && t >= 2) mbar_arrive(mempty + (t - 2) % NS);
+      uint32_t acc_sel = (uint32_t)s;
+      if (!stop) {
+        if (MODE == MSTEP) {
+          if (meta.flags & 1) row_acc ^= 1;
+          acc_sel = (uint32_t)row_acc;
+        }
+        K::convert(g, sm, s, ms, tid);
+        fence_async_smem();
+        fence_before();
+        bar_sync(2, NTHR);
+        if (tid == 0) {
+          fence_after();
+          mbar_arrive(rempty + s);
+          K::issue_mma(g, sm, meta, tmem, acc_sel, mma_done);
+          if (MODE != MSTEP && (meta.flags & 2)) commit(bempty + meta.bs);
+        }
+      }
+      if (t > 0) {
+        fence_after();
+        K::epilogue(g, sm, (t - 1) % NS, tmem, (uint32_t)prev_acc, tid);
+        fence_before();
+      }
+      prev_acc = (int)acc_sel;
+      if (stop) break;
     }
-    prev_acc = (int)acc_sel;
-    if (stop) break;
-    ++t;
-  }
-  if (!ok) {
-    // Wait (bounded) for this CTA's copies and MMAs still in flight before
-    // leaving: the staging of tiles t and t + 1, tile t's W cores, tile t - 1's MMAs.
-    if (tid == 0) {
-      atomicExch(g.err, 1);
-      mbar_wait(xfull + (t & 1), (uint32_t)((t >> 1) & 1));
-      mbar_wait(xfull + ((t + 1) & 1), (uint32_t)(((t + 1) >> 1) & 1));
-      const Meta &meta = metas[t & 3];
-      if (MODE != MSTEP && meta.n >= 0 && (meta.flags & 1)) mbar_wait(bfull + meta.bs, (uint32_t)meta.bph);
-      if (t > 0) mbar_wait(mma_done, (uint32_t)((t - 1) & 1));
+    if (!ok) {
+      // the MMAs of tile t - 1 may still run: wait (bounded) before leaving
+      if (tid == 0) {
+        atomicExch(g.err, 1);
+        if (t > 0) mbar_wait(mma_done, (uint32_t)((t - 1) & 1));
+      }
     }
-  }
-  if (MODE == PRED) {
-    __syncthreads();
-    const float *pm = reinterpret_cast<const float *>(sm + Smem::PM);
-    for (int64_t i = tid; i < g.qn; i += NTHR) {
-      g.ws_m[(int64_t)blockIdx.x * g.Nq + g.q0 + i] = pm[i];
-      g.ws_s[(int64_t)blockIdx.x * g.Nq + g.q0 + i] = pm[PQ + i];
+    if (MODE == PRED) {
+      bar_sync(2, NTHR);
+      const float *pm = reinterpret_cast<const float *>(sm + Smem::PM);
+      for (int64_t i = tid; i < g.qn; i += NTHR) {
+        g.ws_m[(int64_t)blockIdx.x * g.Nq + g.q0 + i] = pm[i];
+        g.ws_s[(int64_t)blockIdx.x * g.Nq + g.q0 + i] = pm[PQ + i];
+      }
     }
   }
   fence_before();
   __syncthreads();
   fence_after();
-  if (warp == 0) tmem_dealloc(tmem, 128);
+  if (warp == 0) tmem_dealloc(tmem, 2 * K::ACC_COLS);
 }
 
 // out[q] = -log N + logsumexp over the chunks' (max, sum) partials
@@ -922,7 +1004,7 @@ int launch_rows(const char *what, tc::Args g, int64_t rows, void *stream) {
   int64_t grid = sm_count();
   if (grid > rows) grid = rows;
   if (grid < 1) grid = 1;
-  kern<<<(unsigned)grid, tc::NTHR, smem, as_stream(stream)>>>(g);
+  kern<<<(unsigned)grid, tc::NTHR + 64, smem, as_stream(stream)>>>(g);
   return check_launch(what);
 }
 
@@ -1166,7 +1248,7 @@ extern "C" int lakde_log_pred_density_tc(int dtype, int64_t N, int64_t Nq, int64
     for (int64_t q0 = 0; q0 < Nq; q0 += tc::PQ) {
       g.q0 = q0;
       g.qn = (Nq - q0) < tc::PQ ? (Nq - q0) : tc::PQ;
-      kern<<<(unsigned)grid, tc::NTHR, smem, as_stream(stream)>>>(g);
+      kern<<<(unsigned)grid, tc::NTHR + 64, smem, as_stream(stream)>>>(g);
       if (int s2 = check_launch("log_pred_density_tc")) return s2;
     }
     return (int)LAKDE_OK;

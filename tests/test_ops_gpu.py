@@ -654,8 +654,10 @@ def test_bounded_wait_times_out_sets_err_and_the_engine_raises(K):
     tiny = torch.tensor(1e-6, device=DEV)
     eng = FusedKNN(Xt, graph, PairPattern.from_knn_graph(graph), float(D), tiny, tiny, 0.0, 8)
     eng.check_errors()
-    st = nat.lib().lakde_tc_wait_timeout_probe(N, D, N, nat.ptr(t(rowptr)), nat.ptr(t(cols, torch.int32)),
-                                               nat.ptr(Xp), Xp.stride(0), nat.ptr(Wc), nat.ptr(nu), nat.ptr(logdet),
+    # the device buffers stay referenced until the launch has completed
+    rowptr_d, cols_d = t(rowptr), t(cols, torch.int32)
+    st = nat.lib().lakde_tc_wait_timeout_probe(N, D, N, nat.ptr(rowptr_d), nat.ptr(cols_d), nat.ptr(Xp),
+                                               Xp.stride(0), nat.ptr(Wc), nat.ptr(nu), nat.ptr(logdet),
                                                nat.ptr(out), nat.ptr(eng.err), nat.stream_of(out))
     nat.check(st, "tc_wait_timeout_probe")
     torch.cuda.synchronize()
