@@ -8,8 +8,10 @@ static stride, the fused D <= 8 pass with 8 lanes or one thread per kernel
 row.  Which is faster depends on D, N and the pair counts, so the
 fused engine times every choice on its own data before its first CUDA-graph
 capture and keeps the fastest, per knob and class of D (the library's table
-is process-wide).  Every choice gives the same results; the state the timed
-launches modify is saved and restored around the tuning.
+is process-wide).  The factorisation and row-schedule choices give identical
+results; the two forms of the fused D <= 8 pass sum a row's pairs in
+different orders, so they agree to rounding.  The state the timed launches
+modify is saved and restored around the tuning.
 """
 
 import torch

@@ -338,7 +338,10 @@ def test_fused_checkpoint_round_trip_is_bit_identical(d, precision):
 
     Xn, _ = heavy_tail_mixture(seed=4, n_train=4000, n_test=10, d=d)
     X = torch.tensor(Xn.astype(np.float32), device=DEV)
-    kw = dict(k_or_knn_graph=16, fused=True, cuda_graph=True, precision=precision)
+    # fixed launch forms: the two forms of the fused D <= 8 pass sum in
+    # different orders, so a run that tuned to the other form differs in the
+    # last bits
+    kw = dict(k_or_knn_graph=16, fused=True, cuda_graph=True, precision=precision, autotune=False)
     whole = LocalKNearestKDE(**kw).fit(X, iterations=5, sparsity_threshold=5e-4)
     first = LocalKNearestKDE(**kw).fit(X, iterations=3, sparsity_threshold=5e-4)
     buf = io.BytesIO()
