@@ -182,8 +182,8 @@ template <int DP, bool LEAN = false>
 struct DmmaCfg {
   static constexpr int NT = DP / 8;
   static constexpr int NTILE = NT * (NT + 1) / 2;
-  // LEAN: no per-matrix T_n staged and no L output (the tiled path with its
-  // trace from the E-step): ~19 KB per warp at DP = 64, one warp per block,
+  // LEAN: no per-matrix T_n staged (the trace reads its tiles from global
+  // memory) and no L output: ~19 KB per warp at DP = 64, one warp per block,
   // 11 blocks per SM (registers capped to fit)
   static constexpr int WPB = LEAN ? 1 : 2;
   static constexpr int BLOCKS_PER_SM = LEAN ? 11 : 1;
@@ -419,7 +419,7 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
   double *rdiag = M + C::off_rdiag;
   // per-matrix FP32 T_n goes through shared memory with the other inputs
   const bool tiled = sizeof(T) == 4 && g.SP != nullptr;
-  const bool staged = sizeof(T) == 4 && !g.L && ((g.Tm && g.Tbs != 0) || (tiled && g.Tt));
+  const bool staged = !LEAN && sizeof(T) == 4 && !g.L && ((g.Tm && g.Tbs != 0) || (tiled && g.Tt));
   float *tstage = staged ? reinterpret_cast<float *>(M + C::off_tstage) : nullptr;
   const int D = g.D;
   const T scale = posterior_scale(g, n);
@@ -598,6 +598,57 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
     }
     acc = warp_sum(acc);
     if (lane == 0) g.trace[n] = (T)acc;
+  } else if (tiled && g.Tt) {
+    // the same product with the tiles of T_n read from global memory (the
+    // lean form stages none): column block Ac + 1's B fragments are loaded
+    // while block Ac's products run
+    const float *tt = reinterpret_cast<const float *>(g.Tt) + n * (int64_t)(C::NTILE * 64);
+    const int fo = (lane & 3) * 8 + (lane >> 2);
+    float tb[NT][2];
+#pragma unroll
+    for (int K = 0; K < NT; ++K) {
+      tb[K][0] = tt[(K * (K + 1) / 2) * 64 + fo];
+      tb[K][1] = tt[(K * (K + 1) / 2) * 64 + fo + 32];
+    }
+    double acc = 0.0;
+#pragma unroll 1
+    for (int Ac = 0; Ac < NT; ++Ac) {
+      double b[NT][2];
+#pragma unroll
+      for (int K = 0; K < NT; ++K) {
+        b[K][0] = (double)tb[K][0];
+        b[K][1] = (double)tb[K][1];
+      }
+      if (Ac + 1 < NT) {
+#pragma unroll
+        for (int K = 0; K < NT; ++K) {
+          if (K >= Ac + 1) {
+            tb[K][0] = tt[(K * (K + 1) / 2 + Ac + 1) * 64 + fo];
+            tb[K][1] = tt[(K * (K + 1) / 2 + Ac + 1) * 64 + fo + 32];
+          }
+        }
+      }
+      double cacc[NT][2];
+#pragma unroll
+      for (int I = 0; I < NT; ++I) {
+        cacc[I][0] = 0.0;
+        cacc[I][1] = 0.0;
+      }
+#pragma unroll
+      for (int K = 0; K < NT; ++K) {
+        if (K < Ac) continue;
+#pragma unroll
+        for (int I = K; I < NT; ++I) {
+          const double *x = M + dmma::tix(I, K);
+          dmma::mma(cacc[I][0], cacc[I][1], dmma::afrag(x, 0, lane), b[K][0]);
+          dmma::mma(cacc[I][0], cacc[I][1], dmma::afrag(x, 1, lane), b[K][1]);
+        }
+      }
+#pragma unroll
+      for (int I = 0; I < NT; ++I) acc = fma(cacc[I][0], cacc[I][0], fma(cacc[I][1], cacc[I][1], acc));
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) g.trace[n] = (T)acc;
   } else if (Tn) {
     // ||X T_n||_F^2 with X lower: (X T)_IA = sum_{K <= I} X_IK T_KA, column
     // block by column block, the next block's loads issued before this one's
@@ -689,11 +740,12 @@ static int launch_factor_dmma_v(const FactorArgs<TT> &g, int64_t N, void *stream
   return check_launch("posterior_factor");
 }
 
-// The lean variant when the call stages no T_n and writes no L and the
-// tuning table selects it (lakde_tuning_set, knob LAKDE_TUNE_FACTOR).
+// The lean variant (no staged T_n: tiles of T_n are read from global memory)
+// when the call writes no L, takes no dense T_n, and the tuning table selects
+// it (lakde_tuning_set, knob LAKDE_TUNE_FACTOR).
 template <typename TT, int DP>
 static int launch_factor_dmma(const FactorArgs<TT> &g, int64_t N, void *stream) {
-  const bool lean_ok = !g.L && !g.Tm && !g.Tt;
+  const bool lean_ok = !g.L && !g.Tm;
   if (lean_ok && tuning(LAKDE_TUNE_FACTOR, g.D) == 1) return launch_factor_dmma_v<TT, DP, true>(g, N, stream);
   return launch_factor_dmma_v<TT, DP, false>(g, N, stream);
 }

@@ -81,3 +81,31 @@ def test_cpu_tensors_are_rejected():
     with pytest.raises((RuntimeError, NotImplementedError)):
         kernels.calc_W_inv(torch.zeros(5, dtype=torch.int64), torch.zeros(0, dtype=torch.int64), torch.zeros(0),
                            X, X)
+
+
+def test_tuning_table_round_trip_and_rejects_bad_choices(nat):
+    """lakde_tuning_set / _get: one entry per knob and class of D (<= 16, 32,
+    48, 64); unknown knobs, out-of-range D and choices are rejected."""
+    from lakde_b200 import tuning
+
+    lib = nat.lib()
+    saved = {(k, d): lib.lakde_tuning_get(idx, d) for k, (idx, _, _) in tuning.KNOBS.items() for d in (8, 21, 40, 63)}
+    try:
+        for knob, (idx, names, _) in tuning.KNOBS.items():
+            for d_set, d_same, d_other in ((8, 16, 17), (21, 32, 33), (40, 48, 49), (63, 64, 16)):
+                for choice in names:
+                    tuning.set_choice(knob, d_set, choice)
+                    assert tuning.get_choice(knob, d_same) == choice
+                other = names[0]
+                tuning.set_choice(knob, d_set, other)
+                tuning.set_choice(knob, d_other, names[1])
+                assert tuning.get_choice(knob, d_set) == other
+        assert lib.lakde_tuning_set(3, 8, 0) != 0
+        assert lib.lakde_tuning_set(-1, 8, 0) != 0
+        assert lib.lakde_tuning_set(0, 0, 0) != 0
+        assert lib.lakde_tuning_set(0, 65, 0) != 0
+        assert lib.lakde_tuning_set(0, 8, 2) != 0
+        assert "no choice" in lib.lakde_last_error().decode()
+    finally:
+        for (k, d), v in saved.items():
+            assert lib.lakde_tuning_set(tuning.KNOBS[k][0], d, v) == 0

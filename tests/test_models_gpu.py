@@ -171,6 +171,76 @@ def test_mixed_precision_within_1e3_nats_of_fp64():
         assert abs(out[name][0] - out["fp64"][0]) <= 1e-4 * abs(out["fp64"][0]), (name, out)
 
 
+def test_heavy_tail_d8_fp32_and_mixed_within_1e3_nats_of_fp64():
+    """The d=8 workload at its size: 200,000 training and 20,000 held-out
+    points of the standardised heavy-tail mixture (9 full-covariance
+    Gaussians, one Student-t component), K=50, 20 iterations, threshold 5e-4,
+    one kNN graph and candidate pattern for all: plain FP32 (the fused
+    register pass) and mixed precision (tensor-core tf32 hi / lo) against
+    FP64, held-out mean log density within 1e-3 nats."""
+    from lakde_b200 import LocalKNearestKDE
+    from lakde_b200.synthetic import heavy_tail_mixture
+    from lakde_b200.utils import compute_knn_graph
+
+    Xn, Yn = heavy_tail_mixture(seed=0, n_train=200_000, n_test=20_000, d=8)
+    X64 = torch.tensor(Xn.astype(np.float64), device=DEV)
+    Y64 = torch.tensor(Yn.astype(np.float64), device=DEV)
+    graph = compute_knn_graph(X64, 50)
+    out = {}
+    for name, dt, prec in (("fp64", torch.float64, "fp32"), ("fp32", torch.float32, "fp32"),
+                           ("mixed", torch.float32, "mixed")):
+        m = LocalKNearestKDE(k_or_knn_graph=graph, fused=True, cuda_graph=True, precision=prec)
+        m.fit(X64.to(dt), iterations=20, sparsity_threshold=5e-4)
+        m.check_errors_()
+        assert m.engine.precision == prec
+        out[name] = (m.log_pred_density(X64.to(dt), Y64.to(dt)).double().mean().item(),
+                     float(m.compute_elbo(X64.to(dt))))
+        del m
+        torch.cuda.empty_cache()
+    print("held-out mean log density and ELBO:", out)
+    for name in ("fp32", "mixed"):
+        assert abs(out[name][0] - out["fp64"][0]) <= 1e-3, (name, out)
+        assert abs(out[name][1] - out["fp64"][1]) <= 1e-4 * abs(out["fp64"][1]), (name, out)
+
+
+def test_knn_pattern_gap_to_the_dense_reference():
+    """What restricting the E-step to the kNN pairs costs, in FP64: the fused
+    kNN pattern against the reference at block_size = N (every pair), on the
+    2-d circle mixture (2,000 points, K=20, 10 iterations; the reference's own
+    trajectory from the golden vectors) and on a 20,000-point subsample of the
+    d=8 heavy-tail mixture (K=50, 20 iterations; the fused all-pairs pattern,
+    which reproduces the reference at block_size = N).  The ELBO and held-out
+    log-density gaps are printed and bounded."""
+    from lakde_b200 import LocalKNearestKDE
+    from lakde_b200.synthetic import heavy_tail_mixture
+
+    g = load("knn_c1_f64_bN")
+    X = torch.tensor(g["X"], device=DEV)
+    Y = torch.tensor(g["Y"], device=DEV)
+    m = LocalKNearestKDE(k_or_knn_graph=torch.tensor(g["knn_graph"], device=DEV), fused=True, candidates="knn")
+    rec = Rec()
+    m.fit(X, iterations=10, callbacks=rec)
+    gaps = {"circle2d": (rec.elbo[-1] - float(g["elbo"][-1]),
+                         float(m.log_pred_density(X, Y).mean()) - float(np.mean(g["ll"])))}
+
+    Xn, Yn = heavy_tail_mixture(seed=1, n_train=20_000, n_test=2_000, d=8)
+    X = torch.tensor(Xn.astype(np.float64), device=DEV)
+    Y = torch.tensor(Yn.astype(np.float64), device=DEV)
+    res = {}
+    for cand in ("knn", "dense"):
+        m = LocalKNearestKDE(k_or_knn_graph=50, fused=True, candidates=cand, cuda_graph=True)
+        m.fit(X, iterations=20)
+        m.check_errors_()
+        res[cand] = (float(m.compute_elbo(X)), float(m.log_pred_density(X, Y).mean()))
+        del m
+        torch.cuda.empty_cache()
+    gaps["heavy_tail8_20k"] = (res["knn"][0] - res["dense"][0], res["knn"][1] - res["dense"][1])
+    print("kNN pattern minus all pairs (ELBO, held-out mean log density):", gaps, res)
+    for name, (d_elbo, d_ll) in gaps.items():
+        assert np.isfinite(d_elbo) and np.isfinite(d_ll), name
+        assert abs(d_ll) <= 0.05, (name, gaps)
+
+
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
 def test_hierarchical_uneven_neighbourhoods_match_restricted_oracle(dtype):
     """d=43 data on a 10-dim subspace plus 1e-3 noise (near-singular local
