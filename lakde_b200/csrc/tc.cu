@@ -293,147 +293,215 @@ struct Kern {
   static constexpr uint32_t ACC_COLS = MODE == MSTEP ? 128u : 64u;
 
   // ------------------------------------------------------- metadata warp
-  // Row state of the metadata warp (uniform over its lanes).
+  // State of the metadata warp.  Rows are fetched 32 at a time, lane j
+  // holding row j of the batch (its index, pair range and row constants:
+  // the dependent loads and the digamma sums of 32 rows run side by side);
+  // tiles are planned from the batch, and each tile's column indices and
+  // weights are loaded one tile before they are written.
   struct Prod {
-    int64_t n;        // current row
-    int64_t next;     // first pair of the current row's next tile
-    int64_t end;      // end of the current row
-    int64_t popped;   // rows taken by this CTA
-    int rows;         // rows started by this CTA (their parity selects the B stage / accumulator)
-    int bpar;         // bit b: parity of the next use of B stage b (its W-copy mbarrier phase)
-    int bused;        // bit b: B stage b has been used
-    float racc;       // M-step: running sum of r over the row
-    int bad;          // M-step: invalid index seen in the row
-    float c0, c1;     // row constants of the E-step / predictive density
+    int64_t bn, ba, bb;  // this lane's batch row: kernel (-1: none) and pair range
+    float bc0, bc1;      // its row constants
+    int bsz, bidx;       // rows in the batch, next one to start
+    int64_t popped;      // row slots taken by this CTA
+    bool exhausted;      // no rows left to fetch
     bool done;
+    int64_t n, next, end;  // current row and the first pair of its next tile
+    int rows;            // rows started (their parity selects the B stage / accumulator)
+    int bpar, bused;     // bit b: parity of the next use of B stage b, stage b used
+    float c0, c1;
+    int rowbad;          // the current row's pair range is invalid
+    float racc;          // M-step: running sum of r over the row (at write time)
+    int bad;             // M-step: invalid index seen in the row (at write time)
   };
 
-  // Next kernel row of this CTA, or -1: the work queue (an atomic counter
-  // over the caller's row order), a static stride over the grid without a
-  // queue, or the CTA's contiguous chunk of kernels for the predictive density.
-  static __device__ __forceinline__ int64_t pop_row(const Args &g, Prod &P, int lane) {
+  struct Plan {
+    int64_t n, base;
+    int cnt, flags, bs, bph;
+    float c0, c1;
+  };
+
+  // The next 32 row slots of this CTA: the work queue (an atomic counter
+  // over the caller's row order, 32 slots per claim), a static stride over
+  // the grid without a queue, or the CTA's contiguous chunk of kernels for the
+  // predictive density.  Valid slots are a prefix of the lanes.
+  static __device__ void fetch_batch(const Args &g, Prod &P, int lane) {
     int64_t it;
+    bool valid = true;
     if (MODE == PRED) {
-      if (P.popped >= g.chunk) return -1;
-      it = (int64_t)blockIdx.x * g.chunk + P.popped;
+      valid = P.popped + lane < g.chunk;
+      it = (int64_t)blockIdx.x * g.chunk + P.popped + lane;
     } else if (g.queue) {
       int v = 0;
-      if (lane == 0) v = atomicAdd(g.queue, 1);
-      it = __shfl_sync(0xffffffffu, v, 0);
+      if (lane == 0) v = atomicAdd(g.queue, 32);
+      it = (int64_t)__shfl_sync(0xffffffffu, v, 0) + lane;
     } else {
-      it = (int64_t)blockIdx.x + P.popped * (int64_t)gridDim.x;
+      it = (int64_t)blockIdx.x + (P.popped + lane) * (int64_t)gridDim.x;
     }
-    ++P.popped;
-    if (it >= g.N) return -1;
-    return (MODE != PRED && g.order) ? (int64_t)g.order[it] : it;
+    P.popped += 32;
+    valid = valid && it < g.N;
+    int64_t n = -1, a = 0, b = 0;
+    float c0 = 0.f, c1 = 0.f;
+    if (valid) {
+      n = (MODE != PRED && g.order) ? (int64_t)g.order[it] : it;
+      if (MODE != PRED) {
+        a = g.rowptr[n];
+        b = g.rowptr[n + 1];
+      } else {
+        b = g.qn;
+      }
+      if (MODE == ESTEP) {
+        // 0.5 (psi_D(nu / 2) + D log 2 + logdet W), -nu / 2
+        const float nv = g.nu[n];
+        const float ld = g.logdet[n];
+        double md = 0.0;
+        for (int i = 1; i <= g.D; ++i) md += digamma_d(0.5 * (double)nv + 0.5 * (1 - i));
+        c0 = (float)(0.5 * (md + g.D * 0.69314718055994530942 + (double)ld));
+        c1 = -0.5f * nv;
+      } else if (MODE == PRED) {
+        c0 = g.lc[n];
+        c1 = 0.5f * (g.nu[n] + 1.f);
+      }
+    }
+    P.bn = n;
+    P.ba = a;
+    P.bb = b;
+    P.bc0 = c0;
+    P.bc1 = c1;
+    P.bsz = __popc(__ballot_sync(0xffffffffu, valid));
+    P.bidx = 0;
+    if (P.bsz < 32) P.exhausted = true;
   }
 
-  // Writes the next tile's metadata into slot ms (or a stop marker when the
-  // CTA has no work left): row, pair range, column indices (validated) and
-  // weights, row constants.  Every lane arrives on mfull afterwards.
-  // Returns false for the stop marker.
-  static __device__ bool produce(const Args &g, Prod &P, unsigned char *sm, uint64_t *mfull, int ms, int lane) {
-    Meta *meta = reinterpret_cast<Meta *>(sm + Smem::META) + ms;
-    int32_t *cidx = reinterpret_cast<int32_t *>(sm + Smem::CIDX) + ms * MT;
-    float *rv = reinterpret_cast<float *>(sm + Smem::RV) + ms * MT;
+  // Plans the next tile (n < 0: no work left).
+  static __device__ Plan plan_tile(const Args &g, Prod &P, int lane) {
+    Plan t{};
     bool first = false;
     if (!P.done && P.next >= P.end) {
       for (;;) {
-        const int64_t n = pop_row(g, P, lane);
-        if (n < 0) {
-          P.done = true;
-          break;
+        if (P.bidx >= P.bsz) {
+          if (P.exhausted) {
+            P.done = true;
+            break;
+          }
+          fetch_batch(g, P, lane);
+          continue;
         }
-        int64_t a = 0, b = g.qn;
-        if (MODE != PRED) {
-          a = g.rowptr[n];
-          b = g.rowptr[n + 1];
-        }
+        const int j = P.bidx++;
+        const int64_t n = __shfl_sync(0xffffffffu, P.bn, j);
+        const int64_t a = __shfl_sync(0xffffffffu, P.ba, j);
+        const int64_t b = __shfl_sync(0xffffffffu, P.bb, j);
+        const float c0 = __shfl_sync(0xffffffffu, P.bc0, j);
+        const float c1 = __shfl_sync(0xffffffffu, P.bc1, j);
         if (MODE == ESTEP && b <= a) continue;  // no pairs: no log rho to write
         P.n = n;
         P.next = a;
         P.end = b < a ? a : b;  // an M-step row without pairs still gets one (empty) tile
-        P.racc = 0.f;
-        P.bad = b < a;
+        P.rowbad = b < a;
+        P.c0 = c0;
+        P.c1 = c1;
         first = true;
         ++P.rows;
-        if (MODE == ESTEP) {
-          // 0.5 (psi_D(nu / 2) + D log 2 + logdet W), -nu / 2: one digamma term per lane
-          const float nv = g.nu[n];
-          double md = 0.0;
-          for (int i = 1 + lane; i <= g.D; i += 32) md += digamma_d(0.5 * (double)nv + 0.5 * (1 - i));
-          md = warp_sum(md);
-          P.c0 = (float)(0.5 * (md + g.D * 0.69314718055994530942 + (double)g.logdet[n]));
-          P.c1 = -0.5f * nv;
-        } else if (MODE == PRED) {
-          P.c0 = g.lc[n];
-          P.c1 = 0.5f * (g.nu[n] + 1.f);
-        }
         break;
       }
     }
     if (P.done) {
+      t.n = -1;
+      return t;
+    }
+    t.n = P.n;
+    t.base = P.next;
+    t.cnt = (int)((P.end - P.next) < MT ? (P.end - P.next) : MT);
+    P.next += t.cnt;
+    const bool last = P.next >= P.end;
+    t.bs = (P.rows - 1) & 1;
+    t.bph = 0;
+    int reused = 0;
+    if (first) {
+      t.bph = (P.bpar >> t.bs) & 1;
+      reused = (P.bused >> t.bs) & 1;
+      P.bpar ^= 1 << t.bs;
+      P.bused |= 1 << t.bs;
+    }
+    t.flags = (first ? 1 : 0) | (last ? 2 : 0) | (P.rowbad ? 4 : 0) | (reused ? 8 : 0);
+    t.c0 = P.c0;
+    t.c1 = P.c1;
+    return t;
+  }
+
+  // Issues the loads of a planned tile's column indices and weights (4 pairs
+  // per lane).
+  static __device__ __forceinline__ void load_tile(const Args &g, const Plan &t, int lane, int32_t (&c)[4],
+                                                   float (&w)[4]) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int p = lane + 32 * k;
+      c[k] = -1;
+      w[k] = 0.f;
+      if (t.n >= 0 && p < t.cnt) {
+        if (MODE == PRED) {
+          c[k] = (int32_t)(g.q0 + t.base + p);
+        } else {
+          c[k] = g.col[t.base + p];
+          if (MODE == MSTEP) w[k] = g.r[t.base + p];
+        }
+      }
+    }
+  }
+
+  // Writes a planned tile (or the stop marker) into slot ms, validating its
+  // column indices, and arrives on mfull (every lane).
+  static __device__ void write_tile(const Args &g, Prod &P, const Plan &t, const int32_t (&c)[4],
+                                    const float (&w)[4], unsigned char *sm, uint64_t *mfull, int ms, int lane) {
+    Meta *meta = reinterpret_cast<Meta *>(sm + Smem::META) + ms;
+    if (t.n < 0) {
       if (lane == 0) meta->n = -1;
       mbar_arrive(mfull);
-      return false;
+      return;
     }
-    const int64_t n = P.n, base = P.next;
-    const int cnt = (int)((P.end - base) < MT ? (P.end - base) : MT);
-    P.next = base + cnt;
-    const bool last = P.next >= P.end;
+    int32_t *cidx = reinterpret_cast<int32_t *>(sm + Smem::CIDX) + ms * MT;
+    float *rv = reinterpret_cast<float *>(sm + Smem::RV) + ms * MT;
     unsigned bad = 0;
     float rs = 0.f;
 #pragma unroll
-    for (int k = 0; k < MT / 32; ++k) {
+    for (int k = 0; k < 4; ++k) {
       const int p = lane + 32 * k;
-      int32_t c = -1;
-      float w = 0.f;
-      if (p < cnt) {
-        if (MODE == PRED) {
-          c = (int32_t)(g.q0 + base + p);
-        } else {
-          c = g.col[base + p];
-          if (MODE == MSTEP) w = g.r[base + p];
-          if (c < 0 || c >= g.npts) {
-            c = -1;
-            w = 0.f;
-            bad = 1;
-          }
-        }
+      int32_t ck = c[k];
+      float wk = w[k];
+      if (MODE != PRED && p < t.cnt && (ck < 0 || ck >= g.npts)) {
+        ck = -1;
+        wk = 0.f;
+        bad = 1;
       }
-      cidx[p] = c;
+      cidx[p] = ck;
       if (MODE == MSTEP) {
-        rv[p] = w;
-        rs += w;
+        rv[p] = wk;
+        rs += wk;
       }
     }
+    int flags = t.flags;
     if (MODE == MSTEP) {
       bad = __reduce_or_sync(0xffffffffu, bad);
       rs = warp_sum(rs);
+      if (t.flags & 1) {
+        P.racc = 0.f;
+        P.bad = 0;
+      }
       P.racc += rs;
       P.bad |= (int)bad;
-    }
-    const int bs = (P.rows - 1) & 1;
-    int bph = 0, reused = 0;
-    if (first) {
-      bph = (P.bpar >> bs) & 1;
-      reused = (P.bused >> bs) & 1;
-      P.bpar ^= 1 << bs;
-      P.bused |= 1 << bs;
+      if (P.bad) flags |= 4;
     }
     if (lane == 0) {
-      meta->n = n;
-      meta->base = base;
-      meta->cnt = cnt;
-      meta->flags = (first ? 1 : 0) | (last ? 2 : 0) | (P.bad ? 4 : 0) | (reused ? 8 : 0);
-      meta->bs = bs;
-      meta->bph = bph;
-      meta->c0 = P.c0;
-      meta->c1 = P.c1;
+      meta->n = t.n;
+      meta->base = t.base;
+      meta->cnt = t.cnt;
+      meta->flags = flags;
+      meta->bs = t.bs;
+      meta->bph = t.bph;
+      meta->c0 = t.c0;
+      meta->c1 = t.c1;
       meta->rsum = P.racc;
     }
     mbar_arrive(mfull);
-    return true;
   }
 
   // --------------------------------------------------------- gather warp
@@ -768,13 +836,29 @@ __global__ void __launch_bounds__(NTHR + 64, 1) tc_kernel(Args g) {
     // ---------------------------------------------------- metadata warp
     typename K::Prod P{};
     P.n = -1;
+    typename K::Plan cur = K::plan_tile(g, P, lane), nxt{};
+    int32_t cc[4], nc[4];
+    float cw[4], nw[4];
+    K::load_tile(g, cur, lane, cc, cw);
     for (int i = 0;; ++i) {
       const int ms = i % NS;
+      if (cur.n >= 0) {
+        // the next tile's loads are in flight while this one is written
+        nxt = K::plan_tile(g, P, lane);
+        K::load_tile(g, nxt, lane, nc, nw);
+      }
       if (i >= NS && !mbar_wait(mempty + ms, (uint32_t)((i / NS - 1) & 1))) {
         if (lane == 0) atomicExch(g.err, 1);
         break;
       }
-      if (!K::produce(g, P, sm, mfull + ms, ms, lane)) break;
+      K::write_tile(g, P, cur, cc, cw, sm, mfull + ms, ms, lane);
+      if (cur.n < 0) break;
+      cur = nxt;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        cc[k] = nc[k];
+        cw[k] = nw[k];
+      }
     }
   } else if (warp == NWARPS - 1) {
     // ------------------------------------------------------ gather warp

@@ -290,7 +290,8 @@ class LocallyAdaptiveKDE(VIModel, ABC):
             v = getattr(self, k, None)
             if torch.is_tensor(v):
                 setattr(self, k, v.to(dev))
-        self.rnm_blocks = [(ind.to(dev), val.to(device=dev, dtype=X.dtype)) for ind, val in self.rnm_blocks]
+        if self.rnm_blocks is not None:  # None while a fused engine holds the responsibilities
+            self.rnm_blocks = [(ind.to(dev), val.to(device=dev, dtype=X.dtype)) for ind, val in self.rnm_blocks]
 
     def _restore_engine_state(self, eng):
         """Responsibilities and per-kernel / per-point state of a checkpoint into a

@@ -139,7 +139,8 @@ def test_cuda_graph_replay_equals_eager():
     X = torch.tensor(Xn, device=DEV)
     res = []
     for graph in (False, True):
-        m = LocalKNearestKDE(k_or_knn_graph=16, fused=True, cuda_graph=graph)
+        # fixed launch forms: both runs must take the same ones
+        m = LocalKNearestKDE(k_or_knn_graph=16, fused=True, cuda_graph=graph, autotune=False)
         m.fit(X, iterations=6, sparsity_threshold=5e-4)
         res.append((m.rnm_log_consts.clone(), m.engine.r.clone(), float(m.compute_elbo(X))))
     torch.testing.assert_close(res[0][0], res[1][0], rtol=0, atol=0)
