@@ -177,11 +177,13 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Round to the nearest tf32 (10 explicit mantissa bits; the low 13 bits zero).
+// Round to the nearest tf32, ties away from zero (10 explicit mantissa bits;
+// the low 13 bits zero): add half of the dropped range to the magnitude bits
+// and clear them.  Two integer ALU operations; finite inputs far below
+// FLT_MAX (centred differences and inverse factors) cannot carry into the
+// exponent's all-ones pattern.
 __device__ __forceinline__ float tf32_rna(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 
 __device__ __forceinline__ void split4(const float4 x, float4 &hi, float4 &lo) {
@@ -253,7 +255,8 @@ struct Bars {
   static constexpr int BFULL = REMPTY + 2; // [2] W cores of a B stage landed
   static constexpr int BEMPTY = BFULL + 2; // [2] MMAs of the stage's last row done (tcgen05.commit)
   static constexpr int MMA = BEMPTY + 2;   // MMAs of a tile done (tcgen05.commit)
-  static constexpr int COUNT = MMA + 1;
+  static constexpr int CONV = MMA + 1;     // tile converted (every consumer thread)
+  static constexpr int COUNT = CONV + 1;
 };
 static_assert(Bars::COUNT * 8 <= 256, "mbarrier area");
 
@@ -522,9 +525,10 @@ struct Kern {
   // The pair (query) rows of the tile in slot ms into raw stage s, and its
   // kernel centre into the slot's centre buffer, completing on mbarrier
   // rfull (33 arrivals: lane 0's byte count for the bulk copy, then one per
-  // lane when its cp.async copies have landed).  Half-warp h copies row
-  // 2 j + h, lane k % 16 its 16-byte chunk k: two 256-byte rows per
-  // instruction.
+  // lane when its cp.async copies have landed).  Half-warp h copies the row
+  // groups 4 (2 j + h) .. + 3, lane k % 16 the 16-byte chunk k of each row:
+  // two 256-byte rows per instruction, the group's four column indices read
+  // as one 16-byte word, four groups in flight.
   static __device__ __forceinline__ void gather(const Args &g, unsigned char *sm, const Meta &meta, int s, int ms,
                                                 uint64_t *rfull, bool stall, int lane) {
     const uint32_t rb = (uint32_t)(((g.D + 3) / 4) * 16);  // bytes per row
@@ -533,17 +537,26 @@ struct Kern {
       const float *xsrc = g.X + (meta.n + (MODE == PRED ? 0 : g.koff)) * g.ldx;
       bulk_g2s(smem_u32(sm + Smem::XN + ms * 256), xsrc, rb, rfull);
     }
-    const int32_t *cidx = reinterpret_cast<const int32_t *>(sm + Smem::CIDX) + ms * MT;
+    const int4 *cid4 = reinterpret_cast<const int4 *>(sm + Smem::CIDX + ms * MT * 4);
     const int h = lane >> 4, k = lane & 15;
     const bool kin = 16 * k < (int)rb;
     const uint32_t dst0 = smem_u32(sm + Smem::RAW + (uint32_t)s * MT * RAW_STRIDE) + 16u * k;
+    const float *base = ((MODE == PRED) ? g.Y : g.X) + 4 * k;
+    const int64_t ld = (MODE == PRED) ? g.ldy : g.ldx;
     const int cnt = meta.cnt;
-    for (int p = h; p < cnt; p += 2) {
-      const int32_t c = cidx[p];
-      if (kin && c >= 0) {
-        const float *src = ((MODE == PRED) ? g.Y + (int64_t)c * g.ldy : g.X + (int64_t)c * g.ldx) + 4 * k;
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst0 + (uint32_t)p * RAW_STRIDE), "l"(src)
-                     : "memory");
+#pragma unroll 4
+    for (int j = 0; j < MT / 8; ++j) {
+      const int grp = 2 * j + h;
+      if (4 * grp >= cnt) break;
+      const int4 c4 = cid4[grp];
+      const int cs[4] = {c4.x, c4.y, c4.z, c4.w};
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int p = 4 * grp + u;
+        if (kin && p < cnt && cs[u] >= 0)
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst0 + (uint32_t)p * RAW_STRIDE),
+                       "l"(base + (int64_t)cs[u] * ld)
+                       : "memory");
       }
     }
     asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(rfull)) : "memory");
@@ -780,13 +793,14 @@ struct Kern {
   }
 };
 
-// Warps 0-7 convert, issue the MMAs (thread 0) and run the epilogue; warp 8
-// writes the tile metadata up to NS - 2 tiles ahead; warp 9 gathers the pair
-// rows, kernel centres and W cores one tile ahead.
-constexpr int NWARPS = NTHR / 32 + 2;
+// Warps 0-7 convert and run the epilogue; warp 8 writes the tile metadata up
+// to NS - 2 tiles ahead; warp 9 gathers the pair rows, kernel centres and W
+// cores one tile ahead; warp 10 issues the MMAs of each converted tile.
+constexpr int NWARPS = NTHR / 32 + 3;
+constexpr int NTHR_ALL = NWARPS * 32;
 
 template <int MODE, int DP>
-__global__ void __launch_bounds__(NTHR + 64, 1) tc_kernel(Args g) {
+__global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
   using K = Kern<MODE, DP>;
   extern __shared__ __align__(1024) unsigned char sm[];
   __shared__ uint32_t s_tmem;
@@ -795,7 +809,7 @@ __global__ void __launch_bounds__(NTHR + 64, 1) tc_kernel(Args g) {
   uint64_t *mfull = bars + Bars::MFULL, *mempty = bars + Bars::MEMPTY;
   uint64_t *rfull = bars + Bars::RFULL, *rempty = bars + Bars::REMPTY;
   uint64_t *bfull = bars + Bars::BFULL, *bempty = bars + Bars::BEMPTY;
-  uint64_t *mma_done = bars + Bars::MMA;
+  uint64_t *mma_done = bars + Bars::MMA, *conv = bars + Bars::CONV;
   const Meta *metas = reinterpret_cast<const Meta *>(sm + Smem::META);
 
   // zero the operand tile (cores past DP stay zero) and the B stages (cores above the block diagonal)
@@ -824,6 +838,7 @@ __global__ void __launch_bounds__(NTHR + 64, 1) tc_kernel(Args g) {
       mbar_init(bempty + i, 1);
     }
     mbar_init(mma_done, 1);
+    mbar_init(conv, NTHR);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   fence_async_smem();
@@ -832,7 +847,39 @@ __global__ void __launch_bounds__(NTHR + 64, 1) tc_kernel(Args g) {
   fence_after();
   const uint32_t tmem = s_tmem;
 
-  if (warp == NWARPS - 2) {
+  if (warp == NWARPS - 1) {
+    // ----------------------------------------------------------- MMA warp
+    int row_acc = 0;  // M-step: accumulator of the current row
+    int last = -1;    // last tile whose MMAs were issued
+    for (int t = 0;; ++t) {
+      const int ms = t % NS, s = t & 1;
+      if (!mbar_wait(mfull + ms, (uint32_t)((t / NS) & 1))) {
+        if (lane == 0) atomicExch(g.err, 1);
+        break;
+      }
+      const Meta &meta = metas[ms];
+      if (meta.n < 0) break;
+      if (!mbar_wait(conv, (uint32_t)(t & 1))) {
+        if (lane == 0) atomicExch(g.err, 1);
+        break;
+      }
+      fence_after();
+      uint32_t acc_sel = (uint32_t)s;
+      if (MODE == MSTEP) {
+        if (meta.flags & 1) row_acc ^= 1;
+        acc_sel = (uint32_t)row_acc;
+      }
+      if (lane == 0) {
+        mbar_arrive(rempty + s);  // every converter has read raw stage s
+        K::issue_mma(g, sm, meta, tmem, acc_sel, mma_done);
+        if (MODE != MSTEP && (meta.flags & 2)) commit(bempty + meta.bs);
+      }
+      __syncwarp();
+      last = t;
+    }
+    // none of this warp's MMAs stays in flight (bounded wait)
+    if (last >= 0) mbar_wait(mma_done, (uint32_t)(last & 1));
+  } else if (warp == NWARPS - 3) {
     // ---------------------------------------------------- metadata warp
     typename K::Prod P{};
     P.n = -1;
@@ -925,15 +972,8 @@ __global__ void __launch_bounds__(NTHR + 64, 1) tc_kernel(Args g) {
           acc_sel = (uint32_t)row_acc;
         }
         K::convert(g, sm, s, ms, tid);
-        fence_async_smem();
-        fence_before();
-        bar_sync(2, NTHR);
-        if (tid == 0) {
-          fence_after();
-          mbar_arrive(rempty + s);
-          K::issue_mma(g, sm, meta, tmem, acc_sel, mma_done);
-          if (MODE != MSTEP && (meta.flags & 2)) commit(bempty + meta.bs);
-        }
+        fence_async_smem();  // the tile is read by the MMAs (async proxy)
+        mbar_arrive(conv);
       }
       if (t > 0) {
         fence_after();
@@ -943,13 +983,7 @@ __global__ void __launch_bounds__(NTHR + 64, 1) tc_kernel(Args g) {
       prev_acc = (int)acc_sel;
       if (stop) break;
     }
-    if (!ok) {
-      // the MMAs of tile t - 1 may still run: wait (bounded) before leaving
-      if (tid == 0) {
-        atomicExch(g.err, 1);
-        if (t > 0) mbar_wait(mma_done, (uint32_t)((t - 1) & 1));
-      }
-    }
+    if (!ok && tid == 0) atomicExch(g.err, 1);  // the MMA warp waits for its own MMAs
     if (MODE == PRED) {
       bar_sync(2, NTHR);
       const float *pm = reinterpret_cast<const float *>(sm + Smem::PM);
@@ -1088,7 +1122,7 @@ int launch_rows(const char *what, tc::Args g, int64_t rows, void *stream) {
   int64_t grid = sm_count();
   if (grid > rows) grid = rows;
   if (grid < 1) grid = 1;
-  kern<<<(unsigned)grid, tc::NTHR + 64, smem, as_stream(stream)>>>(g);
+  kern<<<(unsigned)grid, tc::NTHR_ALL, smem, as_stream(stream)>>>(g);
   return check_launch(what);
 }
 
@@ -1332,7 +1366,7 @@ extern "C" int lakde_log_pred_density_tc(int dtype, int64_t N, int64_t Nq, int64
     for (int64_t q0 = 0; q0 < Nq; q0 += tc::PQ) {
       g.q0 = q0;
       g.qn = (Nq - q0) < tc::PQ ? (Nq - q0) : tc::PQ;
-      kern<<<(unsigned)grid, tc::NTHR + 64, smem, as_stream(stream)>>>(g);
+      kern<<<(unsigned)grid, tc::NTHR_ALL, smem, as_stream(stream)>>>(g);
       if (int s2 = check_launch("log_pred_density_tc")) return s2;
     }
     return (int)LAKDE_OK;
