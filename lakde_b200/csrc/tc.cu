@@ -796,7 +796,9 @@ struct Kern {
 // Warps 0-7 convert and run the epilogue; warp 8 writes the tile metadata up
 // to NS - 2 tiles ahead; warp 9 gathers the pair rows, kernel centres and W
 // cores one tile ahead; warp 10 issues the MMAs of each converted tile.
-constexpr int NWARPS = NTHR / 32 + 3;
+// Named barriers 1 and 2 count the NTHR consumer threads exactly.
+constexpr int WARP_META = NTHR / 32, WARP_GATHER = WARP_META + 1, WARP_MMA = WARP_META + 2;
+constexpr int NWARPS = WARP_MMA + 1;
 constexpr int NTHR_ALL = NWARPS * 32;
 
 template <int MODE, int DP>
@@ -847,7 +849,7 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
   fence_after();
   const uint32_t tmem = s_tmem;
 
-  if (warp == NWARPS - 1) {
+  if (warp == WARP_MMA) {
     // ----------------------------------------------------------- MMA warp
     int row_acc = 0;  // M-step: accumulator of the current row
     int last = -1;    // last tile whose MMAs were issued
@@ -879,7 +881,7 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
     }
     // none of this warp's MMAs stays in flight (bounded wait)
     if (last >= 0) mbar_wait(mma_done, (uint32_t)(last & 1));
-  } else if (warp == NWARPS - 3) {
+  } else if (warp == WARP_META) {
     // ---------------------------------------------------- metadata warp
     typename K::Prod P{};
     P.n = -1;
@@ -907,7 +909,7 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
         cw[k] = nw[k];
       }
     }
-  } else if (warp == NWARPS - 1) {
+  } else if (warp == WARP_GATHER) {
     // ------------------------------------------------------ gather warp
     int issued = 0;        // tiles whose copies this warp issued
     int wlast0 = -1, wlast1 = -1;  // parity of the last W copy into B stage 0 / 1
@@ -944,7 +946,7 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
       if (i >= 0) mbar_wait(rfull + (i & 1), (uint32_t)((i / 2) & 1));
     if (wlast0 >= 0) mbar_wait(bfull, (uint32_t)wlast0);
     if (wlast1 >= 0) mbar_wait(bfull + 1, (uint32_t)wlast1);
-  } else {
+  } else if (warp < WARP_META) {
     // -------------------------------------------------- consumer warps
     bool ok = true;
     int t = 0;
