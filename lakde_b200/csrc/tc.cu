@@ -14,27 +14,27 @@
 // memory.  The M-step forms all four blocks of (G_hi + G_lo)^T (G_hi + G_lo):
 // dropping lo*lo there would take a positive semi-definite 2^-24-relative
 // term off S, which shrinks exactly the small eigenvalues of a near-singular
-// neighbourhood.  The E-step forms hi*hi + lo*hi + hi*lo: its dropped lo*lo
-// and the rounding of lo are below 2^-22 relative with random sign.
+// neighbourhood.  The E-step likewise forms all four products of
+// (D_hi + D_lo) (W_hi + W_lo) (two MMAs per K step against [W_hi | W_lo]);
+// what remains is the rounding of lo, below 2^-22 relative with random sign.
 //
-// One persistent CTA per SM, 256 threads, software-pipelined over 128-pair
-// tiles:
-//   * warp 0 (producer) pops kernel rows from an atomic row queue (rows in
-//     the caller's longest-first order: a pair-count-balanced schedule) and
-//     stages tile t + 2: its column indices / weights in shared memory and a
-//     bulk copy of the kernel centre (on that stage's mbarrier); for the
-//     first tile of a row, one tile ahead, it bulk-copies the row's W cores
-//     into one of two B stages;
-//   * all threads gather tile t + 1's pair rows (rows of X padded to a
-//     multiple of 16 bytes) with 16-byte cp.async copies, a whole iteration
-//     ahead of their use;
-//   * all 8 warps convert tile t: centre, (M-step: scale by sqrt r), split
-//     into the hi / lo core-matrix tile, and for the first tile of a row split
-//     the row's W cores in place;
-//   * thread 0 issues the MMAs of tile t into one of two TMEM accumulators and
-//     commits them to an mbarrier;
-//   * while they run, warps 0-3 read the previous tile's accumulator (one TMEM
-//     lane per pair) and write log rho / S_n / the running log-sum-exp.
+// One persistent CTA per SM, 352 threads in four roles, pipelined over
+// 128-pair tiles with mbarriers:
+//   * a metadata warp takes kernel rows 32 at a time (an atomic row queue
+//     over the caller's longest-first order, or a static stride), one lane
+//     per row for the dependent loads and the E-step's digamma sums, and
+//     writes each tile's row, pair range, column indices and weights into a
+//     ring of 8 slots, loading the next tile's indices while it writes one;
+//   * a gather warp copies each tile's pair rows (rows of X padded to a
+//     multiple of 16 bytes) into one of two raw stages with cp.async, its
+//     kernel centre and, for the first tile of a row, the row's W cores into
+//     one of two B stages by bulk copy, after the stage's last MMAs committed;
+//   * 8 consumer warps convert tile t (centre, M-step: scale by sqrt r, split
+//     into the hi / lo core-matrix tile, for the first tile of a row split the
+//     W cores in place) and read the previous tile's accumulator (one TMEM
+//     lane per pair) to write log rho / S_n / the running log-sum-exp;
+//   * an MMA warp issues each converted tile's MMAs into one of two TMEM
+//     accumulators and commits them to mbarriers.
 // Every wait is bounded: on a time-out the kernel sets *err, waits (bounded)
 // for its own copies and MMAs in flight, frees its TMEM and returns.
 //
@@ -51,8 +51,10 @@
 //          GT_SBO (next 8 rows); GT_SBO = 4112 rather than 4096 keeps the
 //          converters' 16-byte stores on distinct bank groups.
 //   B      W cores (K-major, N = output dim i, K = input dim j, element (i, j)
-//          = W_triu[j][i] = X[i][j] with X = L^-1 lower): per K step J the row
-//          groups I = 0..NT-1 of 2 cores each, LBO = 128, SBO = 256.
+//          = W_triu[j][i] = X[i][j] with X = L^-1 lower): per K step J the
+//          2 DP / 8 row groups of 2 cores each, the hi parts of output
+//          blocks I = 0..DP/8-1 then their lo parts; LBO = 128, SBO = 256,
+//          N = 2 DP.
 #include "common.cuh"
 
 namespace lakde {
@@ -177,6 +179,30 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 16 consecutive fp32 columns at each of two TMEM addresses of this thread's
+// lane, one wait for both.
+__device__ __forceinline__ void tmem_ld16x2(uint32_t ta, uint32_t tb, float (&v)[16], float (&u)[16]) {
+  uint32_t r[16], q[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(ta));
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];\n"
+      : "=r"(q[0]), "=r"(q[1]), "=r"(q[2]), "=r"(q[3]), "=r"(q[4]), "=r"(q[5]), "=r"(q[6]), "=r"(q[7]),
+        "=r"(q[8]), "=r"(q[9]), "=r"(q[10]), "=r"(q[11]), "=r"(q[12]), "=r"(q[13]), "=r"(q[14]), "=r"(q[15])
+      : "r"(tb));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    v[i] = __uint_as_float(r[i]);
+    u[i] = __uint_as_float(q[i]);
+  }
+}
+
 // Round to the nearest tf32, ties away from zero (10 explicit mantissa bits;
 // the low 13 bits zero): add half of the dropped range to the magnitude bits
 // and clear them.  Two integer ALU operations; finite inputs far below
@@ -292,8 +318,10 @@ struct Kern {
   // M-step accumulator columns: the hi rows 0..63 of G^T, then its lo rows
   // 64..64 + DP (rounded up to 16, the MMA's N granule)
   static constexpr int MN = 64 + ((DP + 15) / 16) * 16;
-  // TMEM columns of one accumulator (two are allocated)
-  static constexpr uint32_t ACC_COLS = MODE == MSTEP ? 128u : 64u;
+  // TMEM columns of one accumulator (two are allocated): the M-step's
+  // [hi | lo] rows of G^T, the E-step's [hi | lo] output columns
+  static constexpr uint32_t ACC_COLS = 128u;
+  static constexpr int NG = DP / 8;  // 8-row groups of one half of a B stage's K step
 
   // ------------------------------------------------------- metadata warp
   // State of the metadata warp.  Rows are fetched 32 at a time, lane j
@@ -511,14 +539,13 @@ struct Kern {
   // The W cores of the row starting at the tile in slot ms into its B stage
   // (the E-step and the predictive density), on mbarrier bfull.
   static __device__ void copy_w(const Args &g, unsigned char *sm, const Meta &meta, uint64_t *bfull, int lane) {
-    constexpr int NG = DP / 8;  // row groups of a K step in the B stage
     const float *wsrc = g.Wc + meta.n * (int64_t)(g.ntile * 64);
-    unsigned char *bhi = sm + Smem::BST + (uint32_t)meta.bs * 2 * Smem::B_BYTES;
+    unsigned char *bst = sm + Smem::BST + (uint32_t)meta.bs * 2 * Smem::B_BYTES;
     if (lane == 0) mbar_arrive_tx(bfull, (uint32_t)g.ntile * 256u);
     __syncwarp();
     for (int J = lane; J < g.nt; J += 32) {
       const uint32_t seg_bytes = (uint32_t)(g.nt - J) * 256u;
-      bulk_g2s(smem_u32(bhi + J * NG * 256 + J * 256), wsrc + wseg(J, g.nt), seg_bytes, bfull);
+      bulk_g2s(smem_u32(bst + (J * 2 * NG + J) * 256), wsrc + wseg(J, g.nt), seg_bytes, bfull);
     }
   }
 
@@ -638,9 +665,8 @@ struct Kern {
       *reinterpret_cast<float4 *>(dst + 2048 + k * 128) = lo;
     }
     if (MODE != MSTEP && (meta.flags & 1)) {
-      // W cores of the row: hi in place, lo beside it (the copied cores only)
-      unsigned char *bhi = sm + Smem::BST + (uint32_t)meta.bs * 2 * Smem::B_BYTES;
-      unsigned char *blo = bhi + Smem::B_BYTES;
+      // W cores of the row: hi in place, lo NG groups further (the copied cores only)
+      unsigned char *bst = sm + Smem::BST + (uint32_t)meta.bs * 2 * Smem::B_BYTES;
       const int nt = g.nt, nchunk = g.ntile * 16;
       for (int q = tid; q < nchunk; q += NTHR) {
         const int t = q >> 4, e = q & 15;
@@ -651,12 +677,12 @@ struct Kern {
           ++J;
         }
         const int I = J + rem;
-        const uint32_t o = (uint32_t)(J * (DP / 8) * 256 + I * 256 + e * 16);
-        const float4 v = *reinterpret_cast<const float4 *>(bhi + o);
+        const uint32_t o = (uint32_t)((J * 2 * NG + I) * 256 + e * 16);
+        const float4 v = *reinterpret_cast<const float4 *>(bst + o);
         float4 hi, lo;
         split4(v, hi, lo);
-        *reinterpret_cast<float4 *>(bhi + o) = hi;
-        *reinterpret_cast<float4 *>(blo + o) = lo;
+        *reinterpret_cast<float4 *>(bst + o) = hi;
+        *reinterpret_cast<float4 *>(bst + o + NG * 256) = lo;
       }
     }
   }
@@ -677,16 +703,17 @@ struct Kern {
         mma_tf32(td, desc(a, 128, GT_SBO), desc(a, 128, GT_SBO), idesc, acc);
       }
     } else {
-      const uint32_t idesc = idesc_tf32(128, DP, 0, 0);
+      // [D_hi; D_lo] [W_hi | W_lo] per K step: output columns 0..DP-1 take
+      // the products with W_hi, DP..2 DP-1 those with W_lo (all four hi / lo
+      // products; the epilogue adds the halves)
+      const uint32_t idesc = idesc_tf32(128, 2 * DP, 0, 0);
       const uint32_t td = tmem + acc_sel * ACC_COLS;
-      const uint32_t bhi = smem_u32(sm + Smem::BST + (uint32_t)meta.bs * 2 * Smem::B_BYTES);
-      const uint32_t blo = bhi + Smem::B_BYTES;
+      const uint32_t bst = smem_u32(sm + Smem::BST + (uint32_t)meta.bs * 2 * Smem::B_BYTES);
       const int nt = g.nt;
       for (int J = 0; J < nt; ++J) {
-        const uint32_t ao = (uint32_t)J * 256u, bo = (uint32_t)(J * (DP / 8) * 256);
-        mma_tf32(td, desc(tile + ao, 128, 4096), desc(bhi + bo, 128, 256), idesc, J > 0);
-        mma_tf32(td, desc(tile + 2048 + ao, 128, 4096), desc(bhi + bo, 128, 256), idesc, 1);
-        mma_tf32(td, desc(tile + ao, 128, 4096), desc(blo + bo, 128, 256), idesc, 1);
+        const uint32_t ao = (uint32_t)J * 256u, bo = (uint32_t)(J * 2 * NG * 256);
+        mma_tf32(td, desc(tile + ao, 128, 4096), desc(bst + bo, 128, 256), idesc, J > 0);
+        mma_tf32(td, desc(tile + 2048 + ao, 128, 4096), desc(bst + bo, 128, 256), idesc, 1);
       }
     }
     commit(mma_done);
@@ -712,8 +739,7 @@ struct Kern {
         for (int c0 = 0; c0 < DP; c0 += 16) {
           float v[16], u[16];
           if (!empty) {
-            tmem_ld16(taddr + c0, v);
-            tmem_ld16(taddr + 64 + c0, u);
+            tmem_ld16x2(taddr + c0, taddr + 64 + c0, v, u);
           } else {
 #pragma unroll
             for (int k = 0; k < 16; ++k) v[k] = u[k] = 0.f;
@@ -732,16 +758,26 @@ struct Kern {
       const float *Uh = red, *Vl = red + 64 * Smem::RSTR;
       if (tid == 0) g.nu_out[n] = bad ? NAN : g.nu0 + meta.rsum;
       if (g.SPo) {
+        // four consecutive columns of one tile row per store: tile t = I (I +
+        // 1) / 2 + J (I from the root of 8 t + 1, exact at these sizes), row
+        // r = e / 2, columns 8 J + 4 (e % 2) + 0..3
         float *dst = g.SPo + n * (int64_t)(g.ntile * 128);
-        for (int q = tid; q < g.ntile * 64; q += NTHR) {
-          const int t = q >> 6, e = q & 63;
-          int I = 0;
-          while ((I + 1) * (I + 2) / 2 <= t) ++I;
+        for (int q = tid; q < g.ntile * 16; q += NTHR) {
+          const int t = q >> 4, e = q & 15;
+          const int I = (int)((sqrtf(8.f * (float)t + 1.f) - 1.f) * 0.5f);
           const int J = t - I * (I + 1) / 2;
-          const int i = 8 * I + (e >> 3), j = 8 * J + (e & 7);
-          float v = 0.f;
-          if (i < D && j <= i) v = Vl[i * Smem::RSTR + j] + Uh[i * Smem::RSTR + j];
-          dst[t * 128 + e] = bad ? NAN : v;
+          const int i = 8 * I + (e >> 1), j = 8 * J + 4 * (e & 1);
+          float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (i < D) {
+            const float4 a = *reinterpret_cast<const float4 *>(Vl + i * Smem::RSTR + j);
+            const float4 b = *reinterpret_cast<const float4 *>(Uh + i * Smem::RSTR + j);
+            v.x = (j <= i) ? a.x + b.x : 0.f;
+            v.y = (j + 1 <= i) ? a.y + b.y : 0.f;
+            v.z = (j + 2 <= i) ? a.z + b.z : 0.f;
+            v.w = (j + 3 <= i) ? a.w + b.w : 0.f;
+          }
+          if (bad) v = make_float4(NAN, NAN, NAN, NAN);
+          *reinterpret_cast<float4 *>(dst + t * 128 + (e >> 1) * 8 + 4 * (e & 1)) = v;
         }
       } else {
         float *Sn = g.S + n * (int64_t)D * D;
@@ -761,10 +797,15 @@ struct Kern {
     float q = 0.f;
 #pragma unroll
     for (int c0 = 0; c0 < DP; c0 += 16) {
-      float v[16];
-      tmem_ld16(taddr + c0, v);
+      float v[16], u[16];
+      tmem_ld16x2(taddr + c0, taddr + DP + c0, v, u);
 #pragma unroll
-      for (int k = 0; k < 16; ++k) q = fmaf(v[k], v[k], q);
+      for (int k = 0; k < 16; ++k) {
+        if (c0 + k < DP) {  // columns past 2 DP are not written by the MMAs
+          const float y = v[k] + u[k];
+          q = fmaf(y, y, q);
+        }
+      }
     }
     const int p = tid;
     if (p >= meta.cnt) return;
