@@ -646,45 +646,63 @@ struct Kern {
     const int p = tid & (MT - 1), h = tid >> 7;
     const int cvalid = (p < meta.cnt) ? cidx[p] : -1;
     unsigned char *dst = tile + (uint32_t)(p >> 3) * 4096u + (uint32_t)(p & 7) * 16u;
+    // four chunks at a time: all their loads before any store (the stores
+    // into the tile would otherwise order the next loads behind them)
 #pragma unroll
-    for (int i = 0; i < HCH; ++i) {
-      const int k = h * HCH + i;
-      float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (cvalid >= 0 && k < rch) {
-        const float4 x = *reinterpret_cast<const float4 *>(raw + p * RAW_STRIDE + k * 16);
-        const float4 c = xn[k];
-        const int d0 = 4 * k;
-        d.x = x.x - c.x;
-        d.y = (d0 + 1 < D) ? x.y - c.y : 0.f;
-        d.z = (d0 + 2 < D) ? x.z - c.z : 0.f;
-        d.w = (d0 + 3 < D) ? x.w - c.w : 0.f;
-      }
-      float4 hi, lo;
-      split4(d, hi, lo);
-      *reinterpret_cast<float4 *>(dst + k * 128) = hi;
-      *reinterpret_cast<float4 *>(dst + 2048 + k * 128) = lo;
-    }
-    if (MODE != MSTEP && (meta.flags & 1)) {
-      // W cores of the row: hi in place, lo NG groups further (the copied cores only)
-      unsigned char *bst = sm + Smem::BST + (uint32_t)meta.bs * 2 * Smem::B_BYTES;
-      const int nt = g.nt, nchunk = g.ntile * 16;
-      for (int q = tid; q < nchunk; q += NTHR) {
-        const int t = q >> 4, e = q & 15;
-        // tile t of the segment order: segment J, row block I >= J
-        int J = 0, rem = t;
-        while (rem >= nt - J) {
-          rem -= nt - J;
-          ++J;
+    for (int i0 = 0; i0 < HCH; i0 += 4) {
+      float4 x[4], c[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int k = h * HCH + i0 + i;
+        x[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        c[i] = x[i];
+        if (i0 + i < HCH && cvalid >= 0 && k < rch) {
+          x[i] = *reinterpret_cast<const float4 *>(raw + p * RAW_STRIDE + k * 16);
+          c[i] = xn[k];
         }
-        const int I = J + rem;
-        const uint32_t o = (uint32_t)((J * 2 * NG + I) * 256 + e * 16);
-        const float4 v = *reinterpret_cast<const float4 *>(bst + o);
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int k = h * HCH + i0 + i;
+        if (i0 + i >= HCH) continue;
+        const int d0 = 4 * k;
+        float4 d;
+        d.x = x[i].x - c[i].x;
+        d.y = (d0 + 1 < D) ? x[i].y - c[i].y : 0.f;
+        d.z = (d0 + 2 < D) ? x[i].z - c[i].z : 0.f;
+        d.w = (d0 + 3 < D) ? x[i].w - c[i].w : 0.f;
         float4 hi, lo;
-        split4(v, hi, lo);
-        *reinterpret_cast<float4 *>(bst + o) = hi;
-        *reinterpret_cast<float4 *>(bst + o + NG * 256) = lo;
+        split4(d, hi, lo);
+        *reinterpret_cast<float4 *>(dst + k * 128) = hi;
+        *reinterpret_cast<float4 *>(dst + 2048 + k * 128) = lo;
       }
     }
+  }
+
+  // The W cores of the row starting at the tile of meta, split in place by
+  // the MMA warp (lane of 32): hi where they landed, lo NG groups further
+  // (the copied cores only), then made visible to the MMAs.
+  static __device__ void split_w(const Args &g, unsigned char *sm, const Meta &meta, int lane) {
+    unsigned char *bst = sm + Smem::BST + (uint32_t)meta.bs * 2 * Smem::B_BYTES;
+    const int nt = g.nt, nchunk = g.ntile * 16;
+    for (int q = lane; q < nchunk; q += 32) {
+      const int t = q >> 4, e = q & 15;
+      // tile t of the segment order: segment J, row block I >= J
+      int J = 0, rem = t;
+      while (rem >= nt - J) {
+        rem -= nt - J;
+        ++J;
+      }
+      const int I = J + rem;
+      const uint32_t o = (uint32_t)((J * 2 * NG + I) * 256 + e * 16);
+      const float4 v = *reinterpret_cast<const float4 *>(bst + o);
+      float4 hi, lo;
+      split4(v, hi, lo);
+      *reinterpret_cast<float4 *>(bst + o) = hi;
+      *reinterpret_cast<float4 *>(bst + o + NG * 256) = lo;
+    }
+    fence_async_smem();
+    __syncwarp();
   }
 
   // ---------------------------------------------------------------- MMAs
@@ -892,8 +910,10 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
 
   if (warp == WARP_MMA) {
     // ----------------------------------------------------------- MMA warp
-    int row_acc = 0;  // M-step: accumulator of the current row
-    int last = -1;    // last tile whose MMAs were issued
+    int row_acc = 0;   // M-step: accumulator of the current row
+    int last = -1;     // last tile whose MMAs were issued
+    int split = -1;    // last tile whose row's W cores this warp has split
+    bool fail = false;
     for (int t = 0;; ++t) {
       const int ms = t % NS, s = t & 1;
       if (!mbar_wait(mfull + ms, (uint32_t)((t / NS) & 1))) {
@@ -902,6 +922,14 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
       }
       const Meta &meta = metas[ms];
       if (meta.n < 0) break;
+      if (MODE != MSTEP && (meta.flags & 1) && split != t) {
+        if (!mbar_wait(bfull + meta.bs, (uint32_t)meta.bph)) {
+          if (lane == 0) atomicExch(g.err, 1);
+          break;
+        }
+        K::split_w(g, sm, meta, lane);
+        split = t;
+      }
       if (!mbar_wait(conv, (uint32_t)(t & 1))) {
         if (lane == 0) atomicExch(g.err, 1);
         break;
@@ -919,6 +947,21 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
       }
       __syncwarp();
       last = t;
+      if (MODE != MSTEP) {
+        // while these MMAs run: the W cores of the next tile's row, if it starts one
+        const int t1 = t + 1, ms1 = t1 % NS;
+        if (!mbar_wait(mfull + ms1, (uint32_t)((t1 / NS) & 1))) fail = true;
+        const Meta &m1 = metas[ms1];
+        if (!fail && m1.n >= 0 && (m1.flags & 1)) {
+          if (!mbar_wait(bfull + m1.bs, (uint32_t)m1.bph)) fail = true;
+          else K::split_w(g, sm, m1, lane);
+          split = t1;
+        }
+        if (fail) {
+          if (lane == 0) atomicExch(g.err, 1);
+          break;
+        }
+      }
     }
     // none of this warp's MMAs stays in flight (bounded wait)
     if (last >= 0) mbar_wait(mma_done, (uint32_t)(last & 1));
@@ -998,10 +1041,7 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
       bool w = mbar_wait(mfull + ms, (uint32_t)((t / NS) & 1));
       const Meta &meta = metas[ms];
       const bool stop = w && meta.n < 0;
-      if (w && !stop) {
-        w = mbar_wait(rfull + s, (uint32_t)((t / 2) & 1));
-        if (w && MODE != MSTEP && (meta.flags & 1)) w = mbar_wait(bfull + meta.bs, (uint32_t)meta.bph);
-      }
+      if (w && !stop) w = mbar_wait(rfull + s, (uint32_t)((t / 2) & 1));
       if (t > 0) w = mbar_wait(mma_done, (uint32_t)((t - 1) & 1)) && w;
       ok = bar_and(2, NTHR, w);
       if (!ok) break;
