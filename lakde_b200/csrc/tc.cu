@@ -505,7 +505,7 @@ struct Kern {
       }
       cidx[p] = ck;
       if (MODE == MSTEP) {
-        rv[p] = wk;
+        rv[p] = sqrtf(wk > 0.f ? wk : 0.f);  // the converters scale by sqrt(r)
         rs += wk;
       }
     }
@@ -603,28 +603,40 @@ struct Kern {
       // G^T: unit (pair quad q, dim chunk k) reads the chunk of its 4 pairs
       // (consecutive units: consecutive chunks, distinct bank groups), forms
       // sqrt(r) (x_m - x_n), and writes per dim the 4 pairs as one 16-byte
-      // row of a core, hi at row d, lo at row 64 + d
+      // row of a core, hi at row d, lo at row 64 + d.  Both units' loads are
+      // issued before any store.
+      const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+      float4 xs[2][4], ccs[2];
+      float ws[2][4];
 #pragma unroll
       for (int s2 = 0; s2 < 2; ++s2) {
         const int u = tid + NTHR * s2;
         const int q = u >> 4, k = u & 15;
-        float4 dq[4];
+        ccs[s2] = (k < rch) ? xn[k] : z4;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
           const int p = 4 * q + i;
-          const int c = (p < meta.cnt) ? cidx[p] : -1;
-          float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (c >= 0 && k < rch) {
-            const float rr = rv[p];
-            const float w = sqrtf(rr > 0.f ? rr : 0.f);
-            const float4 x = *reinterpret_cast<const float4 *>(raw + p * RAW_STRIDE + k * 16);
-            const float4 cc = xn[k];
-            const int d0 = 4 * k;
-            d.x = (x.x - cc.x) * w;
-            d.y = (d0 + 1 < D) ? (x.y - cc.y) * w : 0.f;
-            d.z = (d0 + 2 < D) ? (x.z - cc.z) * w : 0.f;
-            d.w = (d0 + 3 < D) ? (x.w - cc.w) * w : 0.f;
-          }
+          const bool ok = p < meta.cnt && k < rch && cidx[p] >= 0;
+          ws[s2][i] = ok ? rv[p] : 0.f;
+          xs[s2][i] = ok ? *reinterpret_cast<const float4 *>(raw + p * RAW_STRIDE + k * 16) : z4;
+        }
+      }
+#pragma unroll
+      for (int s2 = 0; s2 < 2; ++s2) {
+        const int u = tid + NTHR * s2;
+        const int q = u >> 4, k = u & 15;
+        const float4 cc = ccs[s2];
+        const int d0 = 4 * k;
+        float4 dq[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const float4 x = xs[s2][i];
+          const float w = ws[s2][i];
+          float4 d;
+          d.x = (x.x - cc.x) * w;
+          d.y = (d0 + 1 < D) ? (x.y - cc.y) * w : 0.f;
+          d.z = (d0 + 2 < D) ? (x.z - cc.z) * w : 0.f;
+          d.w = (d0 + 3 < D) ? (x.w - cc.w) * w : 0.f;
           dq[i] = d;
         }
 #pragma unroll
@@ -684,22 +696,36 @@ struct Kern {
   // (the copied cores only), then made visible to the MMAs.
   static __device__ void split_w(const Args &g, unsigned char *sm, const Meta &meta, int lane) {
     unsigned char *bst = sm + Smem::BST + (uint32_t)meta.bs * 2 * Smem::B_BYTES;
-    const int nt = g.nt, nchunk = g.ntile * 16;
-    for (int q = lane; q < nchunk; q += 32) {
-      const int t = q >> 4, e = q & 15;
-      // tile t of the segment order: segment J, row block I >= J
-      int J = 0, rem = t;
-      while (rem >= nt - J) {
-        rem -= nt - J;
-        ++J;
+    const int nt = g.nt, e = lane & 15;
+    // half-warp h takes every other tile of the segment order (segment J,
+    // row block I >= J), lane e its 16-byte chunk e; four tiles' loads in
+    // flight before their stores
+    int J = 0, I = 0;
+    auto adv = [&]() {
+      if (++I >= nt) I = ++J;
+    };
+    if (lane >> 4) adv();
+    while (J < nt) {
+      uint32_t o[4];
+      float4 v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        o[u] = 0xFFFFFFFFu;
+        if (J < nt) {
+          o[u] = (uint32_t)((J * 2 * NG + I) * 256 + e * 16);
+          v[u] = *reinterpret_cast<const float4 *>(bst + o[u]);
+          adv();
+          adv();
+        }
       }
-      const int I = J + rem;
-      const uint32_t o = (uint32_t)((J * 2 * NG + I) * 256 + e * 16);
-      const float4 v = *reinterpret_cast<const float4 *>(bst + o);
-      float4 hi, lo;
-      split4(v, hi, lo);
-      *reinterpret_cast<float4 *>(bst + o) = hi;
-      *reinterpret_cast<float4 *>(bst + o + NG * 256) = lo;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (o[u] == 0xFFFFFFFFu) continue;
+        float4 hi, lo;
+        split4(v[u], hi, lo);
+        *reinterpret_cast<float4 *>(bst + o[u]) = hi;
+        *reinterpret_cast<float4 *>(bst + o[u] + NG * 256) = lo;
+      }
     }
     fence_async_smem();
     __syncwarp();
