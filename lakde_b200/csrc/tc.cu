@@ -18,23 +18,25 @@
 // (D_hi + D_lo) (W_hi + W_lo) (two MMAs per K step against [W_hi | W_lo]);
 // what remains is the rounding of lo, below 2^-22 relative with random sign.
 //
-// One persistent CTA per SM, 352 threads in four roles, pipelined over
+// One persistent CTA per SM, 384 threads in four roles, pipelined over
 // 128-pair tiles with mbarriers:
 //   * a metadata warp takes kernel rows 32 at a time (an atomic row queue
 //     over the caller's longest-first order, or a static stride), one lane
 //     per row for the dependent loads and the E-step's digamma sums, and
 //     writes each tile's row, pair range, column indices and weights into a
 //     ring of 8 slots, loading the next tile's indices while it writes one;
-//   * a gather warp copies each tile's pair rows (rows of X padded to a
-//     multiple of 16 bytes) into one of two raw stages with cp.async, its
-//     kernel centre and, for the first tile of a row, the row's W cores into
-//     one of two B stages by bulk copy, after the stage's last MMAs committed;
+//   * two gather warps copy each tile's pair rows (rows of X padded to a
+//     multiple of 16 bytes) into one of two raw stages with cp.async, the
+//     first also its kernel centre and, for the first tile of a row, the row's
+//     W cores into one of two B stages by bulk copy, after the stage's last
+//     MMAs committed;
 //   * 8 consumer warps convert tile t (centre, M-step: scale by sqrt r, split
 //     into the hi / lo core-matrix tile, for the first tile of a row split the
 //     W cores in place) and read the previous tile's accumulator (one TMEM
 //     lane per pair) to write log rho / S_n / the running log-sum-exp;
-//   * an MMA warp issues each converted tile's MMAs into one of two TMEM
-//     accumulators and commits them to mbarriers.
+//   * an MMA warp splits each row's W cores in place (while the previous
+//     tile's MMAs run), issues each converted tile's MMAs into one of two
+//     TMEM accumulators and commits them to mbarriers.
 // Every wait is bounded: on a time-out the kernel sets *err, waits (bounded)
 // for its own copies and MMAs in flight, frees its TMEM and returns.
 //
@@ -551,15 +553,16 @@ struct Kern {
 
   // The pair (query) rows of the tile in slot ms into raw stage s, and its
   // kernel centre into the slot's centre buffer, completing on mbarrier
-  // rfull (33 arrivals: lane 0's byte count for the bulk copy, then one per
-  // lane when its cp.async copies have landed).  Half-warp h copies the row
-  // groups 4 (2 j + h) .. + 3, lane k % 16 the 16-byte chunk k of each row:
-  // two 256-byte rows per instruction, the group's four column indices read
-  // as one 16-byte word, four groups in flight.
+  // rfull (65 arrivals: the byte count for the bulk copy, then one per lane
+  // of both gather warps when its cp.async copies have landed).  Half-warp h
+  // of gather warp gw copies the row groups 4 (4 j + 2 gw + h) .. + 3, lane
+  // k % 16 the 16-byte chunk k of each row: two 256-byte rows per
+  // instruction, the group's four column indices read as one 16-byte word,
+  // four groups in flight.
   static __device__ __forceinline__ void gather(const Args &g, unsigned char *sm, const Meta &meta, int s, int ms,
-                                                uint64_t *rfull, bool stall, int lane) {
+                                                uint64_t *rfull, bool stall, int gw, int lane) {
     const uint32_t rb = (uint32_t)(((g.D + 3) / 4) * 16);  // bytes per row
-    if (lane == 0) {
+    if (gw == 0 && lane == 0) {
       mbar_arrive_tx(rfull, rb + (stall ? 16u : 0u));  // a stalled stage expects 16 bytes no copy delivers
       const float *xsrc = g.X + (meta.n + (MODE == PRED ? 0 : g.koff)) * g.ldx;
       bulk_g2s(smem_u32(sm + Smem::XN + ms * 256), xsrc, rb, rfull);
@@ -572,8 +575,8 @@ struct Kern {
     const int64_t ld = (MODE == PRED) ? g.ldy : g.ldx;
     const int cnt = meta.cnt;
 #pragma unroll 4
-    for (int j = 0; j < MT / 8; ++j) {
-      const int grp = 2 * j + h;
+    for (int j = 0; j < MT / 16; ++j) {
+      const int grp = 4 * j + 2 * gw + h;
       if (4 * grp >= cnt) break;
       const int4 c4 = cid4[grp];
       const int cs[4] = {c4.x, c4.y, c4.z, c4.w};
@@ -879,10 +882,11 @@ struct Kern {
 };
 
 // Warps 0-7 convert and run the epilogue; warp 8 writes the tile metadata up
-// to NS - 2 tiles ahead; warp 9 gathers the pair rows, kernel centres and W
-// cores one tile ahead; warp 10 issues the MMAs of each converted tile.
+// to NS - 2 tiles ahead; warps 9 and 10 gather the pair rows (half of each
+// tile's rows each; warp 9 also the kernel centres and W cores) one tile
+// ahead; warp 11 issues the MMAs of each converted tile.
 // Named barriers 1 and 2 count the NTHR consumer threads exactly.
-constexpr int WARP_META = NTHR / 32, WARP_GATHER = WARP_META + 1, WARP_MMA = WARP_META + 2;
+constexpr int WARP_META = NTHR / 32, WARP_GATHER = WARP_META + 1, WARP_MMA = WARP_META + 3;
 constexpr int NWARPS = WARP_MMA + 1;
 constexpr int NTHR_ALL = NWARPS * 32;
 
@@ -919,7 +923,7 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
       mbar_init(mempty + i, 1);
     }
     for (int i = 0; i < 2; ++i) {
-      mbar_init(rfull + i, 33);
+      mbar_init(rfull + i, 65);
       mbar_init(rempty + i, 1);
       mbar_init(bfull + i, 1);
       mbar_init(bempty + i, 1);
@@ -1019,8 +1023,9 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
         cw[k] = nw[k];
       }
     }
-  } else if (warp == WARP_GATHER) {
-    // ------------------------------------------------------ gather warp
+  } else if (warp == WARP_GATHER || warp == WARP_GATHER + 1) {
+    // ----------------------------------------------------- gather warps
+    const int gw = warp - WARP_GATHER;
     int issued = 0;        // tiles whose copies this warp issued
     int wlast0 = -1, wlast1 = -1;  // parity of the last W copy into B stage 0 / 1
     bool first_tile = true;
@@ -1036,7 +1041,7 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
         if (lane == 0) atomicExch(g.err, 1);
         break;
       }
-      if (MODE != MSTEP && (meta.flags & 1)) {
+      if (gw == 0 && MODE != MSTEP && (meta.flags & 1)) {
         if ((meta.flags & 8) && !mbar_wait(bempty + meta.bs, (uint32_t)(meta.bph ^ 1))) {
           if (lane == 0) atomicExch(g.err, 1);
           break;
@@ -1045,7 +1050,7 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
         if (meta.bs) wlast1 = meta.bph;
         else wlast0 = meta.bph;
       }
-      K::gather(g, sm, meta, s, ms, rfull + s, g.stall && first_tile, lane);
+      K::gather(g, sm, meta, s, ms, rfull + s, g.stall && first_tile, gw, lane);
       first_tile = false;
       issued = i + 1;
     }
