@@ -231,12 +231,15 @@ LAKDE_API int lakde_vi_rows(int dtype, int64_t N, int64_t D, int64_t npts,
 
 /*
  * "W cores": X_n = L_n^-1 = W_triu_n^T (lower) as the K-major 8 x 4 core
- * matrices of the tensor-core B operand, float32.  With NT = 8-row blocks
- * (those of lakde_tile_count for D > 8, one block for D <= 8), per kernel,
- * for column block J = 0..NT-1 the row blocks I = J..NT-1, each as two cores
- * (columns 8J..8J+3, then 8J+4..8J+7) of 32 floats: element X[i][j] at
- * 32 ((j % 8) / 4) + 4 (i % 8) + j % 4.  Zero outside D and above the
- * diagonal.  lakde_w_cores_floats(D) floats per kernel.
+ * matrices of the tensor-core B operand, split into tf32 parts: x = hi + lo
+ * with hi = x rounded to the nearest tf32 (ties away from zero) and lo = the
+ * same rounding of x - hi.  With NT = 8-row blocks (those of
+ * lakde_tile_count for D > 8, one block for D <= 8), per kernel, for column
+ * block J = 0..NT-1 the hi parts of row blocks I = J..NT-1, then their lo
+ * parts, each block as two cores (columns 8J..8J+3, then 8J+4..8J+7) of 32
+ * floats: element X[i][j] at 32 ((j % 8) / 4) + 4 (i % 8) + j % 4 of its
+ * block.  Zero outside D and above the diagonal.  lakde_w_cores_floats(D)
+ * floats per kernel.
  */
 LAKDE_API size_t lakde_w_cores_floats(int64_t D);
 

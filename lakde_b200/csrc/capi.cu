@@ -88,6 +88,6 @@ extern "C" int lakde_tuning_get(int knob, int64_t D) { return lakde::tuning(knob
 
 extern "C" const char *lakde_last_error(void) { return lakde::g_last_error; }
 
-extern "C" int lakde_abi_version(void) { return 5; }
+extern "C" int lakde_abi_version(void) { return 6; }
 
 extern "C" int lakde_max_dim(void) { return lakde::kMaxDim; }

@@ -159,6 +159,15 @@ __device__ __forceinline__ void load_tri(T *__restrict__ sU, const T *__restrict
 // Digamma psi(x) for x > 0 in double precision: upward recurrence to x >= 6,
 // then the Stirling asymptotic series
 //   psi(x) ~ ln x - 1/(2x) - sum_k B_2k / (2k x^2k),  B_2k = 1/6, -1/30, 1/42, -1/30, 5/66.
+// Round to the nearest tf32, ties away from zero (10 explicit mantissa bits;
+// the low 13 bits zero): add half of the dropped range to the magnitude bits
+// and clear them.  Two integer ALU operations; finite inputs far below
+// FLT_MAX (centred differences and inverse factors) cannot carry into the
+// exponent's all-ones pattern.
+__device__ __forceinline__ float tf32_rna(float x) {
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+
 __device__ __forceinline__ double digamma_d(double x) {
   if (!(x > 0.0)) return nan("");
   double acc = 0.0;

@@ -464,7 +464,7 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
   const T nanv = T(NAN);
   T *W = g.W ? g.W + n * (int64_t)D * D : nullptr;
   float *Xt = g.Xt ? g.Xt + n * (int64_t)(C::NTILE * 64) : nullptr;
-  float *Wc = g.Wc ? g.Wc + n * (int64_t)(C::NTILE * 64) : nullptr;
+  float *Wc = g.Wc ? g.Wc + n * (int64_t)(C::NTILE * 128) : nullptr;
   if (!ok) {
     for (int e = lane; e < D * D; e += 32) {
       if (W) W[e] = nanv;
@@ -473,7 +473,7 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
     if (Xt)
       for (int e = lane; e < C::NTILE * 64; e += 32) Xt[e] = NAN;
     if (Wc)
-      for (int e = lane; e < C::NTILE * 64; e += 32) Wc[e] = NAN;
+      for (int e = lane; e < C::NTILE * 128; e += 32) Wc[e] = NAN;
     if (lane == 0) {
       g.logdet[n] = nanv;
       if (g.Tm || g.Tt) g.trace[n] = nanv;
@@ -508,14 +508,15 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
       }
   }
   if (Wc) {
-    // segment J holds the tiles I = J .. NT - 1 of column block J, each as two
-    // K-major cores (columns 8 J .. 8 J + 3, then 8 J + 4 .. 8 J + 7); lane l
-    // writes row l / 4, column l % 4 of a core, so a warp store is one
+    // segment J holds the tf32 hi parts of the tiles I = J .. NT - 1 of
+    // column block J, then their lo parts (tf32 of the rest), each tile as
+    // two K-major cores (columns 8 J .. 8 J + 3, then 8 J + 4 .. 8 J + 7);
+    // lane l writes row l / 4, column l % 4 of a core, so a warp store is one
     // contiguous 128-byte core.  Rows i >= D (the identity padding) are zero.
     const int rr = lane >> 2, cc = lane & 3;
 #pragma unroll
     for (int J = 0; J < NT; ++J) {
-      float *seg = Wc + 64 * (J * NT - J * (J - 1) / 2);
+      float *seg = Wc + 128 * (J * NT - J * (J - 1) / 2);
 #pragma unroll
       for (int I = J; I < NT; ++I) {
         const int i = 8 * I + rr;
@@ -523,7 +524,10 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
         for (int h = 0; h < 2; ++h) {
           const int j = 8 * J + 4 * h + cc;
           const double v = M[dmma::tix(I, J) + rr * 8 + 4 * h + cc];
-          seg[(I - J) * 64 + h * 32 + lane] = (i < D && j <= i) ? (float)v : 0.f;
+          const float x = (i < D && j <= i) ? (float)v : 0.f;
+          const float hi = tf32_rna(x);
+          seg[(I - J) * 64 + h * 32 + lane] = hi;
+          seg[(NT - J) * 64 + (I - J) * 64 + h * 32 + lane] = tf32_rna(x - hi);
         }
       }
     }

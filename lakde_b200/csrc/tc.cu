@@ -31,12 +31,11 @@
 //     W cores into one of two B stages by bulk copy, after the stage's last
 //     MMAs committed;
 //   * 8 consumer warps convert tile t (centre, M-step: scale by sqrt r, split
-//     into the hi / lo core-matrix tile, for the first tile of a row split the
-//     W cores in place) and read the previous tile's accumulator (one TMEM
-//     lane per pair) to write log rho / S_n / the running log-sum-exp;
-//   * an MMA warp splits each row's W cores in place (while the previous
-//     tile's MMAs run), issues each converted tile's MMAs into one of two
-//     TMEM accumulators and commits them to mbarriers.
+//     into the hi / lo core-matrix tile) and read the previous tile's
+//     accumulator (one TMEM lane per pair) to write log rho / S_n / the
+//     running log-sum-exp;
+//   * an MMA warp issues each converted tile's MMAs into one of two TMEM
+//     accumulators and commits them to mbarriers.
 // Every wait is bounded: on a time-out the kernel sets *err, waits (bounded)
 // for its own copies and MMAs in flight, frees its TMEM and returns.
 //
@@ -205,22 +204,14 @@ __device__ __forceinline__ void tmem_ld16x2(uint32_t ta, uint32_t tb, float (&v)
   }
 }
 
-// Round to the nearest tf32, ties away from zero (10 explicit mantissa bits;
-// the low 13 bits zero): add half of the dropped range to the magnitude bits
-// and clear them.  Two integer ALU operations; finite inputs far below
-// FLT_MAX (centred differences and inverse factors) cannot carry into the
-// exponent's all-ones pattern.
-__device__ __forceinline__ float tf32_rna(float x) {
-  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
-}
-
 __device__ __forceinline__ void split4(const float4 x, float4 &hi, float4 &lo) {
   hi = make_float4(tf32_rna(x.x), tf32_rna(x.y), tf32_rna(x.z), tf32_rna(x.w));
   lo = make_float4(tf32_rna(x.x - hi.x), tf32_rna(x.y - hi.y), tf32_rna(x.z - hi.z), tf32_rna(x.w - hi.w));
 }
 
-// Float offset of segment J of a W-core block (segments J' < J hold NT - J' tiles of 64 floats).
-__host__ __device__ constexpr int wseg(int J, int NT) { return 64 * (J * NT - J * (J - 1) / 2); }
+// Float offset of segment J of a W-core block (segments J' < J hold NT - J'
+// hi tiles then as many lo tiles, 64 floats each).
+__host__ __device__ constexpr int wseg(int J, int NT) { return 128 * (J * NT - J * (J - 1) / 2); }
 
 struct Args {
   const int64_t *rowptr;
@@ -541,13 +532,17 @@ struct Kern {
   // The W cores of the row starting at the tile in slot ms into its B stage
   // (the E-step and the predictive density), on mbarrier bfull.
   static __device__ void copy_w(const Args &g, unsigned char *sm, const Meta &meta, uint64_t *bfull, int lane) {
-    const float *wsrc = g.Wc + meta.n * (int64_t)(g.ntile * 64);
+    const float *wsrc = g.Wc + meta.n * (int64_t)(g.ntile * 128);
     unsigned char *bst = sm + Smem::BST + (uint32_t)meta.bs * 2 * Smem::B_BYTES;
-    if (lane == 0) mbar_arrive_tx(bfull, (uint32_t)g.ntile * 256u);
+    if (lane == 0) mbar_arrive_tx(bfull, (uint32_t)g.ntile * 512u);
     __syncwarp();
+    // per segment J: its hi tiles and its lo tiles, each run to its half of
+    // the K step's row groups
     for (int J = lane; J < g.nt; J += 32) {
-      const uint32_t seg_bytes = (uint32_t)(g.nt - J) * 256u;
-      bulk_g2s(smem_u32(bst + (J * 2 * NG + J) * 256), wsrc + wseg(J, g.nt), seg_bytes, bfull);
+      const uint32_t run = (uint32_t)(g.nt - J) * 256u;
+      const float *src = wsrc + wseg(J, g.nt);
+      bulk_g2s(smem_u32(bst + (J * 2 * NG + J) * 256), src, run, bfull);
+      bulk_g2s(smem_u32(bst + (J * 2 * NG + NG + J) * 256), src + (g.nt - J) * 64, run, bfull);
     }
   }
 
@@ -692,46 +687,6 @@ struct Kern {
         *reinterpret_cast<float4 *>(dst + 2048 + k * 128) = lo;
       }
     }
-  }
-
-  // The W cores of the row starting at the tile of meta, split in place by
-  // the MMA warp (lane of 32): hi where they landed, lo NG groups further
-  // (the copied cores only), then made visible to the MMAs.
-  static __device__ void split_w(const Args &g, unsigned char *sm, const Meta &meta, int lane) {
-    unsigned char *bst = sm + Smem::BST + (uint32_t)meta.bs * 2 * Smem::B_BYTES;
-    const int nt = g.nt, e = lane & 15;
-    // half-warp h takes every other tile of the segment order (segment J,
-    // row block I >= J), lane e its 16-byte chunk e; four tiles' loads in
-    // flight before their stores
-    int J = 0, I = 0;
-    auto adv = [&]() {
-      if (++I >= nt) I = ++J;
-    };
-    if (lane >> 4) adv();
-    while (J < nt) {
-      uint32_t o[4];
-      float4 v[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        o[u] = 0xFFFFFFFFu;
-        if (J < nt) {
-          o[u] = (uint32_t)((J * 2 * NG + I) * 256 + e * 16);
-          v[u] = *reinterpret_cast<const float4 *>(bst + o[u]);
-          adv();
-          adv();
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        if (o[u] == 0xFFFFFFFFu) continue;
-        float4 hi, lo;
-        split4(v[u], hi, lo);
-        *reinterpret_cast<float4 *>(bst + o[u]) = hi;
-        *reinterpret_cast<float4 *>(bst + o[u] + NG * 256) = lo;
-      }
-    }
-    fence_async_smem();
-    __syncwarp();
   }
 
   // ---------------------------------------------------------------- MMAs
@@ -942,8 +897,7 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
     // ----------------------------------------------------------- MMA warp
     int row_acc = 0;   // M-step: accumulator of the current row
     int last = -1;     // last tile whose MMAs were issued
-    int split = -1;    // last tile whose row's W cores this warp has split
-    bool fail = false;
+
     for (int t = 0;; ++t) {
       const int ms = t % NS, s = t & 1;
       if (!mbar_wait(mfull + ms, (uint32_t)((t / NS) & 1))) {
@@ -952,13 +906,9 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
       }
       const Meta &meta = metas[ms];
       if (meta.n < 0) break;
-      if (MODE != MSTEP && (meta.flags & 1) && split != t) {
-        if (!mbar_wait(bfull + meta.bs, (uint32_t)meta.bph)) {
-          if (lane == 0) atomicExch(g.err, 1);
-          break;
-        }
-        K::split_w(g, sm, meta, lane);
-        split = t;
+      if (MODE != MSTEP && (meta.flags & 1) && !mbar_wait(bfull + meta.bs, (uint32_t)meta.bph)) {
+        if (lane == 0) atomicExch(g.err, 1);
+        break;
       }
       if (!mbar_wait(conv, (uint32_t)(t & 1))) {
         if (lane == 0) atomicExch(g.err, 1);
@@ -977,21 +927,6 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
       }
       __syncwarp();
       last = t;
-      if (MODE != MSTEP) {
-        // while these MMAs run: the W cores of the next tile's row, if it starts one
-        const int t1 = t + 1, ms1 = t1 % NS;
-        if (!mbar_wait(mfull + ms1, (uint32_t)((t1 / NS) & 1))) fail = true;
-        const Meta &m1 = metas[ms1];
-        if (!fail && m1.n >= 0 && (m1.flags & 1)) {
-          if (!mbar_wait(bfull + m1.bs, (uint32_t)m1.bph)) fail = true;
-          else K::split_w(g, sm, m1, lane);
-          split = t1;
-        }
-        if (fail) {
-          if (lane == 0) atomicExch(g.err, 1);
-          break;
-        }
-      }
     }
     // none of this warp's MMAs stays in flight (bounded wait)
     if (last >= 0) mbar_wait(mma_done, (uint32_t)(last & 1));
@@ -1127,7 +1062,9 @@ __global__ void pred_fold_kernel(const float *__restrict__ ws_m, const float *__
 }
 
 // W_triu (dense, upper) -> W cores: element X[i][j] = W_triu[j][i] (i >= j) of
-// segment J = j / 8, row block I = i / 8, core (j % 8) / 4, row i % 8, column j % 4.
+// segment J = j / 8, row block I = i / 8, core (j % 8) / 4, row i % 8, column
+// j % 4, its tf32 hi part in the segment's hi run and lo = tf32(x - hi) in the
+// lo run.
 __global__ void pack_w_cores_kernel(const float *__restrict__ W, float *__restrict__ out, int64_t N, int D, int nt) {
   const int ntile = nt * (nt + 1) / 2;
   const int64_t total = N * ntile * 64;
@@ -1144,8 +1081,11 @@ __global__ void pack_w_cores_kernel(const float *__restrict__ W, float *__restri
     const int I = J + rem;
     const int half = e >> 5, rr = (e >> 2) & 7, cc = e & 3;
     const int i = 8 * I + rr, j = 8 * J + 4 * half + cc;
-    out[n * (int64_t)ntile * 64 + k % ((int64_t)ntile * 64)] =
-        (i < D && j < D && j <= i) ? W[n * (int64_t)D * D + (int64_t)j * D + i] : 0.f;
+    const float x = (i < D && j < D && j <= i) ? W[n * (int64_t)D * D + (int64_t)j * D + i] : 0.f;
+    const float hi = tf32_rna(x);
+    float *seg = out + n * (int64_t)ntile * 128 + wseg(J, nt);
+    seg[(I - J) * 64 + e] = hi;
+    seg[(nt - J) * 64 + (I - J) * 64 + e] = tf32_rna(x - hi);
   }
 }
 
@@ -1280,7 +1220,7 @@ extern "C" int lakde_tc_wait_timeout_probe(int64_t N, int64_t D, int64_t npts, c
 
 extern "C" size_t lakde_w_cores_floats(int64_t D) {
   if (D < 1 || D > 64) return 0;
-  return (size_t)tile_total(D) * 64;
+  return (size_t)tile_total(D) * 128;
 }
 
 extern "C" int lakde_pack_w_cores(int dtype, int64_t N, int64_t D, const void *W_triu, void *W_cores, void *stream) {

@@ -36,7 +36,7 @@ def test_header_and_library_agree(nat):
 
 def test_metadata(nat):
     lib = nat.lib()
-    assert lib.lakde_abi_version() == 5
+    assert lib.lakde_abi_version() == 6
     assert lib.lakde_max_dim() == 64
 
 
@@ -63,9 +63,9 @@ def test_invalid_arguments_are_rejected_on_the_host(nat):
     assert st == 1
     assert lib.lakde_estep_tc(1, 10, 8, 10, p, p, None, p, 8, 0, p, p, p, p, None, p, None) == 2
     assert lib.lakde_estep_tc(0, 10, 65, 10, p, p, None, p, 68, 0, p, p, p, p, None, p, None) == 4
-    assert lib.lakde_w_cores_floats(63) == 36 * 64
-    assert lib.lakde_w_cores_floats(21) == 6 * 64
-    assert lib.lakde_w_cores_floats(3) == 64
+    assert lib.lakde_w_cores_floats(63) == 36 * 128
+    assert lib.lakde_w_cores_floats(21) == 6 * 128
+    assert lib.lakde_w_cores_floats(3) == 128
     assert lib.lakde_w_cores_floats(65) == 0
 
 

@@ -504,19 +504,28 @@ def test_log_pred_density_tc_matches_fp64(K, D, Nq):
 
 
 # ------------------------------------------------------------ tiled layout
+def tf32_rna(x):
+    """Round float32 to the nearest tf32 (ties away from zero) by bit arithmetic."""
+    return ((x.view(torch.int32) + 0x1000) & ~0x1FFF).view(torch.float32)
+
+
 def w_cores_ref(W, D):
     """The W-cores layout of W_triu [N, D, D] (float32, on the device) built with
-    torch: X = W_triu^T, per column block J the row blocks I >= J, each as the
-    two K-major 8 x 4 cores of its columns 8J..8J+3 and 8J+4..8J+7."""
+    torch: X = W_triu^T, per column block J the tf32 hi parts of row blocks
+    I >= J, then their lo parts (tf32 of X - hi), each block as the two
+    K-major 8 x 4 cores of its columns 8J..8J+3 and 8J+4..8J+7."""
     N = W.shape[0]
     nt = 1 if D <= 8 else {16: 2, 24: 3, 32: 4, 48: 6, 64: 8}[next(p for p in (16, 24, 32, 48, 64) if D <= p)]
     Xp = torch.zeros(N, 8 * nt, 8 * nt, device=W.device)
     Xp[:, :D, :D] = torch.tril(W.mT)
+    hi = tf32_rna(Xp)
+    lo = tf32_rna(Xp - hi)
     segs = []
     for J in range(nt):
-        for I in range(J, nt):
-            for h in range(2):
-                segs.append(Xp[:, 8 * I:8 * I + 8, 8 * J + 4 * h:8 * J + 4 * h + 4].reshape(N, 32))
+        for part in (hi, lo):
+            for I in range(J, nt):
+                for h in range(2):
+                    segs.append(part[:, 8 * I:8 * I + 8, 8 * J + 4 * h:8 * J + 4 * h + 4].reshape(N, 32))
     return torch.cat(segs, dim=1).contiguous()
 
 
