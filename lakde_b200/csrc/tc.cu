@@ -245,12 +245,19 @@ struct Args {
   int stall;             // test hook: the first stage expects 16 bytes no copy delivers
 };
 
-// Shared memory of one CTA.  The B stages of the E-step / predictive density
-// double as the accumulator copy of the M-step's epilogue.
-struct Smem {
-  static constexpr uint32_t TILE = 0;                                   // 64 KB (M-step: 16 x GT_SBO)
-  static constexpr uint32_t RAW = TILE + 16 * GT_SBO;                   // 2 x 34 KB
-  static constexpr uint32_t BST = RAW + 2 * MT * RAW_STRIDE;            // 2 x (hi 16 KB + lo 16 KB)
+// Shared memory of one CTA.  The E-step and the predictive density keep two
+// A tiles that take the gathered pair rows in place (the MMAs of one tile
+// run while the other is converted); the M-step transposes, so its rows
+// land in two raw stages and it converts into one tile.  The B stages of
+// the E-step / predictive density are the accumulator copy of the M-step's
+// epilogue.
+template <int MODE>
+struct SmemL {
+  static constexpr bool DUAL = MODE != MSTEP;
+  static constexpr uint32_t TILE_BYTES = DUAL ? 65536u : 16u * GT_SBO;   // M-step: 16 x GT_SBO
+  static constexpr uint32_t TILE = 0;                                   // 2 (M-step: 1) A tiles
+  static constexpr uint32_t RAW = TILE + (DUAL ? 2 : 1) * TILE_BYTES;   // M-step: 2 x 34 KB
+  static constexpr uint32_t BST = RAW + (DUAL ? 0 : 2 * MT * RAW_STRIDE);  // 2 x (hi 16 KB + lo 16 KB)
   static constexpr uint32_t B_BYTES = 16384;
   static constexpr uint32_t RSTR = 68;                                  // M-step accumulator copy row stride
   static constexpr uint32_t RED = BST;
@@ -262,20 +269,21 @@ struct Smem {
   static constexpr uint32_t BAR = PM + 2 * PQ * 4;                      // mbarriers
   static constexpr uint32_t bytes = BAR + 256;
 };
-static_assert(Smem::RSTR * 128 * 4 <= 4 * Smem::B_BYTES, "accumulator copy fits the B stages");
-static_assert(Smem::bytes + 1024 <= 232448, "shared memory of one CTA");
+static_assert(SmemL<MSTEP>::RSTR * 128 * 4 <= 4 * SmemL<MSTEP>::B_BYTES, "accumulator copy fits the B stages");
+static_assert(SmemL<MSTEP>::bytes + 1024 <= 232448 && SmemL<ESTEP>::bytes + 1024 <= 232448,
+              "shared memory of one CTA");
 
-// mbarriers (8 bytes each from Smem::BAR)
+// mbarriers (8 bytes each from SmemL::BAR)
 struct Bars {
   static constexpr int MFULL = 0;          // [NS] metadata of a slot written (32 producer lanes)
   static constexpr int MEMPTY = NS;        // [NS] slot free again (consumer thread 0)
-  static constexpr int RFULL = 2 * NS;     // [2] pair rows and kernel centre landed (32 gatherer lanes + 1)
-  static constexpr int REMPTY = RFULL + 2; // [2] raw stage converted (consumer thread 0)
+  static constexpr int RFULL = 2 * NS;     // [2] pair rows and kernel centre landed (64 gatherer lanes + 1)
+  static constexpr int REMPTY = RFULL + 2; // [2] rows' buffer free: M-step raw stage converted, else A tile's MMAs done
   static constexpr int BFULL = REMPTY + 2; // [2] W cores of a B stage landed
   static constexpr int BEMPTY = BFULL + 2; // [2] MMAs of the stage's last row done (tcgen05.commit)
-  static constexpr int MMA = BEMPTY + 2;   // MMAs of a tile done (tcgen05.commit)
-  static constexpr int CONV = MMA + 1;     // tile converted (every consumer thread)
-  static constexpr int COUNT = CONV + 1;
+  static constexpr int MMA = BEMPTY + 2;   // [2] MMAs of tile t done (t % 2; tcgen05.commit)
+  static constexpr int CONV = MMA + 2;     // [2] tile t converted (t % 2; every consumer thread)
+  static constexpr int COUNT = CONV + 2;
 };
 static_assert(Bars::COUNT * 8 <= 256, "mbarrier area");
 
@@ -306,6 +314,7 @@ __device__ __forceinline__ void bar_sync(int id, int n) { asm volatile("bar.sync
 
 template <int MODE, int DP>
 struct Kern {
+  using Smem = SmemL<MODE>;
   static constexpr int NCH = DP / 4;     // 4-dim chunks of a row
   static constexpr int HCH = NCH / 2;    // chunks per converter thread
   // M-step accumulator columns: the hi rows 0..63 of G^T, then its lo rows
@@ -562,13 +571,41 @@ struct Kern {
       const float *xsrc = g.X + (meta.n + (MODE == PRED ? 0 : g.koff)) * g.ldx;
       bulk_g2s(smem_u32(sm + Smem::XN + ms * 256), xsrc, rb, rfull);
     }
+    const int64_t ld = (MODE == PRED) ? g.ldy : g.ldx;
+    const int cnt = meta.cnt;
+    if (Smem::DUAL) {
+      // straight into A tile s: chunk k of pair p at its hi slot (core (p / 8,
+      // k), row p % 8); lane (p % 8, k % 4), so a warp instruction fills four
+      // whole cores of one 8-pair group; gather warp gw takes the groups
+      // gw, gw + 2, ...
+      const int32_t *cidx = reinterpret_cast<const int32_t *>(sm + Smem::CIDX) + ms * MT;
+      const uint32_t tb = smem_u32(sm + Smem::TILE + (uint32_t)s * Smem::TILE_BYTES);
+      const int pl = lane & 7, kk = lane >> 3;
+      const int rch = (g.D + 3) / 4;
+      const float *base = (MODE == PRED) ? g.Y : g.X;
+      for (int grp = gw; grp < MT / 8; grp += 2) {
+        if (8 * grp >= cnt) break;
+        const int p = 8 * grp + pl;
+        const int32_t c = (p < cnt) ? cidx[p] : -1;
+        const float *src = base + (int64_t)(c < 0 ? 0 : c) * ld;
+#pragma unroll
+        for (int kq = 0; kq < NCH / 4; ++kq) {
+          const int k = 4 * kq + kk;
+          if (c >= 0 && k < rch)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(tb + (uint32_t)grp * 4096u +
+                                                                              (uint32_t)k * 128u + (uint32_t)pl * 16u),
+                         "l"(src + 4 * k)
+                         : "memory");
+        }
+      }
+      asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(rfull)) : "memory");
+      return;
+    }
     const int4 *cid4 = reinterpret_cast<const int4 *>(sm + Smem::CIDX + ms * MT * 4);
     const int h = lane >> 4, k = lane & 15;
     const bool kin = 16 * k < (int)rb;
     const uint32_t dst0 = smem_u32(sm + Smem::RAW + (uint32_t)s * MT * RAW_STRIDE) + 16u * k;
     const float *base = ((MODE == PRED) ? g.Y : g.X) + 4 * k;
-    const int64_t ld = (MODE == PRED) ? g.ldy : g.ldx;
-    const int cnt = meta.cnt;
 #pragma unroll 4
     for (int j = 0; j < MT / 16; ++j) {
       const int grp = 4 * j + 2 * gw + h;
@@ -653,9 +690,10 @@ struct Kern {
       }
       return;
     }
+    // in place: the gathered row chunk sits in its hi slot of A tile s
     const int p = tid & (MT - 1), h = tid >> 7;
     const int cvalid = (p < meta.cnt) ? cidx[p] : -1;
-    unsigned char *dst = tile + (uint32_t)(p >> 3) * 4096u + (uint32_t)(p & 7) * 16u;
+    unsigned char *dst = tile + (uint32_t)s * Smem::TILE_BYTES + (uint32_t)(p >> 3) * 4096u + (uint32_t)(p & 7) * 16u;
     // four chunks at a time: all their loads before any store (the stores
     // into the tile would otherwise order the next loads behind them)
 #pragma unroll
@@ -667,7 +705,7 @@ struct Kern {
         x[i] = make_float4(0.f, 0.f, 0.f, 0.f);
         c[i] = x[i];
         if (i0 + i < HCH && cvalid >= 0 && k < rch) {
-          x[i] = *reinterpret_cast<const float4 *>(raw + p * RAW_STRIDE + k * 16);
+          x[i] = *reinterpret_cast<const float4 *>(dst + k * 128);
           c[i] = xn[k];
         }
       }
@@ -691,8 +729,8 @@ struct Kern {
 
   // ---------------------------------------------------------------- MMAs
   static __device__ __forceinline__ void issue_mma(const Args &g, unsigned char *sm, const Meta &meta, uint32_t tmem,
-                                                   uint32_t acc_sel, uint64_t *mma_done) {
-    const uint32_t tile = smem_u32(sm + Smem::TILE);
+                                                   uint32_t acc_sel, int s, uint64_t *mma_done) {
+    const uint32_t tile = smem_u32(sm + Smem::TILE + (Smem::DUAL ? (uint32_t)s * Smem::TILE_BYTES : 0u));
     if (MODE == MSTEP) {
       // [G_hi; G_lo]^T [G_hi, G_lo] over the tile's pairs, 8 per MMA: the
       // four blocks hh, hl, lh, ll of (G_hi + G_lo)^T (G_hi + G_lo)
@@ -848,6 +886,7 @@ constexpr int NTHR_ALL = NWARPS * 32;
 template <int MODE, int DP>
 __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
   using K = Kern<MODE, DP>;
+  using Smem = SmemL<MODE>;
   extern __shared__ __align__(1024) unsigned char sm[];
   __shared__ uint32_t s_tmem;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -883,8 +922,10 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
       mbar_init(bfull + i, 1);
       mbar_init(bempty + i, 1);
     }
-    mbar_init(mma_done, 1);
-    mbar_init(conv, NTHR);
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(mma_done + i, 1);
+      mbar_init(conv + i, NTHR);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   fence_async_smem();
@@ -910,7 +951,7 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
         if (lane == 0) atomicExch(g.err, 1);
         break;
       }
-      if (!mbar_wait(conv, (uint32_t)(t & 1))) {
+      if (!mbar_wait(conv + s, (uint32_t)((t / 2) & 1))) {
         if (lane == 0) atomicExch(g.err, 1);
         break;
       }
@@ -921,15 +962,16 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
         acc_sel = (uint32_t)row_acc;
       }
       if (lane == 0) {
-        mbar_arrive(rempty + s);  // every converter has read raw stage s
-        K::issue_mma(g, sm, meta, tmem, acc_sel, mma_done);
+        if (!Smem::DUAL) mbar_arrive(rempty + s);  // every converter has read raw stage s
+        K::issue_mma(g, sm, meta, tmem, acc_sel, s, mma_done + s);
+        if (Smem::DUAL) commit(rempty + s);  // A tile s free once its MMAs are done
         if (MODE != MSTEP && (meta.flags & 2)) commit(bempty + meta.bs);
       }
       __syncwarp();
       last = t;
     }
     // none of this warp's MMAs stays in flight (bounded wait)
-    if (last >= 0) mbar_wait(mma_done, (uint32_t)(last & 1));
+    if (last >= 0) mbar_wait(mma_done + (last & 1), (uint32_t)((last / 2) & 1));
   } else if (warp == WARP_META) {
     // ---------------------------------------------------- metadata warp
     typename K::Prod P{};
@@ -998,7 +1040,7 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
     if (wlast1 >= 0) mbar_wait(bfull + 1, (uint32_t)wlast1);
   } else if (warp < WARP_META) {
     // -------------------------------------------------- consumer warps
-    bool ok = true;
+    bool ok = true, epi_ok = true;
     int t = 0;
     int row_acc = 0;  // M-step: accumulator of the current row
     int prev_acc = 0;
@@ -1008,8 +1050,9 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
       const Meta &meta = metas[ms];
       const bool stop = w && meta.n < 0;
       if (w && !stop) w = mbar_wait(rfull + s, (uint32_t)((t / 2) & 1));
-      if (t > 0) w = mbar_wait(mma_done, (uint32_t)((t - 1) & 1)) && w;
-      ok = bar_and(2, NTHR, w);
+      // M-step: one A tile, rewritten only after the last tile's MMAs
+      if (!Smem::DUAL && t > 0) w = mbar_wait(mma_done + ((t - 1) & 1), (uint32_t)(((t - 1) / 2) & 1)) && w;
+      ok = bar_and(2, NTHR, w && epi_ok);
       if (!ok) break;
       fence_after();
       // tile t - 2's epilogue ran in the last iteration: its slot is free
@@ -1022,17 +1065,23 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
         }
         K::convert(g, sm, s, ms, tid);
         fence_async_smem();  // the tile is read by the MMAs (async proxy)
-        mbar_arrive(conv);
+        mbar_arrive(conv + s);
       }
       if (t > 0) {
-        fence_after();
-        K::epilogue(g, sm, (t - 1) % NS, tmem, (uint32_t)prev_acc, tid);
-        fence_before();
+        // two A tiles: the previous tile's MMAs may still run (waited per warp;
+        // a time-out skips the epilogue and ends the loop at the next barrier)
+        if (Smem::DUAL)
+          epi_ok = __all_sync(0xffffffffu, mbar_wait(mma_done + ((t - 1) & 1), (uint32_t)(((t - 1) / 2) & 1)));
+        if (epi_ok) {
+          fence_after();
+          K::epilogue(g, sm, (t - 1) % NS, tmem, (uint32_t)prev_acc, tid);
+          fence_before();
+        }
       }
       prev_acc = (int)acc_sel;
       if (stop) break;
     }
-    if (!ok && tid == 0) atomicExch(g.err, 1);  // the MMA warp waits for its own MMAs
+    if ((!ok || !epi_ok) && tid == 0) atomicExch(g.err, 1);  // the MMA warp waits for its own MMAs
     if (MODE == PRED) {
       bar_sync(2, NTHR);
       const float *pm = reinterpret_cast<const float *>(sm + Smem::PM);
@@ -1159,7 +1208,7 @@ int sm_count() {
 template <int MODE, int DP>
 int launch_rows(const char *what, tc::Args g, int64_t rows, void *stream) {
   auto kern = tc::tc_kernel<MODE, DP>;
-  const size_t smem = tc::Smem::bytes;
+  const size_t smem = tc::SmemL<MODE>::bytes;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) {
     set_error("%s: %s", what, cudaGetErrorString(e));
@@ -1411,7 +1460,7 @@ extern "C" int lakde_log_pred_density_tc(int dtype, int64_t N, int64_t Nq, int64
   int st = dispatch_tc(D, [&](auto dp) {
     constexpr int DP = decltype(dp)::value;
     auto kern = tc::tc_kernel<tc::PRED, DP>;
-    const size_t smem = tc::Smem::bytes;
+    const size_t smem = tc::SmemL<tc::PRED>::bytes;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) {
       set_error("log_pred_density_tc: %s", cudaGetErrorString(e));
