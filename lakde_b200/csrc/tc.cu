@@ -493,6 +493,13 @@ struct Kern {
     }
     int32_t *cidx = reinterpret_cast<int32_t *>(sm + Smem::CIDX) + ms * MT;
     float *rv = reinterpret_cast<float *>(sm + Smem::RV) + ms * MT;
+    const uint32_t rb = (uint32_t)(((g.D + 3) / 4) * 16);  // bytes per row
+    // this slot is up to NS - 2 tiles ahead of the converters: pull its pair
+    // rows (and a new row's W cores) into L2 now, so the gather finds them there
+    if (MODE != PRED && lane == 0 && (t.flags & 1)) {
+      if (MODE == ESTEP) prefetch_l2(g.Wc + t.n * (int64_t)(g.ntile * 128), (uint32_t)g.ntile * 512u);
+      prefetch_l2(g.X + (t.n + g.koff) * g.ldx, rb);
+    }
     unsigned bad = 0;
     float rs = 0.f;
 #pragma unroll
@@ -505,6 +512,7 @@ struct Kern {
         wk = 0.f;
         bad = 1;
       }
+      if (MODE != PRED && p < t.cnt && ck >= 0) prefetch_l2(g.X + (int64_t)ck * g.ldx, rb);
       cidx[p] = ck;
       if (MODE == MSTEP) {
         rv[p] = sqrtf(wk > 0.f ? wk : 0.f);  // the converters scale by sqrt(r)
