@@ -152,6 +152,13 @@ __device__ __forceinline__ void prefetch_l2(const void *src, uint32_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
 
+// L2 prefetch of the 128-byte lines of one row (an ordinary memory
+// instruction per line: far cheaper to issue than a bulk prefetch).
+__device__ __forceinline__ void prefetch_row_l2(const float *src, uint32_t bytes) {
+  for (uint32_t o = 0; o < bytes; o += 128)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char *>(src) + o));
+}
+
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -512,7 +519,7 @@ struct Kern {
         wk = 0.f;
         bad = 1;
       }
-      if (MODE != PRED && p < t.cnt && ck >= 0) prefetch_l2(g.X + (int64_t)ck * g.ldx, rb);
+      if (MODE != PRED && p < t.cnt && ck >= 0) prefetch_row_l2(g.X + (int64_t)ck * g.ldx, rb);
       cidx[p] = ck;
       if (MODE == MSTEP) {
         rv[p] = sqrtf(wk > 0.f ? wk : 0.f);  // the converters scale by sqrt(r)
@@ -781,10 +788,14 @@ struct Kern {
       // lower triangle
       float *red = reinterpret_cast<float *>(sm + Smem::RED);
       const bool empty = (meta.cnt == 0) && (meta.flags & 1);
-      if (tid < 128) {
-        const uint32_t taddr = tmem + acc_sel * ACC_COLS + ((uint32_t)(warp * 32) << 16);
+      {
+        // warps w and w + 4 read the same 32 TMEM lanes, alternate 16-column blocks
+        const int row = tid & 127, half = tid >> 7;
+        const uint32_t taddr = tmem + acc_sel * ACC_COLS + ((uint32_t)((warp & 3) * 32) << 16);
 #pragma unroll
-        for (int c0 = 0; c0 < DP; c0 += 16) {
+        for (int cb = 0; cb < (DP + 15) / 16; ++cb) {
+          if ((cb & 1) != half) continue;
+          const int c0 = 16 * cb;
           float v[16], u[16];
           if (!empty) {
             tmem_ld16x2(taddr + c0, taddr + 64 + c0, v, u);
@@ -794,7 +805,7 @@ struct Kern {
           }
 #pragma unroll
           for (int k = 0; k < 16; k += 4)
-            *reinterpret_cast<float4 *>(red + tid * Smem::RSTR + c0 + k) =
+            *reinterpret_cast<float4 *>(red + row * Smem::RSTR + c0 + k) =
                 make_float4(v[k] + u[k], v[k + 1] + u[k + 1], v[k + 2] + u[k + 2], v[k + 3] + u[k + 3]);
         }
       }
