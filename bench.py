@@ -216,13 +216,14 @@ def _cpu_rows(job):
     t0 = _time.perf_counter()
     Xn = Xs[self_idx]
     S = O.calc_W_inv(rowptr, col, r, Xn, Xs)
-    nu = nu0 + np.add.reduceat(r, rowptr[:-1]) if len(r) else np.full(len(self_idx), nu0)
+    rows = O._rows_of(rowptr)
+    # per-row sums of r (rows without pairs, last in the longest-first order, sum to 0)
+    nu = nu0 + np.bincount(rows, weights=r, minlength=len(self_idx))
     A = (sigma0 * scale[:, None, None] + S).astype(np.float64)
     L, _ = O.stabilized_cholesky(A, eps=float(np.finfo(np.float32).eps))
     W = np.swapaxes(O.tril_inverse(L), -1, -2)
     logdet = O.chol_logdet(W)
     O.chol_mm_trace(L0.astype(np.float64), W)
-    rows = O._rows_of(rowptr)
     delta = Xs[col] - Xn[rows]
     y = np.einsum("pji,pj->pi", np.triu(W)[rows], delta, optimize=True)
     Q = (y * y).sum(-1)
