@@ -228,22 +228,14 @@ __global__ void __launch_bounds__(128, (sizeof(T) == 4 && DP == 8) ? 3 : 1) vi_r
   load_row<T, DP>(g.X, n + g.koff, D, xn);
 
   // ---------------------------------------------------------------- M-step
-  // pairs in batches of U: the point rows of a batch are all loaded before
-  // any is used (the gathers of a row overlap), and the next batch's indices
-  // are loaded while they are in flight, so a batch waits on one round trip
-  // instead of two; the accumulation order is the pair order
+  // pairs in batches of U: the indices, then the point rows of a batch are
+  // all loaded before any is used (the gathers of a row overlap); the
+  // accumulation order is the pair order
   constexpr int U = 4;
   T S[TT];
 #pragma unroll
   for (int e = 0; e < TT; ++e) S[e] = T(0);
   T vsum = T(0);
-  int32_t cn[U];
-  T vn[U];
-#pragma unroll
-  for (int u = 0; u < U; ++u) {
-    cn[u] = (start + u < end) ? g.col[start + u] : -1;
-    vn[u] = (start + u < end) ? g.r[start + u] : T(0);
-  }
   for (int64_t p0 = start; p0 < end; p0 += U) {
     int64_t c[U];
     T v[U];
@@ -252,19 +244,13 @@ __global__ void __launch_bounds__(128, (sizeof(T) == 4 && DP == 8) ? 3 : 1) vi_r
       c[u] = -1;
       v[u] = T(0);
       if (p0 + u < end) {
-        c[u] = cn[u];
-        v[u] = vn[u];
+        c[u] = g.col[p0 + u];
+        v[u] = g.r[p0 + u];
         if (c[u] < 0 || c[u] >= g.npts) {
           bad = true;
           c[u] = -1;
         }
       }
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int64_t q = p0 + U + u;
-      cn[u] = (q < end) ? g.col[q] : -1;
-      vn[u] = (q < end) ? g.r[q] : T(0);
     }
     T dl[U][DP];
 #pragma unroll
@@ -302,20 +288,16 @@ __global__ void __launch_bounds__(128, (sizeof(T) == 4 && DP == 8) ? 3 : 1) vi_r
   const double e = mvdigamma_d(0.5 * (double)nu, D) + D * 0.69314718055994530942 + (double)logdet;
   const T cst = (T)(0.5 * e);
   const T expo = T(-0.5) * nu;
-#pragma unroll
-  for (int u = 0; u < U; ++u) cn[u] = (start + u < end) ? g.col[start + u] : -1;
   for (int64_t p0 = start; p0 < end; p0 += U) {
     int64_t c[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       c[u] = -1;
       if (p0 + u < end) {
-        c[u] = cn[u];
+        c[u] = g.col[p0 + u];
         if (!ok || c[u] < 0 || c[u] >= g.npts) c[u] = -2;
       }
     }
-#pragma unroll
-    for (int u = 0; u < U; ++u) cn[u] = (p0 + U + u < end) ? g.col[p0 + U + u] : -1;
     T dl[U][DP];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
