@@ -18,14 +18,14 @@
 // (D_hi + D_lo) (W_hi + W_lo) (two MMAs per K step against [W_hi | W_lo]);
 // what remains is the rounding of lo, below 2^-22 relative with random sign.
 //
-// One persistent CTA per SM, 384 threads in four roles, pipelined over
+// One persistent CTA per SM, 448 threads in four roles, pipelined over
 // 128-pair tiles with mbarriers:
 //   * a metadata warp takes kernel rows 32 at a time (an atomic row queue
 //     over the caller's longest-first order, or a static stride), one lane
 //     per row for the dependent loads and the E-step's digamma sums, and
 //     writes each tile's row, pair range, column indices and weights into a
 //     ring of 8 slots, loading the next tile's indices while it writes one;
-//   * two gather warps copy each tile's pair rows (rows of X padded to a
+//   * four gather warps copy each tile's pair rows (rows of X padded to a
 //     multiple of 16 bytes) into one of two raw stages with cp.async, the
 //     first also its kernel centre and, for the first tile of a row, the row's
 //     W cores into one of two B stages by bulk copy, after the stage's last
@@ -64,6 +64,7 @@ namespace tc {
 constexpr int MT = 128;        // pairs (queries) per tile: the MMA M
 constexpr int NTHR = 256;      // 8 consumer warps (two more produce)
 constexpr int NS = 8;          // metadata slots
+constexpr int NGW = 4;         // gather warps
 constexpr int RAW_STRIDE = 272;  // bytes per staged pair row: 64 floats + 16 bytes against bank conflicts
 constexpr uint32_t kSpinLimit = 1u << 26;
 constexpr uint64_t kWaitLimitNs = 1500000000ull;  // 1.5 s: far above any copy or MMA of one tile
@@ -572,8 +573,8 @@ struct Kern {
 
   // The pair (query) rows of the tile in slot ms into raw stage s, and its
   // kernel centre into the slot's centre buffer, completing on mbarrier
-  // rfull (65 arrivals: the byte count for the bulk copy, then one per lane
-  // of both gather warps when its cp.async copies have landed).  Half-warp h
+  // rfull (32 NGW + 1 arrivals: the byte count for the bulk copy, then one
+  // per lane of every gather warp when its cp.async copies have landed).  Half-warp h
   // of gather warp gw copies the row groups 4 (4 j + 2 gw + h) .. + 3, lane
   // k % 16 the 16-byte chunk k of each row: two 256-byte rows per
   // instruction, the group's four column indices read as one 16-byte word,
@@ -592,13 +593,13 @@ struct Kern {
       // straight into A tile s: chunk k of pair p at its hi slot (core (p / 8,
       // k), row p % 8); lane (p % 8, k % 4), so a warp instruction fills four
       // whole cores of one 8-pair group; gather warp gw takes the groups
-      // gw, gw + 2, ...
+      // gw, gw + NGW, ...
       const int32_t *cidx = reinterpret_cast<const int32_t *>(sm + Smem::CIDX) + ms * MT;
       const uint32_t tb = smem_u32(sm + Smem::TILE + (uint32_t)s * Smem::TILE_BYTES);
       const int pl = lane & 7, kk = lane >> 3;
       const int rch = (g.D + 3) / 4;
       const float *base = (MODE == PRED) ? g.Y : g.X;
-      for (int grp = gw; grp < MT / 8; grp += 2) {
+      for (int grp = gw; grp < MT / 8; grp += NGW) {
         if (8 * grp >= cnt) break;
         const int p = 8 * grp + pl;
         const int32_t c = (p < cnt) ? cidx[p] : -1;
@@ -622,8 +623,8 @@ struct Kern {
     const uint32_t dst0 = smem_u32(sm + Smem::RAW + (uint32_t)s * MT * RAW_STRIDE) + 16u * k;
     const float *base = ((MODE == PRED) ? g.Y : g.X) + 4 * k;
 #pragma unroll 4
-    for (int j = 0; j < MT / 16; ++j) {
-      const int grp = 4 * j + 2 * gw + h;
+    for (int j = 0; j < MT / (8 * NGW); ++j) {
+      const int grp = 2 * NGW * j + 2 * gw + h;
       if (4 * grp >= cnt) break;
       const int4 c4 = cid4[grp];
       const int cs[4] = {c4.x, c4.y, c4.z, c4.w};
@@ -894,11 +895,11 @@ struct Kern {
 };
 
 // Warps 0-7 convert and run the epilogue; warp 8 writes the tile metadata up
-// to NS - 2 tiles ahead; warps 9 and 10 gather the pair rows (half of each
-// tile's rows each; warp 9 also the kernel centres and W cores) one tile
-// ahead; warp 11 issues the MMAs of each converted tile.
+// to NS - 2 tiles ahead; warps 9 .. 8 + NGW gather the pair rows (a share of
+// each tile's rows each; the first also the kernel centres and W cores) one
+// tile ahead; the last warp issues the MMAs of each converted tile.
 // Named barriers 1 and 2 count the NTHR consumer threads exactly.
-constexpr int WARP_META = NTHR / 32, WARP_GATHER = WARP_META + 1, WARP_MMA = WARP_META + 3;
+constexpr int WARP_META = NTHR / 32, WARP_GATHER = WARP_META + 1, WARP_MMA = WARP_GATHER + NGW;
 constexpr int NWARPS = WARP_MMA + 1;
 constexpr int NTHR_ALL = NWARPS * 32;
 
@@ -936,7 +937,7 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
       mbar_init(mempty + i, 1);
     }
     for (int i = 0; i < 2; ++i) {
-      mbar_init(rfull + i, 65);
+      mbar_init(rfull + i, 32 * NGW + 1);
       mbar_init(rempty + i, 1);
       mbar_init(bfull + i, 1);
       mbar_init(bempty + i, 1);
@@ -1019,7 +1020,7 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
         cw[k] = nw[k];
       }
     }
-  } else if (warp == WARP_GATHER || warp == WARP_GATHER + 1) {
+  } else if (warp >= WARP_GATHER && warp < WARP_GATHER + NGW) {
     // ----------------------------------------------------- gather warps
     const int gw = warp - WARP_GATHER;
     int issued = 0;        // tiles whose copies this warp issued
