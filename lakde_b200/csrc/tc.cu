@@ -18,14 +18,14 @@
 // (D_hi + D_lo) (W_hi + W_lo) (two MMAs per K step against [W_hi | W_lo]);
 // what remains is the rounding of lo, below 2^-22 relative with random sign.
 //
-// One persistent CTA per SM, 448 threads in four roles, pipelined over
+// One persistent CTA per SM, 384 threads in four roles, pipelined over
 // 128-pair tiles with mbarriers:
 //   * a metadata warp takes kernel rows 32 at a time (an atomic row queue
 //     over the caller's longest-first order, or a static stride), one lane
 //     per row for the dependent loads and the E-step's digamma sums, and
 //     writes each tile's row, pair range, column indices and weights into a
 //     ring of 8 slots, loading the next tile's indices while it writes one;
-//   * four gather warps copy each tile's pair rows (rows of X padded to a
+//   * two gather warps copy each tile's pair rows (rows of X padded to a
 //     multiple of 16 bytes) into one of two raw stages with cp.async, the
 //     first also its kernel centre and, for the first tile of a row, the row's
 //     W cores into one of two B stages by bulk copy, after the stage's last
@@ -64,7 +64,7 @@ namespace tc {
 constexpr int MT = 128;        // pairs (queries) per tile: the MMA M
 constexpr int NTHR = 256;      // 8 consumer warps (two more produce)
 constexpr int NS = 8;          // metadata slots
-constexpr int NGW = 4;         // gather warps
+constexpr int NGW = 2;         // gather warps (four measured no faster: the scattered copies, not their issue, set the rate)
 constexpr int RAW_STRIDE = 272;  // bytes per staged pair row: 64 floats + 16 bytes against bank conflicts
 constexpr uint32_t kSpinLimit = 1u << 26;
 constexpr uint64_t kWaitLimitNs = 1500000000ull;  // 1.5 s: far above any copy or MMA of one tile
