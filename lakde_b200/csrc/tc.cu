@@ -18,7 +18,7 @@
 // (D_hi + D_lo) (W_hi + W_lo) (two MMAs per K step against [W_hi | W_lo]);
 // what remains is the rounding of lo, below 2^-22 relative with random sign.
 //
-// One persistent CTA per SM, 512 threads in five roles, pipelined over
+// One persistent CTA per SM, 640 threads in five roles, pipelined over
 // 128-pair tiles with mbarriers:
 //   * a metadata warp takes kernel rows 32 at a time (an atomic row queue
 //     over the caller's longest-first order, or a static stride), one lane
@@ -35,7 +35,7 @@
 //     split into the hi / lo core-matrix tile);
 //   * an MMA warp issues each converted tile's MMAs into one of two TMEM
 //     accumulators and commits them to mbarriers;
-//   * 4 epilogue warps read each finished tile's accumulator (one TMEM lane
+//   * 8 epilogue warps read each finished tile's accumulator (one TMEM lane
 //     per pair) and write log rho / S_n / the running log-sum-exp, while the
 //     converters work on the next tiles.
 // Every wait is bounded: on a time-out the kernel sets *err, waits (bounded)
@@ -65,7 +65,7 @@ namespace tc {
 
 constexpr int MT = 128;        // pairs (queries) per tile: the MMA M
 constexpr int NTHR = 256;      // 8 converter warps
-constexpr int ETHR = 128;      // 4 epilogue warps
+constexpr int ETHR = 256;      // 8 epilogue warps
 constexpr int NS = 8;          // metadata slots
 constexpr int NGW = 2;         // gather warps (four measured no faster: the scattered copies, not their issue, set the rate)
 constexpr int RAW_STRIDE = 272;  // bytes per staged pair row: 64 floats + 16 bytes against bank conflicts
@@ -780,13 +780,15 @@ struct Kern {
   }
 
   // ---------------------------------------------------------------- epilogue
-  // Run by the 4 epilogue warps (thread et = 0..127; warp et / 32 reads TMEM
-  // lanes 32 (et / 32) .. + 31, the lanes its hardware warp index allows).
+  // Run by the 8 epilogue warps (thread et = 0..255; warp et / 32 reads TMEM
+  // lanes 32 (et / 32 % 4) .. + 31, the lanes its hardware warp index allows;
+  // the M-step splits the 16-column blocks between the two warps of a lane
+  // quarter, the E-step and the predictive density use the first four).
   static __device__ void epilogue(const Args &g, unsigned char *sm, int ms, uint32_t tmem, uint32_t acc_sel,
                                   int et) {
     const Meta &meta = reinterpret_cast<const Meta *>(sm + Smem::META)[ms];
     const int32_t *cidx = reinterpret_cast<const int32_t *>(sm + Smem::CIDX) + ms * MT;
-    const int warp = et >> 5;
+    const int warp = (et >> 5) & 3;
     if (MODE == MSTEP) {
       if (!(meta.flags & 2)) return;
       // accumulator row i < 64 holds (hh_ij, hl_ij) in columns (j, 64 + j),
@@ -796,10 +798,11 @@ struct Kern {
       float *red = reinterpret_cast<float *>(sm + Smem::RED);
       const bool empty = (meta.cnt == 0) && (meta.flags & 1);
       {
-        const int row = et;
+        const int row = et & 127, half = et >> 7;
         const uint32_t taddr = tmem + acc_sel * ACC_COLS + ((uint32_t)(warp * 32) << 16);
 #pragma unroll
         for (int cb = 0; cb < (DP + 15) / 16; ++cb) {
+          if ((cb & 1) != half) continue;
           const int c0 = 16 * cb;
           float v[16], u[16];
           if (!empty) {
@@ -855,6 +858,7 @@ struct Kern {
       asm volatile("bar.sync 1, %0;" ::"n"(ETHR) : "memory");
       return;
     }
+    if (et >= MT) return;
     // lane = pair (query) row
     const uint32_t taddr = tmem + acc_sel * ACC_COLS + ((uint32_t)(warp * 32) << 16);
     float q = 0.f;
@@ -900,7 +904,7 @@ struct Kern {
 // Warps 0-7 convert; warp 8 writes the tile metadata up to NS - 2 tiles
 // ahead; warps 9 .. 8 + NGW gather the pair rows (a share of each tile's rows
 // each; the first also the kernel centres and W cores) one tile ahead; warp
-// 11 issues the MMAs of each converted tile; warps 12-15 (one per TMEM lane
+// 11 issues the MMAs of each converted tile; warps 12-19 (two per TMEM lane
 // quarter) run the epilogue of each finished tile.  Named barrier 2 counts
 // the NTHR converter threads, barriers 1 and 3 the ETHR epilogue threads.
 constexpr int WARP_META = NTHR / 32, WARP_GATHER = WARP_META + 1, WARP_MMA = WARP_GATHER + NGW;
