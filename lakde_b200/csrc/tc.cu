@@ -18,7 +18,7 @@
 // (D_hi + D_lo) (W_hi + W_lo) (two MMAs per K step against [W_hi | W_lo]);
 // what remains is the rounding of lo, below 2^-22 relative with random sign.
 //
-// One persistent CTA per SM, 640 threads in five roles, pipelined over
+// One persistent CTA per SM, 384 threads in four roles, pipelined over
 // 128-pair tiles with mbarriers:
 //   * a metadata warp takes kernel rows 32 at a time (an atomic row queue
 //     over the caller's longest-first order, or a static stride), one lane
@@ -26,18 +26,16 @@
 //     writes each tile's row, pair range, column indices and weights into a
 //     ring of 8 slots, loading the next tile's indices while it writes one;
 //   * two gather warps copy each tile's pair rows (rows of X padded to a
-//     multiple of 16 bytes) with cp.async, the first also its kernel centre
-//     and, for the first tile of a row, the row's pre-split W cores into one
-//     of two B stages by bulk copy, after the stage's last MMAs committed;
-//     E-step / predictive density: into the hi slots of one of two A tiles
-//     (converted in place); M-step: into one of two raw stages;
-//   * 8 converter warps convert tile t (centre, M-step: scale by sqrt r,
-//     split into the hi / lo core-matrix tile);
+//     multiple of 16 bytes) into one of two raw stages with cp.async, the
+//     first also its kernel centre and, for the first tile of a row, the row's
+//     W cores into one of two B stages by bulk copy, after the stage's last
+//     MMAs committed;
+//   * 8 consumer warps convert tile t (centre, M-step: scale by sqrt r, split
+//     into the hi / lo core-matrix tile) and read the previous tile's
+//     accumulator (one TMEM lane per pair) to write log rho / S_n / the
+//     running log-sum-exp;
 //   * an MMA warp issues each converted tile's MMAs into one of two TMEM
-//     accumulators and commits them to mbarriers;
-//   * 8 epilogue warps read each finished tile's accumulator (one TMEM lane
-//     per pair) and write log rho / S_n / the running log-sum-exp, while the
-//     converters work on the next tiles.
+//     accumulators and commits them to mbarriers.
 // Every wait is bounded: on a time-out the kernel sets *err, waits (bounded)
 // for its own copies and MMAs in flight, frees its TMEM and returns.
 //
@@ -64,8 +62,7 @@ namespace lakde {
 namespace tc {
 
 constexpr int MT = 128;        // pairs (queries) per tile: the MMA M
-constexpr int NTHR = 256;      // 8 converter warps
-constexpr int ETHR = 256;      // 8 epilogue warps
+constexpr int NTHR = 256;      // 8 consumer warps (two more produce)
 constexpr int NS = 8;          // metadata slots
 constexpr int NGW = 2;         // gather warps (four measured no faster: the scattered copies, not their issue, set the rate)
 constexpr int RAW_STRIDE = 272;  // bytes per staged pair row: 64 floats + 16 bytes against bank conflicts
@@ -287,15 +284,14 @@ static_assert(SmemL<MSTEP>::bytes + 1024 <= 232448 && SmemL<ESTEP>::bytes + 1024
 // mbarriers (8 bytes each from SmemL::BAR)
 struct Bars {
   static constexpr int MFULL = 0;          // [NS] metadata of a slot written (32 producer lanes)
-  static constexpr int MEMPTY = NS;        // [NS] slot free again (every epilogue thread)
+  static constexpr int MEMPTY = NS;        // [NS] slot free again (consumer thread 0)
   static constexpr int RFULL = 2 * NS;     // [2] pair rows and kernel centre landed (64 gatherer lanes + 1)
   static constexpr int REMPTY = RFULL + 2; // [2] rows' buffer free: M-step raw stage converted, else A tile's MMAs done
   static constexpr int BFULL = REMPTY + 2; // [2] W cores of a B stage landed
   static constexpr int BEMPTY = BFULL + 2; // [2] MMAs of the stage's last row done (tcgen05.commit)
   static constexpr int MMA = BEMPTY + 2;   // [2] MMAs of tile t done (t % 2; tcgen05.commit)
-  static constexpr int CONV = MMA + 2;     // [2] tile t converted (t % 2; every converter thread)
-  static constexpr int EDONE = CONV + 2;   // [2] tile t's epilogue done (t % 2; every epilogue thread)
-  static constexpr int COUNT = EDONE + 2;
+  static constexpr int CONV = MMA + 2;     // [2] tile t converted (t % 2; every consumer thread)
+  static constexpr int COUNT = CONV + 2;
 };
 static_assert(Bars::COUNT * 8 <= 256, "mbarrier area");
 
@@ -780,15 +776,11 @@ struct Kern {
   }
 
   // ---------------------------------------------------------------- epilogue
-  // Run by the 8 epilogue warps (thread et = 0..255; warp et / 32 reads TMEM
-  // lanes 32 (et / 32 % 4) .. + 31, the lanes its hardware warp index allows;
-  // the M-step splits the 16-column blocks between the two warps of a lane
-  // quarter, the E-step and the predictive density use the first four).
   static __device__ void epilogue(const Args &g, unsigned char *sm, int ms, uint32_t tmem, uint32_t acc_sel,
-                                  int et) {
+                                  int tid) {
     const Meta &meta = reinterpret_cast<const Meta *>(sm + Smem::META)[ms];
     const int32_t *cidx = reinterpret_cast<const int32_t *>(sm + Smem::CIDX) + ms * MT;
-    const int warp = (et >> 5) & 3;
+    const int warp = tid >> 5;
     if (MODE == MSTEP) {
       if (!(meta.flags & 2)) return;
       // accumulator row i < 64 holds (hh_ij, hl_ij) in columns (j, 64 + j),
@@ -798,8 +790,9 @@ struct Kern {
       float *red = reinterpret_cast<float *>(sm + Smem::RED);
       const bool empty = (meta.cnt == 0) && (meta.flags & 1);
       {
-        const int row = et & 127, half = et >> 7;
-        const uint32_t taddr = tmem + acc_sel * ACC_COLS + ((uint32_t)(warp * 32) << 16);
+        // warps w and w + 4 read the same 32 TMEM lanes, alternate 16-column blocks
+        const int row = tid & 127, half = tid >> 7;
+        const uint32_t taddr = tmem + acc_sel * ACC_COLS + ((uint32_t)((warp & 3) * 32) << 16);
 #pragma unroll
         for (int cb = 0; cb < (DP + 15) / 16; ++cb) {
           if ((cb & 1) != half) continue;
@@ -818,18 +811,18 @@ struct Kern {
         }
       }
       fence_before();
-      asm volatile("bar.sync 1, %0;" ::"n"(ETHR) : "memory");
+      asm volatile("bar.sync 1, %0;" ::"n"(NTHR) : "memory");
       const int64_t n = meta.n;
       const bool bad = (meta.flags & 4) != 0;
       const int D = g.D;
       const float *Uh = red, *Vl = red + 64 * Smem::RSTR;
-      if (et == 0) g.nu_out[n] = bad ? NAN : g.nu0 + meta.rsum;
+      if (tid == 0) g.nu_out[n] = bad ? NAN : g.nu0 + meta.rsum;
       if (g.SPo) {
         // four consecutive columns of one tile row per store: tile t = I (I +
         // 1) / 2 + J (I from the root of 8 t + 1, exact at these sizes), row
         // r = e / 2, columns 8 J + 4 (e % 2) + 0..3
         float *dst = g.SPo + n * (int64_t)(g.ntile * 128);
-        for (int q = et; q < g.ntile * 16; q += ETHR) {
+        for (int q = tid; q < g.ntile * 16; q += NTHR) {
           const int t = q >> 4, e = q & 15;
           const int I = (int)((sqrtf(8.f * (float)t + 1.f) - 1.f) * 0.5f);
           const int J = t - I * (I + 1) / 2;
@@ -848,17 +841,17 @@ struct Kern {
         }
       } else {
         float *Sn = g.S + n * (int64_t)D * D;
-        for (int q = et; q < D * D; q += ETHR) {
+        for (int q = tid; q < D * D; q += NTHR) {
           const int i = q / D, j = q % D;
           if (g.lower_only && j > i) continue;
           const int a = i > j ? i : j, b = i > j ? j : i;  // symmetric: from the lower triangle
           Sn[q] = bad ? NAN : Vl[a * Smem::RSTR + b] + Uh[a * Smem::RSTR + b];
         }
       }
-      asm volatile("bar.sync 1, %0;" ::"n"(ETHR) : "memory");
+      asm volatile("bar.sync 1, %0;" ::"n"(NTHR) : "memory");
       return;
     }
-    if (et >= MT) return;
+    if (tid >= 128) return;
     // lane = pair (query) row
     const uint32_t taddr = tmem + acc_sel * ACC_COLS + ((uint32_t)(warp * 32) << 16);
     float q = 0.f;
@@ -874,7 +867,7 @@ struct Kern {
         }
       }
     }
-    const int p = et;
+    const int p = tid;
     if (p >= meta.cnt) return;
     if (MODE == ESTEP) {
       const int32_t c = cidx[p];
@@ -901,16 +894,13 @@ struct Kern {
   }
 };
 
-// Warps 0-7 convert; warp 8 writes the tile metadata up to NS - 2 tiles
-// ahead; warps 9 .. 8 + NGW gather the pair rows (a share of each tile's rows
-// each; the first also the kernel centres and W cores) one tile ahead; warp
-// 11 issues the MMAs of each converted tile; warps 12-19 (two per TMEM lane
-// quarter) run the epilogue of each finished tile.  Named barrier 2 counts
-// the NTHR converter threads, barriers 1 and 3 the ETHR epilogue threads.
+// Warps 0-7 convert and run the epilogue; warp 8 writes the tile metadata up
+// to NS - 2 tiles ahead; warps 9 .. 8 + NGW gather the pair rows (a share of
+// each tile's rows each; the first also the kernel centres and W cores) one
+// tile ahead; the last warp issues the MMAs of each converted tile.
+// Named barriers 1 and 2 count the NTHR consumer threads exactly.
 constexpr int WARP_META = NTHR / 32, WARP_GATHER = WARP_META + 1, WARP_MMA = WARP_GATHER + NGW;
-constexpr int WARP_EPI = WARP_MMA + 1;
-constexpr int NWARPS = WARP_EPI + ETHR / 32;
-static_assert(WARP_EPI % 4 == 0, "the epilogue warps cover the four TMEM lane quarters in order");
+constexpr int NWARPS = WARP_MMA + 1;
 constexpr int NTHR_ALL = NWARPS * 32;
 
 template <int MODE, int DP>
@@ -924,7 +914,7 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
   uint64_t *mfull = bars + Bars::MFULL, *mempty = bars + Bars::MEMPTY;
   uint64_t *rfull = bars + Bars::RFULL, *rempty = bars + Bars::REMPTY;
   uint64_t *bfull = bars + Bars::BFULL, *bempty = bars + Bars::BEMPTY;
-  uint64_t *mma_done = bars + Bars::MMA, *conv = bars + Bars::CONV, *edone = bars + Bars::EDONE;
+  uint64_t *mma_done = bars + Bars::MMA, *conv = bars + Bars::CONV;
   const Meta *metas = reinterpret_cast<const Meta *>(sm + Smem::META);
 
   // zero the operand tile (cores past DP stay zero) and the B stages (cores above the block diagonal)
@@ -944,7 +934,7 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
   if (tid == 0) {
     for (int i = 0; i < NS; ++i) {
       mbar_init(mfull + i, 32);
-      mbar_init(mempty + i, ETHR);
+      mbar_init(mempty + i, 1);
     }
     for (int i = 0; i < 2; ++i) {
       mbar_init(rfull + i, 32 * NGW + 1);
@@ -955,7 +945,6 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
     for (int i = 0; i < 2; ++i) {
       mbar_init(mma_done + i, 1);
       mbar_init(conv + i, NTHR);
-      mbar_init(edone + i, ETHR);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -983,12 +972,6 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
         break;
       }
       if (!mbar_wait(conv + s, (uint32_t)((t / 2) & 1))) {
-        if (lane == 0) atomicExch(g.err, 1);
-        break;
-      }
-      // the accumulator this tile writes was last read by tile t - 2's
-      // epilogue at the latest (epilogues run in tile order)
-      if (t >= 2 && !mbar_wait(edone + s, (uint32_t)(((t - 2) / 2) & 1))) {
         if (lane == 0) atomicExch(g.err, 1);
         break;
       }
@@ -1076,9 +1059,12 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
     if (wlast0 >= 0) mbar_wait(bfull, (uint32_t)wlast0);
     if (wlast1 >= 0) mbar_wait(bfull + 1, (uint32_t)wlast1);
   } else if (warp < WARP_META) {
-    // ------------------------------------------------- converter warps
-    bool ok = true;
-    for (int t = 0;; ++t) {
+    // -------------------------------------------------- consumer warps
+    bool ok = true, epi_ok = true;
+    int t = 0;
+    int row_acc = 0;  // M-step: accumulator of the current row
+    int prev_acc = 0;
+    for (;; ++t) {
       const int ms = t % NS, s = t & 1;
       bool w = mbar_wait(mfull + ms, (uint32_t)((t / NS) & 1));
       const Meta &meta = metas[ms];
@@ -1086,48 +1072,40 @@ __global__ void __launch_bounds__(NTHR_ALL, 1) tc_kernel(Args g) {
       if (w && !stop) w = mbar_wait(rfull + s, (uint32_t)((t / 2) & 1));
       // M-step: one A tile, rewritten only after the last tile's MMAs
       if (!Smem::DUAL && t > 0) w = mbar_wait(mma_done + ((t - 1) & 1), (uint32_t)(((t - 1) / 2) & 1)) && w;
-      ok = bar_and(2, NTHR, w);
-      if (!ok || stop) break;
+      ok = bar_and(2, NTHR, w && epi_ok);
+      if (!ok) break;
       fence_after();
-      K::convert(g, sm, s, ms, tid);
-      fence_async_smem();  // the tile is read by the MMAs (async proxy)
-      mbar_arrive(conv + s);
-    }
-    if (!ok && tid == 0) atomicExch(g.err, 1);
-  } else if (warp >= WARP_EPI) {
-    // -------------------------------------------------- epilogue warps
-    const int et = tid - WARP_EPI * 32;
-    int row_acc = 0;  // M-step: accumulator of the current row
-    for (int t = 0;; ++t) {
-      const int ms = t % NS, s = t & 1;
-      if (!mbar_wait(mfull + ms, (uint32_t)((t / NS) & 1))) {
-        if (et == 0) atomicExch(g.err, 1);
-        break;
-      }
-      const Meta &meta = metas[ms];
-      if (meta.n < 0) break;
+      // tile t - 2's epilogue ran in the last iteration: its slot is free
+      if (tid == 0 && t >= 2) mbar_arrive(mempty + (t - 2) % NS);
       uint32_t acc_sel = (uint32_t)s;
-      if (MODE == MSTEP) {
-        if (meta.flags & 1) row_acc ^= 1;
-        acc_sel = (uint32_t)row_acc;
+      if (!stop) {
+        if (MODE == MSTEP) {
+          if (meta.flags & 1) row_acc ^= 1;
+          acc_sel = (uint32_t)row_acc;
+        }
+        K::convert(g, sm, s, ms, tid);
+        fence_async_smem();  // the tile is read by the MMAs (async proxy)
+        mbar_arrive(conv + s);
       }
-      // agreed over all epilogue threads (barrier 3), so that a time-out
-      // leaves none of them inside the epilogue's named barrier
-      const bool w = bar_and(3, ETHR, mbar_wait(mma_done + s, (uint32_t)((t / 2) & 1)));
-      if (!w) {
-        if (et == 0) atomicExch(g.err, 1);
-        break;
+      if (t > 0) {
+        // two A tiles: the previous tile's MMAs may still run (waited per warp;
+        // a time-out skips the epilogue and ends the loop at the next barrier)
+        if (Smem::DUAL)
+          epi_ok = __all_sync(0xffffffffu, mbar_wait(mma_done + ((t - 1) & 1), (uint32_t)(((t - 1) / 2) & 1)));
+        if (epi_ok) {
+          fence_after();
+          K::epilogue(g, sm, (t - 1) % NS, tmem, (uint32_t)prev_acc, tid);
+          fence_before();
+        }
       }
-      fence_after();
-      K::epilogue(g, sm, ms, tmem, acc_sel, et);
-      fence_before();
-      mbar_arrive(edone + s);
-      mbar_arrive(mempty + ms);  // every reader of slot ms is done with this tile
+      prev_acc = (int)acc_sel;
+      if (stop) break;
     }
+    if ((!ok || !epi_ok) && tid == 0) atomicExch(g.err, 1);  // the MMA warp waits for its own MMAs
     if (MODE == PRED) {
-      bar_sync(1, ETHR);
+      bar_sync(2, NTHR);
       const float *pm = reinterpret_cast<const float *>(sm + Smem::PM);
-      for (int64_t i = et; i < g.qn; i += ETHR) {
+      for (int64_t i = tid; i < g.qn; i += NTHR) {
         g.ws_m[(int64_t)blockIdx.x * g.Nq + g.q0 + i] = pm[i];
         g.ws_s[(int64_t)blockIdx.x * g.Nq + g.q0 + i] = pm[PQ + i];
       }
