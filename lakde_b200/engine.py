@@ -429,6 +429,20 @@ class FusedHier(FusedVI):
             self._gram_out = torch.empty(self.D, self.D, dtype=torch.float64, device=self.device)
         return K.weighted_gram(self.U, weights, out=self._gram_out, workspace=self._gram_ws)
 
+    def kernel_launches(self):
+        """The library launches of one iteration as callables by kernel name
+        (to time them one by one; the step runs them in this order)."""
+        p = self.pattern
+        mixed = self.precision == "mixed"
+        return {
+            ("mstep_tc" if mixed else "mstep"): self.mstep,
+            "posterior_factor": self.factor,
+            ("estep_tc" if mixed else "estep_logrho"): self.estep_numerators,
+            "estep_normalise": lambda: K.estep_normalise(p.cptr, p.pos, self.logrho, self.r, self.c, self.rsum, 1,
+                                                         self.threshold),
+            "weighted_gram": lambda: self._lambda_contrib(self.nu * (self.a / self.b)),
+        }
+
     def init_summaries(self):
         """lakde/local_hierarchical_kde.py:198-258 at block_size = N."""
         self.refresh_points()

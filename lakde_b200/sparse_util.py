@@ -111,6 +111,17 @@ class PairPattern:
         return cls.from_pairs(kern, point, N, N, rank)
 
     @classmethod
+    def from_knn_counts(cls, graph, counts):
+        """Uneven neighbourhoods: point m is explained by its first counts[m]
+        nearest kernels graph[m, :counts[m]] (graph [N, Kmax], counts <= Kmax)."""
+        N, Kmax = graph.shape
+        counts = torch.as_tensor(counts, device=graph.device).long().clamp(0, Kmax)
+        keep = torch.arange(Kmax, device=graph.device)[None, :] < counts[:, None]
+        kern = graph.long()[keep]
+        point = torch.arange(N, device=graph.device).repeat_interleave(counts)
+        return cls.from_pairs(kern, point, N, N)
+
+    @classmethod
     def from_neighbour_lists(cls, graph, counts):
         """Variable-length candidate lists: the first counts[m] entries of graph[m]."""
         N, K = graph.shape
