@@ -15,7 +15,6 @@ namespace lakde {
 
 constexpr int kGramBlocks = 592;
 constexpr int kGramThreads = 160;  // >= the 136 lower 4 x 4 blocks at D = 64
-constexpr int kGramPer = (64 * 64 + kGramThreads - 1) / kGramThreads;  // staged elements per thread
 
 template <typename T>
 __global__ void __launch_bounds__(kGramThreads) gram_partial_kernel(const T *__restrict__ W, const T *__restrict__ w,
@@ -36,29 +35,15 @@ __global__ void __launch_bounds__(kGramThreads) gram_partial_kernel(const T *__r
     for (int y = 0; y < 4; ++y) acc[x][y] = 0.0;
   const int64_t n0 = (int64_t)blockIdx.x * chunk;
   const int64_t n1 = (n0 + chunk < N) ? n0 + chunk : N;
-  // the next kernel's elements are loaded into registers while this one's
-  // products run (element e = tid + kGramThreads u: row e / DP, column e % DP)
-  T pre[kGramPer];
-  auto load = [&](int64_t n) {
-    const T *Wn = W + n * (int64_t)D * D;
-#pragma unroll
-    for (int u = 0; u < kGramPer; ++u) {
-      const int e = tid + kGramThreads * u;
-      const int i = e / DP, j = e % DP;
-      pre[u] = (e < DP * DP && i < D && j < D && j >= i) ? Wn[i * D + j] : T(0);
-    }
-  };
-  if (n0 < n1) load(n0);
   for (int64_t n = n0; n < n1; ++n) {
+    const T *Wn = W + n * (int64_t)D * D;
     __syncthreads();
-    // stored transposed: column j of W_triu_n as row j
-#pragma unroll
-    for (int u = 0; u < kGramPer; ++u) {
-      const int e = tid + kGramThreads * u;
-      if (e < DP * DP) sWt[(e % DP) * DP + e / DP] = (double)pre[u];
+    // coalesced over the row-major W_triu_n, stored transposed
+    for (int e = tid; e < DP * DP; e += kGramThreads) {
+      const int i = e / DP, j = e % DP;
+      sWt[j * DP + i] = (i < D && j < D && j >= i) ? (double)Wn[i * D + j] : 0.0;
     }
     __syncthreads();
-    if (n + 1 < n1) load(n + 1);
     if (!active) continue;
     const double wn = (double)w[n];
     double t[4][4];
