@@ -516,8 +516,11 @@ LAKDE_API int lakde_log_pred_density_bwd(int dtype, int64_t N, int64_t Nq,
  * that would need more than 16 MiB of scratch (see
  * lakde_log_pred_density_workspace) are rejected with LAKDE_EINVAL; split the
  * queries.  The first call on each device looks up the array's device address
- * with that device current; make that first call before any stream capture.
- * All calls share the array: calls that overlap on the GPU race on it.
+ * with that device current and keeps it for the life of the process, so it is
+ * stale after a cudaDeviceReset (or any re-creation of the primary context):
+ * do not use this entry point across a device reset.  Make the first call
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race on it.
  */
 LAKDE_API int lakde_log_pred_density_noalloc(int dtype, int64_t N, int64_t Nq,
                                              int64_t D, const void *X,
