@@ -324,17 +324,27 @@ def run_reference(args):
     rng = np.random.default_rng(0)
     perm = rng.permutation(N)
     pool = Xtr[: min(N, 50_000)].astype(np.float64)
+    pool_sq = (pool * pool).sum(1)
+    nbr_cache = {}
+
+    def knn_rows(rows):
+        # squared distances by |x|^2 + |p|^2 - 2 x.p (one GEMM, no [rows, pool, D] temporary)
+        key = (int(rows[0]), len(rows)) if len(rows) else None
+        if key not in nbr_cache:
+            xr = Xtr[rows].astype(np.float64)
+            d = (xr * xr).sum(1)[:, None] + pool_sq[None, :] - 2.0 * (xr @ pool.T)
+            nbr_cache.clear()
+            nbr_cache[key] = np.argpartition(d, k, axis=1)[:, :k]
+        return nbr_cache[key]
 
     def source(start, count):
         rows = perm[start:start + count].astype(np.int64)
-        d = ((Xtr[rows, None, :].astype(np.float64) - pool[None]) ** 2).sum(-1)
-        nbr = np.argpartition(d, k, axis=1)[:, :k]
+        nbr = knn_rows(rows)
         ptr = np.arange(0, (len(rows) + 1) * k, k, dtype=np.int64)
         return rows, ptr, nbr.reshape(-1).astype(np.int64)
 
     def sigma0_fn(rows):
-        d = ((Xtr[rows, None, :].astype(np.float64) - pool[None]) ** 2).sum(-1)
-        nbr = np.argpartition(d, k, axis=1)[:, :k]
+        nbr = knn_rows(rows)
         diff = pool[nbr] - Xtr[rows][:, None, :]
         sig = np.einsum("nki,nkj->nij", diff, diff) / k + 1e-6 * np.eye(D)
         return sig.astype(np.float32), np.linalg.cholesky(sig).astype(np.float32)
