@@ -453,7 +453,7 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
       assemble_tiles<T, DP>(g, n, scale, jt, M, tstage, lane);
     }
     __syncwarp();
-    ok = lout ? dmma::chol_blocked<NT, T>(M, scratch, rdiag, lane, lout, D) : dmma::chol_blocked_la<NT>(M, rdiag, lane);
+    ok = dmma::chol_blocked<NT, T>(M, scratch, rdiag, lane, lout, D);
     if (ok) jit = jt;
     __syncwarp();
   }

@@ -128,150 +128,6 @@ __device__ __forceinline__ bool diag_tile(double *t, double *rdiag, double *lt, 
   return ok;
 }
 
-// The register part of diag_tile: Cholesky and inverse of the 8 x 8 tile t
-// into a (packed lower, the inverse on return) and rd (1 / L_kk), with no
-// barrier and no store, so that the compiler can interleave it with
-// independent tile products.  Returns whether every pivot was positive.
-__device__ __forceinline__ bool diag_compute(const double *t, double (&a)[36], double (&rd)[8]) {
-#pragma unroll
-  for (int i = 0; i < 8; ++i)
-#pragma unroll
-    for (int j = 0; j <= i; j += 2) {
-      const double2 v = *reinterpret_cast<const double2 *>(t + i * 8 + j);
-      a[i * (i + 1) / 2 + j] = v.x;
-      if (j + 1 <= i) a[i * (i + 1) / 2 + j + 1] = v.y;
-    }
-  bool ok = true;
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const double piv = a[k * (k + 1) / 2 + k];
-    ok = ok && (piv > 0.0);
-    const double rs = rsqrt(piv > 0.0 ? piv : 1.0);
-    rd[k] = rs;
-    a[k * (k + 1) / 2 + k] = piv * rs;
-#pragma unroll
-    for (int i = k + 1; i < 8; ++i) a[i * (i + 1) / 2 + k] *= rs;
-#pragma unroll
-    for (int i = k + 1; i < 8; ++i)
-#pragma unroll
-      for (int j = k + 1; j <= i; ++j)
-        a[i * (i + 1) / 2 + j] = fma(-a[i * (i + 1) / 2 + k], a[j * (j + 1) / 2 + k], a[i * (i + 1) / 2 + j]);
-  }
-#pragma unroll
-  for (int j = 7; j >= 0; --j) {
-    double col[8];
-#pragma unroll
-    for (int i = j + 1; i < 8; ++i) {
-      double sacc = 0.0;
-#pragma unroll
-      for (int k = j + 1; k <= i; ++k) sacc = fma(a[i * (i + 1) / 2 + k], a[k * (k + 1) / 2 + j], sacc);
-      col[i] = -sacc * rd[j];
-    }
-#pragma unroll
-    for (int i = j + 1; i < 8; ++i) a[i * (i + 1) / 2 + j] = col[i];
-    a[j * (j + 1) / 2 + j] = rd[j];
-  }
-  return ok;
-}
-
-// Writes what diag_compute produced: inv(L_KK) (lower, zero upper) into t and
-// 1 / L_kk into rdiag (lane 0; every lane holds the same values).
-__device__ __forceinline__ void diag_store(double *t, double *rdiag, const double (&a)[36], const double (&rd)[8],
-                                           int lane) {
-  __syncwarp();
-  if (lane == 0) {
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-#pragma unroll
-      for (int j = 0; j < 8; j += 2)
-        *reinterpret_cast<double2 *>(t + i * 8 + j) =
-            make_double2((j <= i) ? a[i * (i + 1) / 2 + j] : 0.0, (j + 1 <= i) ? a[i * (i + 1) / 2 + j + 1] : 0.0);
-    }
-#pragma unroll
-    for (int i = 0; i < 8; i += 2) *reinterpret_cast<double2 *>(rdiag + i) = make_double2(rd[i], rd[i + 1]);
-  }
-  __syncwarp();
-}
-
-// Blocked right-looking Cholesky with look-ahead (no L output): in step K the
-// trailing update of tile (K + 1, K + 1) comes first, then that tile's
-// factor and inverse are computed in registers while the rest of step K's
-// trailing update runs (independent products, no barrier in between); they
-// are stored at the start of step K + 1.  Same arithmetic, in the same order
-// per element, as chol_blocked.
-template <int NT>
-__device__ __forceinline__ bool chol_blocked_la(double *M, double *rdiag, int lane) {
-  double a[36], rd[8];
-  bool ok = diag_compute(M, a, rd);
-#pragma unroll 1
-  for (int K = 0; K < NT; ++K) {
-    double *dk = M + tix(K, K);
-    diag_store(dk, rdiag + 8 * K, a, rd, lane);
-    if (!ok) return false;
-    // panel: L_IK = A_IK inv(L_KK)^T
-    const double b0 = bfrag_t(dk, 0, lane), b1 = bfrag_t(dk, 1, lane);
-    double pc[NT][2];
-#pragma unroll
-    for (int I = 1; I < NT; ++I) {
-      if (I > K) {
-        const double *t = M + tix(I, 0) + K * TILE;
-        pc[I][0] = 0.0;
-        pc[I][1] = 0.0;
-        mma(pc[I][0], pc[I][1], afrag(t, 0, lane), b0);
-        mma(pc[I][0], pc[I][1], afrag(t, 1, lane), b1);
-      }
-    }
-    __syncwarp();
-#pragma unroll
-    for (int I = 1; I < NT; ++I)
-      if (I > K) store_c(M + tix(I, 0) + K * TILE, lane, pc[I][0], pc[I][1]);
-    __syncwarp();
-    double pa[NT][2];
-#pragma unroll
-    for (int I = 1; I < NT; ++I) {
-      if (I > K) {
-        pa[I][0] = afrag(M + tix(I, 0) + K * TILE, 0, lane);
-        pa[I][1] = afrag(M + tix(I, 0) + K * TILE, 1, lane);
-      }
-    }
-    if (K + 1 < NT) {
-      // the next diagonal tile first, then its factor while the rest updates
-      double *t = M + tix(K + 1, K + 1);
-      double q0 = 0.0, q1 = 0.0;  // pa[K + 1] without a run-time register index
-#pragma unroll
-      for (int I = 1; I < NT; ++I)
-        if (I == K + 1) {
-          q0 = pa[I][0];
-          q1 = pa[I][1];
-        }
-      double c0, c1;
-      load_c(t, lane, c0, c1);
-      mma(c0, c1, -q0, q0);
-      mma(c0, c1, -q1, q1);
-      store_c(t, lane, c0, c1);
-      __syncwarp();
-      ok = diag_compute(t, a, rd);
-    }
-#pragma unroll
-    for (int J = 1; J < NT; ++J) {
-      if (J > K) {
-#pragma unroll
-        for (int I = J; I < NT; ++I) {
-          if (I == K + 1 && J == K + 1) continue;
-          double *t = M + tix(I, J);
-          double c0, c1;
-          load_c(t, lane, c0, c1);
-          mma(c0, c1, -pa[I][0], pa[J][0]);
-          mma(c0, c1, -pa[I][1], pa[J][1]);
-          store_c(t, lane, c0, c1);
-        }
-      }
-    }
-    __syncwarp();
-  }
-  return true;
-}
-
 // Blocked right-looking Cholesky of the tiled matrix M.  On return the
 // diagonal tiles hold inv(L_KK) and the off-diagonal tiles L_IK; rdiag[i]
 // holds 1 / L_ii.  If lout is given (row-major D x D), the
