@@ -153,12 +153,6 @@ __device__ __forceinline__ void prefetch_l2(const void *src, uint32_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
 
-// L2 prefetch of the 128-byte lines of one row (an ordinary memory
-// instruction per line: far cheaper to issue than a bulk prefetch).
-__device__ __forceinline__ void prefetch_row_l2(const float *src, uint32_t bytes) {
-  for (uint32_t o = 0; o < bytes; o += 128)
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char *>(src) + o));
-}
 
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -502,8 +496,8 @@ struct Kern {
     int32_t *cidx = reinterpret_cast<int32_t *>(sm + Smem::CIDX) + ms * MT;
     float *rv = reinterpret_cast<float *>(sm + Smem::RV) + ms * MT;
     const uint32_t rb = (uint32_t)(((g.D + 3) / 4) * 16);  // bytes per row
-    // this slot is up to NS - 2 tiles ahead of the converters: pull its pair
-    // rows (and a new row's W cores) into L2 now, so the gather finds them there
+    // this slot is up to NS - 2 tiles ahead of the converters: pull a new
+    // row's W cores and kernel centre into L2 now
     if (MODE != PRED && lane == 0 && (t.flags & 1)) {
       if (MODE == ESTEP) prefetch_l2(g.Wc + t.n * (int64_t)(g.ntile * 128), (uint32_t)g.ntile * 512u);
       prefetch_l2(g.X + (t.n + g.koff) * g.ldx, rb);
@@ -520,7 +514,6 @@ struct Kern {
         wk = 0.f;
         bad = 1;
       }
-      if (MODE != PRED && p < t.cnt && ck >= 0) prefetch_row_l2(g.X + (int64_t)ck * g.ldx, rb);
       cidx[p] = ck;
       if (MODE == MSTEP) {
         rv[p] = sqrtf(wk > 0.f ? wk : 0.f);  // the converters scale by sqrt(r)
