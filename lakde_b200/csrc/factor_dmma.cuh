@@ -1,4 +1,4 @@
-// Warp-level FP64 blocked Cholesky, triangular inverse and trace on the FP64
+// Warp-level FP64 blocked Cholesky with its triangular inverse on the FP64
 // tensor cores (mma.sync m8n8k4 f64), for the batched posterior factorisation
 // with 16 <= D <= 64.
 //
@@ -54,9 +54,10 @@ __device__ __forceinline__ double c_to_b(double c0, double c1, int s, int lane) 
   return ((lane >> 2) & 1) ? v1 : v0;
 }
 
-// Cholesky and inverse of the 8 x 8 diagonal tile t (lower part), computed
-// redundantly by every lane from broadcast shared-memory reads (no shuffles
-// on the critical path).  On return t holds inv(L_KK) (lower, zero upper)
+// Cholesky and inverse of the 8 x 8 diagonal tile t (lower part): the
+// Cholesky redundantly on every lane from broadcast shared-memory reads (no
+// shuffles on its rsqrt chain), the inverse one column per lane.  On return
+// t holds inv(L_KK) (lower, zero upper)
 // and rdiag[k] = 1 / L_kk.  Returns false (warp-uniform) if a
 // pivot is not positive.  If lt is given, L_KK (lower, zero upper) is written
 // there too.
@@ -94,33 +95,26 @@ __device__ __forceinline__ bool diag_tile(double *t, double *rdiag, double *lt, 
 #pragma unroll
       for (int j = 0; j < 8; ++j) lt[i * 8 + j] = (j <= i) ? a[i * (i + 1) / 2 + j] : 0.0;
   }
-  // X = L^-1 in place, column by column from the right: with the block below
-  // and right of (j, j) already inverted, X_jj = 1 / L_jj and
-  // X_ij = -X_jj sum_{k=j+1}^{i} X_ik L_kj (i > j)
+  // X = L^-1 by forward substitution, one column per lane (j = lane % 8):
+  // X_ij = (δ_ij - sum_{k<i} L_ik X_kj) / L_ii, zero above the diagonal.  The
+  // lanes run the same instructions on their own column (36 FP64 operations
+  // instead of the whole inverse on every lane); X_(i-1)j enters last, so the
+  // chain is one FMA and one multiply per row.
+  const int jc = lane & 7;
+  double x[8];
 #pragma unroll
-  for (int j = 7; j >= 0; --j) {
-    double col[8];
+  for (int i = 0; i < 8; ++i) {
+    double acc = (i == jc) ? 1.0 : 0.0;
 #pragma unroll
-    for (int i = j + 1; i < 8; ++i) {
-      double sacc = 0.0;
-#pragma unroll
-      for (int k = j + 1; k <= i; ++k) sacc = fma(a[i * (i + 1) / 2 + k], a[k * (k + 1) / 2 + j], sacc);
-      col[i] = -sacc * rd[j];
-    }
-#pragma unroll
-    for (int i = j + 1; i < 8; ++i) a[i * (i + 1) / 2 + j] = col[i];
-    a[j * (j + 1) / 2 + j] = rd[j];
+    for (int k = 0; k < i; ++k) acc = fma(-a[i * (i + 1) / 2 + k], x[k], acc);
+    x[i] = acc * rd[i];
   }
   __syncwarp();
-  // lane 0 writes, in pairs: every lane holds the same values
+  if (lane < 8) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) t[i * 8 + jc] = x[i];
+  }
   if (lane == 0) {
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-#pragma unroll
-      for (int j = 0; j < 8; j += 2)
-        *reinterpret_cast<double2 *>(t + i * 8 + j) =
-            make_double2((j <= i) ? a[i * (i + 1) / 2 + j] : 0.0, (j + 1 <= i) ? a[i * (i + 1) / 2 + j + 1] : 0.0);
-    }
 #pragma unroll
     for (int i = 0; i < 8; i += 2) *reinterpret_cast<double2 *>(rdiag + i) = make_double2(rd[i], rd[i + 1]);
   }
@@ -128,14 +122,24 @@ __device__ __forceinline__ bool diag_tile(double *t, double *rdiag, double *lt, 
   return ok;
 }
 
-// Blocked right-looking Cholesky of the tiled matrix M.  On return the
-// diagonal tiles hold inv(L_KK) and the off-diagonal tiles L_IK; rdiag[i]
-// holds 1 / L_ii.  If lout is given (row-major D x D), the
-// factor L is written there as well (through the scratch tile).  The step loop runs at run time (small
-// code); the tile loops inside a step are unrolled and predicated.
+// Blocked right-looking Cholesky of the tiled matrix M with the inverse
+// X = L^-1 formed in the same sweep.  Forward substitution L X = I by row
+// blocks gives X_KK = inv(L_KK), X_KJ = inv(L_KK) X'_KJ and, for the rows
+// below, X'_IJ -= L_IK X_KJ, so step K:
+//   1. factorises the diagonal tile (inv(L_KK) in place of A_KK);
+//   2. forms the panel L_IK = A_IK inv(L_KK)^T (I > K) and, independently,
+//      the finished row X_KJ = inv(L_KK) X'_KJ (J < K);
+//   3. per column J: the trailing update A_IJ -= L_IK L_JK^T (J > K) or the
+//      substitution update X'_IJ -= L_IK X_KJ (J <= K, I > K), both with the
+//      panel's A fragments.
+// Column K of L is consumed in step K, and X'_IK (= -L_IK X_KK) takes its
+// tile.  On return the tiles hold X (diagonal tiles inv(L_KK)) and rdiag[i]
+// holds 1 / L_ii.  If lout is given (row-major D x D), the factor L is
+// written there as well.  The step loop runs at run time (small code); the
+// tile loops inside a step are unrolled and predicated.
 template <int NT, typename T>
-__device__ __forceinline__ bool chol_blocked(double *M, double *scratch, double *rdiag, int lane, T *lout,
-                                             int D) {
+__device__ __forceinline__ bool chol_inv_blocked(double *M, double *scratch, double *rdiag, int lane, T *lout,
+                                                 int D) {
 #pragma unroll 1
   for (int K = 0; K < NT; ++K) {
     double *dk = M + tix(K, K);
@@ -146,39 +150,63 @@ __device__ __forceinline__ bool chol_blocked(double *M, double *scratch, double 
         if (i < D && j < D) lout[i * D + j] = (T)scratch[e];
       }
     }
-    // panel: L_IK = A_IK inv(L_KK)^T
-    const double b0 = bfrag_t(dk, 0, lane), b1 = bfrag_t(dk, 1, lane);
-    double pc[NT][2];
+    // fragments of inv(L_KK): B = inv(L_KK)^T for the panel, A = inv(L_KK)
+    // for the finished row of X (the same elements)
+    const double g0 = afrag(dk, 0, lane), g1 = afrag(dk, 1, lane);
+    double pc[NT][2], xr[NT][2];
 #pragma unroll
     for (int I = 1; I < NT; ++I) {
       if (I > K) {
         const double *t = M + tix(I, 0) + K * TILE;
         pc[I][0] = 0.0;
         pc[I][1] = 0.0;
-        mma(pc[I][0], pc[I][1], afrag(t, 0, lane), b0);
-        mma(pc[I][0], pc[I][1], afrag(t, 1, lane), b1);
+        mma(pc[I][0], pc[I][1], afrag(t, 0, lane), g0);
+        mma(pc[I][0], pc[I][1], afrag(t, 1, lane), g1);
+      }
+    }
+#pragma unroll
+    for (int J = 0; J < NT - 1; ++J) {
+      if (J < K) {
+        const double *t = M + tix(K, J);
+        xr[J][0] = 0.0;
+        xr[J][1] = 0.0;
+        mma(xr[J][0], xr[J][1], g0, bfrag(t, 0, lane));
+        mma(xr[J][0], xr[J][1], g1, bfrag(t, 1, lane));
       }
     }
     __syncwarp();
 #pragma unroll
     for (int I = 1; I < NT; ++I)
       if (I > K) store_c(M + tix(I, 0) + K * TILE, lane, pc[I][0], pc[I][1]);
+#pragma unroll
+    for (int J = 0; J < NT - 1; ++J)
+      if (J < K) store_c(M + tix(K, J), lane, xr[J][0], xr[J][1]);
     __syncwarp();
-    // A fragments of the new panel (= B fragments of its transpose)
+    if (lout) {
+      for (int I = K + 1; I < NT; ++I)
+        for (int e = lane; e < 64; e += 32) {
+          const int i = 8 * I + e / 8, j = 8 * K + e % 8;
+          if (i < D && j < D) lout[i * D + j] = (T)M[tix(I, K) + e];
+        }
+    }
+    // A fragments of the panel (= B fragments of its transpose); the tiles
+    // (I, K) are rewritten with X'_IK below, after every lane has read them
     double pa[NT][2];
 #pragma unroll
     for (int I = 1; I < NT; ++I) {
       if (I > K) {
-        pa[I][0] = afrag(M + tix(I, 0) + K * TILE, 0, lane);
-        pa[I][1] = afrag(M + tix(I, 0) + K * TILE, 1, lane);
+        pa[I][0] = afrag(M + tix(I, K), 0, lane);
+        pa[I][1] = afrag(M + tix(I, K), 1, lane);
       }
     }
-    // trailing update: A_IJ -= L_IK L_JK^T, K < J <= I (each lane touches its own C elements)
+    __syncwarp();
 #pragma unroll
-    for (int J = 1; J < NT; ++J) {
+    for (int J = 0; J < NT; ++J) {
+      // keeps the loads of two columns of tiles together (register pressure;
+      // the second column's loads overlap the first one's products)
+      if ((J & 1) == 0) asm volatile("" ::: "memory");
       if (J > K) {
-        // keeps the loads of one column of tiles together (register pressure)
-        asm volatile("" ::: "memory");
+        // trailing update: A_IJ -= L_IK L_JK^T, J <= I
 #pragma unroll
         for (int I = J; I < NT; ++I) {
           double *t = M + tix(I, J);
@@ -188,67 +216,26 @@ __device__ __forceinline__ bool chol_blocked(double *M, double *scratch, double 
           mma(c0, c1, -pa[I][1], pa[J][1]);
           store_c(t, lane, c0, c1);
         }
+      } else if (K + 1 < NT) {
+        // substitution update: X'_IJ -= L_IK X_KJ, I > K (X'_IK starts at 0)
+        const double *xk = M + tix(K, J);
+        const double b0 = bfrag(xk, 0, lane), b1 = bfrag(xk, 1, lane);
+#pragma unroll
+        for (int I = 1; I < NT; ++I) {
+          if (I > K) {
+            double *t = M + tix(I, J);
+            double c0 = 0.0, c1 = 0.0;
+            if (J < K) load_c(t, lane, c0, c1);
+            mma(c0, c1, -pa[I][0], b0);
+            mma(c0, c1, -pa[I][1], b1);
+            store_c(t, lane, c0, c1);
+          }
+        }
       }
     }
     __syncwarp();
-    if (lout) {
-      for (int I = K + 1; I < NT; ++I)
-        for (int e = lane; e < 64; e += 32) {
-          const int i = 8 * I + e / 8, j = 8 * K + e % 8;
-          if (i < D && j < D) lout[i * D + j] = (T)M[tix(I, K) + e];
-        }
-    }
   }
   return true;
-}
-
-// In-place blocked inverse: on entry the diagonal tiles hold inv(L_II) and the
-// off-diagonal tiles L_IJ; on return the tiles hold X = L^-1.  Row block by
-// row block: X_IJ = -inv(L_II) sum_{K=J}^{I-1} L_IK X_KJ needs the finished
-// rows above and the L tiles of row I only, so the I tiles of row I are
-// independent; their products are interleaved (K outer, J inner) and they are
-// stored together once all of them are computed.
-template <int NT>
-__device__ __forceinline__ void trtri_blocked(double *M, int lane) {
-#pragma unroll 1
-  for (int I = 1; I < NT; ++I) {
-    const double *rowI = M + tix(I, 0);
-    double c[NT][2];
-#pragma unroll
-    for (int J = 0; J < NT; ++J) {
-      c[J][0] = 0.0;
-      c[J][1] = 0.0;
-    }
-#pragma unroll 1
-    for (int K = 0; K < I; ++K) {
-      const double a0 = afrag(rowI + K * TILE, 0, lane), a1 = afrag(rowI + K * TILE, 1, lane);
-      const double *rowK = M + (K * (K + 1) / 2) * TILE;
-#pragma unroll
-      for (int J = 0; J < NT - 1; ++J) {
-        if (J <= K) {
-          mma(c[J][0], c[J][1], a0, bfrag(rowK + J * TILE, 0, lane));
-          mma(c[J][0], c[J][1], a1, bfrag(rowK + J * TILE, 1, lane));
-        }
-      }
-    }
-    const double *di = rowI + I * TILE;
-    const double n0 = -afrag(di, 0, lane), n1 = -afrag(di, 1, lane);
-    double xo[NT][2];
-#pragma unroll
-    for (int J = 0; J < NT - 1; ++J) {
-      if (J < I) {
-        xo[J][0] = 0.0;
-        xo[J][1] = 0.0;
-        mma(xo[J][0], xo[J][1], n0, c_to_b(c[J][0], c[J][1], 0, lane));
-        mma(xo[J][0], xo[J][1], n1, c_to_b(c[J][0], c[J][1], 1, lane));
-      }
-    }
-    __syncwarp();
-#pragma unroll
-    for (int J = 0; J < NT - 1; ++J)
-      if (J < I) store_c(M + tix(I, 0) + J * TILE, lane, xo[J][0], xo[J][1]);
-    __syncwarp();
-  }
 }
 
 }  // namespace dmma
