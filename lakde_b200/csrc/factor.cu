@@ -425,6 +425,9 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
   const T scale = posterior_scale(g, n);
   T jit = g.jitter[n];
   T *lout = g.L ? g.L + n * (int64_t)D * D : nullptr;
+  // tiled FP32 input with its T_n tiles staged: the trace runs inside the sweep
+  const bool fused_trace = staged && tiled;
+  double trace_acc = 0.0;
   bool ok = false;
   for (int attempt = 0; attempt <= 32 && !ok; ++attempt) {
     T jt = jit;
@@ -453,7 +456,8 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
       assemble_tiles<T, DP>(g, n, scale, jt, M, tstage, lane);
     }
     __syncwarp();
-    ok = dmma::chol_inv_blocked<NT, T>(M, scratch, rdiag, lane, lout, D);
+    trace_acc = 0.0;
+    ok = dmma::chol_inv_blocked<NT, T>(M, scratch, rdiag, lane, lout, D, fused_trace ? tstage : nullptr, trace_acc);
     if (ok) jit = jt;
     __syncwarp();
   }
@@ -556,57 +560,8 @@ __device__ __forceinline__ void factor_one(const FactorArgs<T> &g, int64_t n, do
   for (int i = lane; i < D; i += 32) ld += log((double)(T)rdiag[i]);
   ld = warp_sum(ld);
   if (lane == 0) g.logdet[n] = (T)(2.0 * ld);
-  if (staged && tiled) {
-    // ||X T_n||_F^2 with X and T_n lower: (X T)_IA = sum_{A <= K <= I} X_IK T_KA.
-    // Column blocks A and NT - 1 - A run together (one long and one short
-    // accumulation, sharing the A fragments of X), and the squares are
-    // summed per tile before the running total, so no chain spans a block.
-    double acc = 0.0;
-#pragma unroll 1
-    for (int p = 0; p < (NT + 1) / 2; ++p) {
-      const int a0 = p, a1 = NT - 1 - p;
-      double c[NT][2], e[NT][2];
-#pragma unroll
-      for (int I = 0; I < NT; ++I) {
-        c[I][0] = c[I][1] = 0.0;
-        e[I][0] = e[I][1] = 0.0;
-      }
-#pragma unroll
-      for (int K = 0; K < NT; ++K) {
-        if (K < a0) continue;
-        // tile (K, A): local row lane % 4 (+ 4), local column lane / 4
-        const float *t0 = tstage + (K * (K + 1) / 2 + a0) * 64 + (lane & 3) * 8 + (lane >> 2);
-        const double b0 = (double)t0[0], b1 = (double)t0[32];
-        const bool second = K >= a1 && a1 != a0;
-        double f0 = 0.0, f1 = 0.0;
-        if (second) {
-          const float *t1 = tstage + (K * (K + 1) / 2 + a1) * 64 + (lane & 3) * 8 + (lane >> 2);
-          f0 = (double)t1[0];
-          f1 = (double)t1[32];
-        }
-#pragma unroll
-        for (int I = K; I < NT; ++I) {
-          const double *x = M + dmma::tix(I, K);
-          const double x0 = dmma::afrag(x, 0, lane), x1 = dmma::afrag(x, 1, lane);
-          dmma::mma(c[I][0], c[I][1], x0, b0);
-          dmma::mma(c[I][0], c[I][1], x1, b1);
-          if (second) {
-            dmma::mma(e[I][0], e[I][1], x0, f0);
-            dmma::mma(e[I][0], e[I][1], x1, f1);
-          }
-        }
-      }
-      double sq[NT];
-#pragma unroll
-      for (int I = 0; I < NT; ++I)
-        sq[I] = fma(c[I][0], c[I][0], fma(c[I][1], c[I][1], fma(e[I][0], e[I][0], e[I][1] * e[I][1])));
-#pragma unroll
-      for (int w = 1; w < NT; w *= 2)
-#pragma unroll
-        for (int I = 0; I + w < NT; I += 2 * w) sq[I] += sq[I + w];
-      acc += sq[0];
-    }
-    acc = warp_sum(acc);
+  if (fused_trace) {
+    const double acc = warp_sum(trace_acc);
     if (lane == 0) g.trace[n] = (T)acc;
   } else if (staged) {
     // ||X T_n||_F^2 with X lower: (X T)_IA = sum_{K <= I} X_IK T_KA, column

@@ -135,11 +135,15 @@ __device__ __forceinline__ bool diag_tile(double *t, double *rdiag, double *lt, 
 // Column K of L is consumed in step K, and X'_IK (= -L_IK X_KK) takes its
 // tile.  On return the tiles hold X (diagonal tiles inv(L_KK)) and rdiag[i]
 // holds 1 / L_ii.  If lout is given (row-major D x D), the factor L is
-// written there as well.  The step loop runs at run time (small code); the
+// written there as well.  If l0t is given (the lower 8 x 8 tiles of a lower
+// triangular L0 in FP32, same tile order), each lane's share of
+// ||X L0||_F^2 is added to trace_acc: row K of Z = X L0 is
+// Z_KA = sum_{A <= J <= K} X_KJ L0_JA, formed column by column beside the
+// substitution update once row K of X is final.  The step loop runs at run time (small code); the
 // tile loops inside a step are unrolled and predicated.
 template <int NT, typename T>
 __device__ __forceinline__ bool chol_inv_blocked(double *M, double *scratch, double *rdiag, int lane, T *lout,
-                                                 int D) {
+                                                 int D, const float *l0t, double &trace_acc) {
 #pragma unroll 1
   for (int K = 0; K < NT; ++K) {
     double *dk = M + tix(K, K);
@@ -200,6 +204,9 @@ __device__ __forceinline__ bool chol_inv_blocked(double *M, double *scratch, dou
       }
     }
     __syncwarp();
+    double z[NT][2];
+#pragma unroll
+    for (int A = 0; A < NT; ++A) z[A][0] = z[A][1] = 0.0;
 #pragma unroll
     for (int J = 0; J < NT; ++J) {
       // keeps the loads of two columns of tiles together (register pressure;
@@ -216,22 +223,46 @@ __device__ __forceinline__ bool chol_inv_blocked(double *M, double *scratch, dou
           mma(c0, c1, -pa[I][1], pa[J][1]);
           store_c(t, lane, c0, c1);
         }
-      } else if (K + 1 < NT) {
-        // substitution update: X'_IJ -= L_IK X_KJ, I > K (X'_IK starts at 0)
+      } else {
         const double *xk = M + tix(K, J);
-        const double b0 = bfrag(xk, 0, lane), b1 = bfrag(xk, 1, lane);
+        if (K + 1 < NT) {
+          // substitution update: X'_IJ -= L_IK X_KJ, I > K (X'_IK starts at 0)
+          const double b0 = bfrag(xk, 0, lane), b1 = bfrag(xk, 1, lane);
 #pragma unroll
-        for (int I = 1; I < NT; ++I) {
-          if (I > K) {
-            double *t = M + tix(I, J);
-            double c0 = 0.0, c1 = 0.0;
-            if (J < K) load_c(t, lane, c0, c1);
-            mma(c0, c1, -pa[I][0], b0);
-            mma(c0, c1, -pa[I][1], b1);
-            store_c(t, lane, c0, c1);
+          for (int I = 1; I < NT; ++I) {
+            if (I > K) {
+              double *t = M + tix(I, J);
+              double c0 = 0.0, c1 = 0.0;
+              if (J < K) load_c(t, lane, c0, c1);
+              mma(c0, c1, -pa[I][0], b0);
+              mma(c0, c1, -pa[I][1], b1);
+              store_c(t, lane, c0, c1);
+            }
+          }
+        }
+        if (l0t) {
+          // trace row K: Z_KA += X_KJ L0_JA, A <= J (L0 tile: local row
+          // lane % 4 (+ 4), local column lane / 4)
+          const double a0 = afrag(xk, 0, lane), a1 = afrag(xk, 1, lane);
+#pragma unroll
+          for (int A = 0; A <= J; ++A) {
+            const float *tk = l0t + (J * (J + 1) / 2 + A) * 64 + (lane & 3) * 8 + (lane >> 2);
+            mma(z[A][0], z[A][1], a0, (double)tk[0]);
+            mma(z[A][0], z[A][1], a1, (double)tk[32]);
           }
         }
       }
+    }
+    if (l0t) {
+      // ||Z_K.||^2: squares per tile, then a tree over the tiles
+      double sq[NT];
+#pragma unroll
+      for (int A = 0; A < NT; ++A) sq[A] = fma(z[A][0], z[A][0], z[A][1] * z[A][1]);
+#pragma unroll
+      for (int w = 1; w < NT; w *= 2)
+#pragma unroll
+        for (int A = 0; A + w < NT; A += 2 * w) sq[A] += sq[A + w];
+      trace_acc += sq[0];
     }
     __syncwarp();
   }
