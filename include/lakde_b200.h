@@ -67,7 +67,8 @@ LAKDE_API int lakde_max_dim(void);
  *                          that stage no T and write no L (else 0 is used).
  *   LAKDE_TUNE_ROWS:   0 = tensor-core rows from the caller's work queue;
  *                      1 = a static stride over the grid (the queue ignored).
- *   LAKDE_TUNE_VI_ROWS: 0 = lakde_vi_rows with 8 lanes per kernel row;
+ *   LAKDE_TUNE_VI_ROWS: 0 = lakde_vi_rows with a kernel row's pairs on two
+ *                          lanes and its FP64 posterior on one lane per row;
  *                      1 = one thread per kernel row.
  */
 typedef enum {

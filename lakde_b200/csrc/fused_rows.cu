@@ -64,6 +64,28 @@ __device__ __forceinline__ constexpr int tix(int i, int j) { return i * (i + 1) 
 template <typename T, int DP>
 __device__ __forceinline__ void load_row(const T *__restrict__ X, int64_t m, int D, T (&out)[DP]) {
   const uintptr_t base = reinterpret_cast<uintptr_t>(X);
+  // rows of 32 bytes (or 64) from a 32-byte aligned base: one 256-bit load
+  // per 32 bytes, so a warp's gather of scattered rows touches each row's
+  // line once instead of once per 16 bytes
+  if constexpr (sizeof(T) * DP >= 32) {
+    if (D == DP && (base & 31u) == 0) {
+#pragma unroll
+      for (int v = 0; v < (int)(sizeof(T) * DP / 32); ++v) {
+        const T *p = X + m * DP + v * (32 / (int)sizeof(T));
+        if constexpr (sizeof(T) == 4) {
+          asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                       : "=f"(out[8 * v]), "=f"(out[8 * v + 1]), "=f"(out[8 * v + 2]), "=f"(out[8 * v + 3]),
+                         "=f"(out[8 * v + 4]), "=f"(out[8 * v + 5]), "=f"(out[8 * v + 6]), "=f"(out[8 * v + 7])
+                       : "l"(p));
+        } else {
+          asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+                       : "=d"(out[4 * v]), "=d"(out[4 * v + 1]), "=d"(out[4 * v + 2]), "=d"(out[4 * v + 3])
+                       : "l"(p));
+        }
+      }
+      return;
+    }
+  }
   if constexpr (sizeof(T) == 4 && DP >= 4) {
     if (D == DP && (base & 15u) == 0) {
       const float4 *p = reinterpret_cast<const float4 *>(X + m * DP);
@@ -329,157 +351,205 @@ __global__ void __launch_bounds__(128, (sizeof(T) == 4 && DP == 8) ? 3 : 1) vi_r
   }
 }
 
-// The same pass with a kernel row per group of LPR lanes (4 rows per warp):
-// the row's pairs are dealt to the lanes (pair start + l + LPR k to lane l),
-// so a lane gathers a few point rows instead of the whole row's, in batches of
-// B whose gathers are all in flight together.  Each lane accumulates its share
-// of S_n and of sum r; an xor butterfly over the group sums them (every lane
-// ends with the same bits, in a fixed order).  Lane 0 of the group factorises
-// and writes the per-kernel outputs, then broadcasts the factor's pieces;
-// every lane then gathers its pairs again (mostly L2 hits by then) and
-// computes their log rho.  Only S is live across the factorisation.
+// The same pass with the pairs of a kernel row dealt to a group of LPR lanes
+// and the FP64 posterior one row per lane.  A warp takes 32 consecutive rows
+// of the order, 32 / LPR rows at a time in the M- and E-steps: a row's pairs
+// go to the group's lanes (pair start + l + LPR k to lane l, so the index,
+// responsibility and log rho accesses of a warp are coalesced), in batches of
+// B whose gathers are all in flight together.  An xor butterfly sums the
+// group's shares of S_n and sum r (every lane ends with the same bits, in a
+// fixed order) and lane 0 of the group parks them in the row's slot of the
+// warp's shared memory.  Posterior: lane l factorises row l from its slot
+// (all 32 lanes on the FP64 work) and parks the factor's pieces in the same
+// slot, which the groups read back for the E-step.
+template <typename T, int DP>
+struct RowSlot {
+  static constexpr int TT = DP * (DP + 1) / 2;
+  // S (TT), sum r, bad | strictly lower L (TT - DP), 1 / L_ii (DP), c, -nu / 2, ok;
+  // an odd stride keeps the lanes' slots on distinct banks
+  static constexpr int SIZE = (TT + 4) | 1;
+  static constexpr int VSUM = TT, BAD = TT + 1, RINV = TT - DP, CST = TT, EXPO = TT + 1, OK = TT + 2;
+};
+
 template <typename T, int DP, int LPR, int B>
 __global__ void __launch_bounds__(128, 3) vi_rows_lanes_kernel(RowArgs<T> g) {
   constexpr int TT = DP * (DP + 1) / 2;
+  constexpr int GROUPS = 32 / LPR;
   constexpr unsigned FULL = 0xffffffffu;
-  const int lane = threadIdx.x & 31, sub = lane & (LPR - 1), leader = lane & ~(LPR - 1);
-  const int64_t it = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / LPR;
-  const bool live = it < g.N;
-  const int64_t n = live ? (g.order ? (int64_t)g.order[it] : it) : 0;
+  using RS = RowSlot<T, DP>;
+  __shared__ T park[4][32][RS::SIZE];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, sub = lane & (LPR - 1), grp = lane / LPR;
+  const int64_t base = ((int64_t)blockIdx.x * 4 + warp) * 32;
+  T(*slot)[RS::SIZE] = park[warp];
   const int D = g.D;
-  int64_t start = 0, end = 0;
-  if (live) {
-    start = g.rowptr[n];
-    end = g.rowptr[n + 1];
+  // each lane loads the setup of one of the warp's rows (row index, pair
+  // range, its point row); the groups take their row's from that lane
+  int64_t own_n = 0, own_start = 0, own_end = 0;
+  if (base + lane < g.N) {
+    own_n = g.order ? (int64_t)g.order[base + lane] : base + lane;
+    own_start = g.rowptr[own_n];
+    own_end = g.rowptr[own_n + 1];
   }
-  int bad = end < start;
-  if (bad) end = start;
-
-  T xn[DP];
-  load_row<T, DP>(g.X, n + g.koff, D, xn);
+  T own_x[DP];
+  load_row<T, DP>(g.X, own_n + g.koff, D, own_x);
 
   // ---------------------------------------------------------------- M-step
-  T S[TT];
+#pragma unroll 1
+  for (int pass = 0; pass < LPR; ++pass) {
+    const int rl = pass * GROUPS + grp;
+    const int64_t n = __shfl_sync(FULL, own_n, rl);
+    const int64_t start = __shfl_sync(FULL, own_start, rl);
+    int64_t end = __shfl_sync(FULL, own_end, rl);
+    T xn[DP];
 #pragma unroll
-  for (int e = 0; e < TT; ++e) S[e] = T(0);
-  T vsum = T(0);
-  for (int64_t p0 = start + sub; p0 < end; p0 += (int64_t)LPR * B) {
-    int32_t c[B];
-    T v[B];
+    for (int d = 0; d < DP; ++d) xn[d] = __shfl_sync(FULL, own_x[d], rl);
+    int bad = end < start;
+    if (bad) end = start;
+    T S[TT];
 #pragma unroll
-    for (int k = 0; k < B; ++k) {
-      const int64_t p = p0 + (int64_t)LPR * k;
-      c[k] = -1;
-      v[k] = T(0);
-      if (p < end) {
-        c[k] = g.col[p];
-        v[k] = g.r[p];
-        if (c[k] < 0 || c[k] >= g.npts) {
-          bad = 1;
-          c[k] = -1;
+    for (int e = 0; e < TT; ++e) S[e] = T(0);
+    T vsum = T(0);
+    for (int64_t p0 = start + sub; p0 < end; p0 += (int64_t)LPR * B) {
+      int32_t c[B];
+      T v[B];
+#pragma unroll
+      for (int k = 0; k < B; ++k) {
+        const int64_t p = p0 + (int64_t)LPR * k;
+        c[k] = -1;
+        v[k] = T(0);
+        if (p < end) {
+          c[k] = g.col[p];
+          v[k] = g.r[p];
+          if (c[k] < 0 || c[k] >= g.npts) {
+            bad = 1;
+            c[k] = -1;
+          }
         }
       }
+      T dl[B][DP];
+#pragma unroll
+      for (int k = 0; k < B; ++k) {
+        load_row<T, DP>(g.X, c[k] < 0 ? 0 : c[k], D, dl[k]);
+#pragma unroll
+        for (int d = 0; d < DP; ++d) dl[k][d] = (c[k] >= 0 && d < D) ? dl[k][d] - xn[d] : T(0);
+      }
+#pragma unroll
+      for (int k = 0; k < B; ++k) {
+        if (c[k] < 0) continue;
+#pragma unroll
+        for (int i = 0; i < DP; ++i) {
+          const T vi = v[k] * dl[k][i];
+#pragma unroll
+          for (int j = 0; j <= i; ++j) S[tix<DP>(i, j)] = fma(vi, dl[k][j], S[tix<DP>(i, j)]);
+        }
+        vsum += v[k];
+      }
     }
-    T dl[B][DP];
+    // group sums (xor butterfly: the same bits in every lane of the group)
 #pragma unroll
-    for (int k = 0; k < B; ++k) {
-      load_row<T, DP>(g.X, c[k] < 0 ? 0 : c[k], D, dl[k]);
+    for (int off = LPR / 2; off >= 1; off >>= 1) {
 #pragma unroll
-      for (int d = 0; d < DP; ++d) dl[k][d] = (c[k] >= 0 && d < D) ? dl[k][d] - xn[d] : T(0);
+      for (int e = 0; e < TT; ++e) S[e] += __shfl_xor_sync(FULL, S[e], off, LPR);
+      vsum += __shfl_xor_sync(FULL, vsum, off, LPR);
+      bad |= __shfl_xor_sync(FULL, bad, off, LPR);
     }
+    if (sub == 0) {
 #pragma unroll
-    for (int k = 0; k < B; ++k) {
-      if (c[k] < 0) continue;
+      for (int e = 0; e < TT; ++e) slot[rl][e] = S[e];
+      slot[rl][RS::VSUM] = vsum;
+      slot[rl][RS::BAD] = bad ? T(1) : T(0);
+    }
+  }
+  __syncwarp();
+
+  // ------------------------------------------------------ posterior, a lane per row
+  {
+    if (base + lane < g.N) {
+      const int64_t n = own_n;
+      T S[TT];
+#pragma unroll
+      for (int e = 0; e < TT; ++e) S[e] = slot[lane][e];
+      const T nu = g.nu0 + slot[lane][RS::VSUM];
+      const bool bad = slot[lane][RS::BAD] != T(0);
+      double L[TT];
+      T logdet;
+      const bool ok = row_posterior<T, DP>(g, n, S, nu, bad, L, logdet);
 #pragma unroll
       for (int i = 0; i < DP; ++i) {
-        const T vi = v[k] * dl[k][i];
 #pragma unroll
-        for (int j = 0; j <= i; ++j) S[tix<DP>(i, j)] = fma(vi, dl[k][j], S[tix<DP>(i, j)]);
+        for (int j = 0; j < i; ++j) slot[lane][i * (i - 1) / 2 + j] = (T)L[tix<DP>(i, j)];
+        slot[lane][RS::RINV + i] = (T)(1.0 / L[tix<DP>(i, i)]);
       }
-      vsum += v[k];
+      const double e = mvdigamma_d(0.5 * (double)nu, D) + D * 0.69314718055994530942 + (double)logdet;
+      slot[lane][RS::CST] = (T)(0.5 * e);
+      slot[lane][RS::EXPO] = T(-0.5) * nu;
+      slot[lane][RS::OK] = ok ? T(1) : T(0);
     }
   }
-  // group sums (xor butterfly: the same bits in every lane of the group)
-#pragma unroll
-  for (int off = LPR / 2; off >= 1; off >>= 1) {
-#pragma unroll
-    for (int e = 0; e < TT; ++e) S[e] += __shfl_xor_sync(FULL, S[e], off, LPR);
-    vsum += __shfl_xor_sync(FULL, vsum, off, LPR);
-    bad |= __shfl_xor_sync(FULL, bad, off, LPR);
-  }
-
-  // ------------------------------------------------------- posterior, lane 0
-  T Lf[TT], rinv[DP];
-  T cst = T(0), expo = T(0);
-  int ok = 0;
-  const T nu = g.nu0 + vsum;
-  if (sub == 0 && live) {
-    double L[TT];
-    T logdet;
-    ok = row_posterior<T, DP>(g, n, S, nu, bad != 0, L, logdet) ? 1 : 0;
-#pragma unroll
-    for (int i = 0; i < DP; ++i) {
-#pragma unroll
-      for (int j = 0; j < i; ++j) Lf[tix<DP>(i, j)] = (T)L[tix<DP>(i, j)];
-      rinv[i] = (T)(1.0 / L[tix<DP>(i, i)]);
-    }
-    const double e = mvdigamma_d(0.5 * (double)nu, D) + D * 0.69314718055994530942 + (double)logdet;
-    cst = (T)(0.5 * e);
-    expo = T(-0.5) * nu;
-  }
-  // broadcast from the group's lane 0
-  ok = __shfl_sync(FULL, ok, leader);
-  cst = __shfl_sync(FULL, cst, leader);
-  expo = __shfl_sync(FULL, expo, leader);
-#pragma unroll
-  for (int i = 0; i < DP; ++i) {
-#pragma unroll
-    for (int j = 0; j < i; ++j) Lf[tix<DP>(i, j)] = __shfl_sync(FULL, Lf[tix<DP>(i, j)], leader);
-    rinv[i] = __shfl_sync(FULL, rinv[i], leader);
-  }
-  if (!live) return;
+  __syncwarp();
 
   // ---------------------------------------------------------------- E-step
   const T nanv = T(NAN);
-  for (int64_t p0 = start + sub; p0 < end; p0 += (int64_t)LPR * B) {
-    int32_t c[B];
+#pragma unroll 1
+  for (int pass = 0; pass < LPR; ++pass) {
+    const int rl = pass * GROUPS + grp;
+    const int64_t n = __shfl_sync(FULL, own_n, rl);
+    const int64_t start = __shfl_sync(FULL, own_start, rl);
+    int64_t end = __shfl_sync(FULL, own_end, rl);
+    T xn[DP];
 #pragma unroll
-    for (int k = 0; k < B; ++k) {
-      const int64_t p = p0 + (int64_t)LPR * k;
-      c[k] = -1;
-      if (p < end) {
-        c[k] = g.col[p];
-        if (!ok || c[k] < 0 || c[k] >= g.npts) c[k] = -2;
-      }
+    for (int d = 0; d < DP; ++d) xn[d] = __shfl_sync(FULL, own_x[d], rl);
+    if (base + rl >= g.N) continue;
+    if (end < start) end = start;
+    T Lf[TT], rinv[DP];
+#pragma unroll
+    for (int i = 0; i < DP; ++i) {
+#pragma unroll
+      for (int j = 0; j < i; ++j) Lf[tix<DP>(i, j)] = slot[rl][i * (i - 1) / 2 + j];
+      rinv[i] = slot[rl][RS::RINV + i];
     }
-    T dl[B][DP];
+    const T cst = slot[rl][RS::CST], expo = slot[rl][RS::EXPO];
+    const bool ok = slot[rl][RS::OK] != T(0);
+    for (int64_t p0 = start + sub; p0 < end; p0 += (int64_t)LPR * B) {
+      int32_t c[B];
 #pragma unroll
-    for (int k = 0; k < B; ++k) {
-      load_row<T, DP>(g.X, c[k] < 0 ? 0 : c[k], D, dl[k]);
-#pragma unroll
-      for (int d = 0; d < DP; ++d) dl[k][d] = (c[k] >= 0 && d < D) ? dl[k][d] - xn[d] : T(0);
-    }
-#pragma unroll
-    for (int k = 0; k < B; ++k) {
-      const int64_t p = p0 + (int64_t)LPR * k;
-      if (c[k] == -1) continue;  // past the end of the row
-      if (c[k] == -2) {
-        g.logrho[p] = nanv;
-        continue;
+      for (int k = 0; k < B; ++k) {
+        const int64_t p = p0 + (int64_t)LPR * k;
+        c[k] = -1;
+        if (p < end) {
+          c[k] = g.col[p];
+          if (!ok || c[k] < 0 || c[k] >= g.npts) c[k] = -2;
+        }
       }
-      T y[DP];
-      T q = T(0);
+      T dl[B][DP];
 #pragma unroll
-      for (int i = 0; i < DP; ++i) {
-        T s2 = dl[k][i];
+      for (int k = 0; k < B; ++k) {
+        load_row<T, DP>(g.X, c[k] < 0 ? 0 : c[k], D, dl[k]);
 #pragma unroll
-        for (int j = 0; j < i; ++j) s2 = fma(-Lf[tix<DP>(i, j)], y[j], s2);
-        y[i] = s2 * rinv[i];
-        q = fma(y[i], y[i], q);
+        for (int d = 0; d < DP; ++d) dl[k][d] = (c[k] >= 0 && d < D) ? dl[k][d] - xn[d] : T(0);
       }
-      T lr = f_add(f_mul(q, expo), cst);
-      if (c[k] == n + g.koff) lr = neg_inf<T>();
-      g.logrho[p] = lr;
+#pragma unroll
+      for (int k = 0; k < B; ++k) {
+        const int64_t p = p0 + (int64_t)LPR * k;
+        if (c[k] == -1) continue;  // past the end of the row
+        if (c[k] == -2) {
+          g.logrho[p] = nanv;
+          continue;
+        }
+        T y[DP];
+        T q = T(0);
+#pragma unroll
+        for (int i = 0; i < DP; ++i) {
+          T s2 = dl[k][i];
+#pragma unroll
+          for (int j = 0; j < i; ++j) s2 = fma(-Lf[tix<DP>(i, j)], y[j], s2);
+          y[i] = s2 * rinv[i];
+          q = fma(y[i], y[i], q);
+        }
+        T lr = f_add(f_mul(q, expo), cst);
+        if (c[k] == n + g.koff) lr = neg_inf<T>();
+        g.logrho[p] = lr;
+      }
     }
   }
 }
@@ -549,9 +619,11 @@ extern "C" int lakde_vi_rows(int dtype, int64_t N, int64_t D, int64_t npts, cons
         vi_rows_kernel<TT, 8><<<blocks, 128, 0, as_stream(stream)>>>(g);
       return check_launch("vi_rows");
     }
-    // 8 lanes per row (16 rows per 128-thread block)
-    constexpr int LPR = 8, B = sizeof(TT) == 4 ? 4 : 2;
-    const int64_t blocks = (N * LPR + 127) / 128;
+    // 2 lanes per row for the pairs, a lane per row for the posterior (128
+    // rows per 128-thread block; 8 lanes per row measured 10 % slower: more
+    // passes of fewer rows each)
+    constexpr int LPR = 2, B = sizeof(TT) == 4 ? 4 : 2;
+    const int64_t blocks = (N + 127) / 128;
     if (blocks > 0x7fffffffLL) {
       set_error("vi_rows: too many rows");
       return (int)LAKDE_EUNSUPPORTED;

@@ -4,8 +4,8 @@ Some kernels have more than one launch form that computes the same values
 (``lakde_tuning_set`` in include/lakde_b200.h): the FP64 factorisation with two
 warps per block or a lean form with one warp per block and 11 blocks per SM,
 the tensor-core kernels with their rows from an atomic work queue or on a
-static stride, the fused D <= 8 pass with 8 lanes or one thread per kernel
-row.  Which is faster depends on D, N and the pair counts, so the
+static stride, the fused D <= 8 pass with a kernel row's pairs on two lanes
+(its FP64 posterior on one lane per row) or with one thread per kernel row.  Which is faster depends on D, N and the pair counts, so the
 fused engine times every choice on its own data before its first CUDA-graph
 capture and keeps the fastest, per knob and class of D (the library's table
 is process-wide).  The factorisation and row-schedule choices give identical
@@ -22,7 +22,7 @@ from . import _native as nat
 KNOBS = {
     "factor": (0, ("two_warps_per_block", "one_warp_per_block_11_per_sm"), ("posterior_factor",)),
     "rows": (1, ("work_queue", "static_stride"), ("mstep_tc", "estep_tc")),
-    "vi_rows": (2, ("eight_lanes_per_row", "thread_per_row"), ("vi_rows",)),
+    "vi_rows": (2, ("two_lanes_per_row", "thread_per_row"), ("vi_rows",)),
 }
 
 
