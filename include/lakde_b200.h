@@ -428,6 +428,25 @@ LAKDE_API int lakde_weighted_gram(int dtype, int64_t N, int64_t D,
                                   double *out, void *workspace,
                                   size_t workspace_bytes, void *stream);
 
+/*
+ * Selection half of the exact kNN graph (lakde/utils.py:77-116: cdist +
+ * topk per row block, the point itself excluded at :104-105 unless
+ * include_self).  dist [nb, N] (float64, row-major) holds the squared
+ * distances of points row0 .. row0 + nb - 1 to all N points of X [N, D]
+ * (float64), e.g. |a|^2 + |b|^2 - 2ab from a library GEMM.  Per row: the
+ * k + 8 smallest entries (one pass, a shared-memory candidate buffer with a
+ * running threshold) are re-ranked by exact float64 differences, and the k
+ * nearest by (exact distance, index) go to out_idx [nb, k] (idx_dtype I32 /
+ * I64) and, if out_dist is given, their distances to out_dist [nb, k]
+ * (dist_dtype F32 / F64).  k <= N (include_self) or N - 1; candidates must
+ * fit in 200 KB of shared memory (k up to 15,352).
+ */
+LAKDE_API int lakde_knn_select(const void *dist, int64_t nb, int64_t N,
+                               int64_t row0, const void *X, int64_t D,
+                               int include_self, int64_t k, int idx_dtype,
+                               void *out_idx, int dist_dtype, void *out_dist,
+                               void *stream);
+
 /* Workspace bytes lakde_knn_elbo needs. */
 LAKDE_API size_t lakde_knn_elbo_workspace(void);
 

@@ -101,6 +101,10 @@ _SIGNATURES = {
     "lakde_knn_elbo_workspace": ([], ctypes.c_size_t),
     "lakde_weighted_gram_workspace": ([_c_i64], ctypes.c_size_t),
     "lakde_weighted_gram": ([_c_int, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, ctypes.c_size_t, _c_vp], _c_int),
+    "lakde_knn_select": (
+        [_c_vp, _c_i64, _c_i64, _c_i64, _c_vp, _c_i64, _c_int, _c_i64, _c_int, _c_vp, _c_int, _c_vp, _c_vp],
+        _c_int,
+    ),
     "lakde_tile_count": ([_c_i64], _c_i64),
     "lakde_pack_tiles": ([_c_int, _c_i64, _c_i64, _c_vp, _c_i64, _c_vp, _c_i64, _c_i64, _c_i64, _c_vp], _c_int),
     "lakde_mstep_tc_tiled": (

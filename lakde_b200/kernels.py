@@ -442,6 +442,28 @@ def weighted_gram(W_triu, w, out=None, workspace=None):
     return out
 
 
+def knn_select(dist, X, row0, k, include_self=False, out_idx=None, out_dist=None):
+    """The k nearest points of rows row0 .. row0 + nb - 1 from their float64
+    squared distances dist [nb, N] to all rows of X [N, D] (float64), nearest
+    first, ties by index, re-ranked by exact differences (lakde_knn_select,
+    see include/lakde_b200.h).  out_idx [nb, k] int32 or int64 (int64 if not
+    given); out_dist [nb, k] float32 or float64 (optional)."""
+    nat.require_cuda(dist, X, out_idx, out_dist, op="knn_select")
+    nb, N = dist.shape
+    dist = dist.contiguous()
+    X = X.contiguous()
+    if dist.dtype != torch.float64 or X.dtype != torch.float64:
+        raise TypeError("knn_select: dist and X must be float64")
+    if out_idx is None:
+        out_idx = torch.empty(nb, k, dtype=torch.int64, device=dist.device)
+    dist_code = nat.dtype_code(out_dist) if out_dist is not None else 0
+    nat.check(nat.lib().lakde_knn_select(nat.ptr(dist), nb, N, int(row0), nat.ptr(X), X.size(1), int(bool(include_self)),
+                                         int(k), nat.dtype_code(out_idx), nat.ptr(out_idx), dist_code,
+                                         nat.ptr(out_dist) if out_dist is not None else None, nat.stream_of(dist)),
+              "knn_select")
+    return out_idx
+
+
 def knn_elbo(a, b, nu, logdet_W, logdet_sigma_0, mm, c, a_0, b_0, nu_0, D, out=None, workspace=None):
     """ELBO of LocalKNearestKDE in float64 as a 0-dim device tensor (see include/lakde_b200.h)."""
     nat.require_cuda(a, b, nu, logdet_W, logdet_sigma_0, mm, c, op="knn_elbo")

@@ -1,8 +1,9 @@
 """Host-side helpers of the VI path, mirroring lakde/utils.py.
 
-compute_knn_graph ranks exact float64 distances on the GPU with a
-lower-index tie break (the order the oracle defines); batched_knn_cov is the
-scatter-covariance kernel on the kNN rows.
+compute_knn_graph ranks exact float64 distances on the GPU (a library GEMM
+for the candidate distances, the library's selection kernel for the rest)
+with a lower-index tie break (the order the oracle defines); batched_knn_cov
+is the scatter-covariance kernel on the kNN rows.
 """
 
 import signal
@@ -49,36 +50,24 @@ def batched_knn_cov(X, X_self, knn_graph, include_self=False, self_center=True):
 def compute_knn_graph(X, k, bsize=1024, return_dists=False, include_self=False, metric="l2", dtype=torch.int32):
     """k nearest neighbours of every row of X, nearest first (lakde/utils.py:77-116).
 
-    Candidates come from float64 distances |a|^2 + |b|^2 - 2ab (one cuBLAS
-    GEMM per row block); the best k + 8 are re-ranked by exact float64
-    differences, and equal distances are ordered by index.
+    Per block of rows, one library GEMM gives the float64 squared distances
+    |a|^2 + |b|^2 - 2ab to all points; lakde_knn_select (kernels.knn_select)
+    keeps each row's k + 8 smallest in one pass, re-ranks them by exact
+    float64 differences and writes the k nearest, equal distances ordered by
+    index.
     """
     if metric.lower() != "l2":
         raise ValueError("only the l2 metric is supported")
     N = X.size(0)
-    Xd = X.double()
+    Xd = X.double().contiguous()
     sq = (Xd * Xd).sum(1)
     I = torch.empty(N, k, dtype=dtype, device=X.device)
     Dout = X.new_empty(N, k) if return_dists else None
-    kc = min(k + 8, N)
     for i in range(0, N, bsize):
         Xb = Xd[i : i + bsize]
-        nb = Xb.size(0)
-        rows = torch.arange(nb, device=X.device)
         d = torch.addmm(sq[None, :], Xb, Xd.T, alpha=-2.0).add_(sq[i : i + bsize, None])
-        if not include_self:
-            d[rows, i + rows] = float("inf")
-        cand = d.topk(kc, dim=1, largest=False, sorted=False).indices
-        exact = ((Xd[cand] - Xb[:, None, :]) ** 2).sum(-1)
-        if not include_self:
-            exact[cand == (i + rows)[:, None]] = float("inf")
-        # order by exact distance, ties by index: sort by index, then stably by distance
-        o = torch.argsort(cand, dim=1)
-        cand, exact = cand.gather(1, o), exact.gather(1, o)
-        o = torch.argsort(exact, dim=1, stable=True)[:, :k]
-        I[i : i + bsize] = cand.gather(1, o).to(dtype)
-        if return_dists:
-            Dout[i : i + bsize] = exact.gather(1, o).sqrt().to(X.dtype)
+        kernels.knn_select(d, Xd, i, k, include_self=include_self, out_idx=I[i : i + bsize],
+                           out_dist=None if Dout is None else Dout[i : i + bsize])
     if return_dists:
         return Dout, I
     return I

@@ -12,7 +12,7 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("include_self", [False, True])
-@pytest.mark.parametrize("N,D,k", [(700, 3, 10), (3000, 8, 50), (2500, 43, 30)])
+@pytest.mark.parametrize("N,D,k", [(700, 3, 10), (3000, 8, 50), (2500, 43, 30), (3000, 6, 600), (4100, 5, 1500)])
 def test_knn_graph_is_exact(N, D, k, include_self):
     from lakde_b200.utils import compute_knn_graph
 
@@ -21,6 +21,22 @@ def test_knn_graph_is_exact(N, D, k, include_self):
     X[5] = X[9]  # an exact duplicate: tie broken by index
     g = compute_knn_graph(torch.tensor(X, device="cuda"), k, bsize=512, include_self=include_self)
     np.testing.assert_array_equal(g.cpu().numpy(), O.knn_graph(X, k, include_self=include_self))
+
+
+@pytest.mark.parametrize("out_dtype", [torch.float32, torch.float64])
+def test_knn_graph_distances_and_index_dtype(out_dtype):
+    from lakde_b200.utils import compute_knn_graph
+
+    rng = np.random.default_rng(7)
+    X = rng.standard_normal((1500, 7)).astype(np.float32)
+    Xt = torch.tensor(X, device="cuda").to(out_dtype)
+    d, g = compute_knn_graph(Xt, 20, bsize=256, return_dists=True, dtype=torch.int64)
+    assert g.dtype == torch.int64 and d.dtype == out_dtype
+    g = g.cpu().numpy()
+    np.testing.assert_array_equal(g, O.knn_graph(X, 20))
+    X64 = X.astype(np.float64)
+    exact = np.sqrt(((X64[g] - X64[:, None, :]) ** 2).sum(-1))
+    np.testing.assert_allclose(d.cpu().numpy(), exact, rtol=1e-6 if out_dtype == torch.float32 else 1e-12)
 
 
 def test_pattern_views_are_consistent():
