@@ -164,7 +164,6 @@ extern "C" int lakde_knn_select(const void *dist, int64_t nb, int64_t N, int64_t
     set_error("knn_select: null pointer or unsupported dtype");
     return LAKDE_EINVAL;
   }
-  if (int st = bind_device("knn_select", {dist, X, out_idx, out_dist})) return st;
   const int64_t kc = (k + 8 < avail) ? k + 8 : avail;
   int64_t cap = 2048;
   while (cap < kc + kKnnChunk) cap <<= 1;
@@ -173,6 +172,7 @@ extern "C" int lakde_knn_select(const void *dist, int64_t nb, int64_t N, int64_t
     set_error("knn_select: k=%lld needs %zu bytes of shared memory for its candidates", (long long)k, smem);
     return LAKDE_EUNSUPPORTED;
   }
+  if (int st = bind_device("knn_select", {dist, X, out_idx, out_dist})) return st;
   cudaStream_t s = as_stream(stream);
   auto launch = [&](auto ti, auto to) {
     using I = decltype(ti);

@@ -67,6 +67,14 @@ def test_invalid_arguments_are_rejected_on_the_host(nat):
     assert lib.lakde_w_cores_floats(21) == 6 * 128
     assert lib.lakde_w_cores_floats(3) == 128
     assert lib.lakde_w_cores_floats(65) == 0
+    # kNN selection: sizes, k against the candidate count, dtypes and the
+    # shared-memory bound of the candidate buffer, all before device work
+    assert lib.lakde_knn_select(p, 4, 10, 0, p, 3, 0, 10, 2, p, 0, None, None) == 1
+    assert b"exceeds" in lib.lakde_last_error()
+    assert lib.lakde_knn_select(p, 4, 10, 8, p, 3, 0, 5, 2, p, 0, None, None) == 1
+    assert lib.lakde_knn_select(p, 4, 10, 0, p, 3, 1, 10, 0, p, 0, None, None) == 1
+    assert lib.lakde_knn_select(p, 4, 100000, 0, p, 3, 0, 20000, 3, p, 0, None, None) == 4
+    assert b"shared memory" in lib.lakde_last_error()
 
 
 def test_cpu_tensors_are_rejected():
