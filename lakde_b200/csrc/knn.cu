@@ -17,8 +17,11 @@
 
 namespace lakde {
 
-constexpr int kKnnThreads = 256;
-constexpr int kKnnChunk = 4 * kKnnThreads;  // values a CTA scans between buffer checks
+// 256 threads per row, or 1,024 when the candidate buffer holds 4,096 or
+// more entries (large k: the buffer's sorts dominate, so more threads share
+// them; two such CTAs still fit an SM)
+constexpr int kKnnThreads = 256, kKnnThreadsLarge = 1024;
+constexpr int kKnnChunk = 1024;  // values a CTA scans between buffer checks
 
 // Ascending bitonic sort of n (a power of two) (key, index) pairs in shared
 // memory, ties by index; every thread of the CTA takes part.
@@ -46,7 +49,7 @@ __device__ __forceinline__ void bitonic_sort(double *key, int32_t *idx, int n) {
 }
 
 template <typename I, typename O>
-__global__ void __launch_bounds__(kKnnThreads) knn_select_kernel(const double *__restrict__ dist, int64_t N,
+__global__ void __launch_bounds__(kKnnThreadsLarge) knn_select_kernel(const double *__restrict__ dist, int64_t N,
                                                                  int64_t row0, const double *__restrict__ X, int D,
                                                                  int include_self, int k, int kc, int cap,
                                                                  I *__restrict__ out_idx, O *__restrict__ out_dist) {
@@ -84,9 +87,8 @@ __global__ void __launch_bounds__(kKnnThreads) knn_select_kernel(const double *_
       __syncthreads();
     }
     const double t_now = thr;
-#pragma unroll
-    for (int u = 0; u < kKnnChunk / kKnnThreads; ++u) {
-      const int64_t j = base + u * kKnnThreads + threadIdx.x;
+    for (int u = threadIdx.x; u < kKnnChunk; u += blockDim.x) {
+      const int64_t j = base + u;
       if (j < N) {
         double v = drow[j];
         if (v != v || (!include_self && j == self)) v = inf;
@@ -182,7 +184,8 @@ extern "C" int lakde_knn_select(const void *dist, int64_t nb, int64_t N, int64_t
       set_error("knn_select: cannot reserve %zu bytes of shared memory", smem);
       return (int)LAKDE_ECUDA;
     }
-    kern<<<(unsigned)nb, kKnnThreads, smem, s>>>(static_cast<const double *>(dist), N, row0,
+    const int threads = cap >= 4096 ? kKnnThreadsLarge : kKnnThreads;
+    kern<<<(unsigned)nb, threads, smem, s>>>(static_cast<const double *>(dist), N, row0,
                                                  static_cast<const double *>(X), (int)D, include_self, (int)k,
                                                  (int)kc, (int)cap, static_cast<I *>(out_idx),
                                                  static_cast<O *>(out_dist));
